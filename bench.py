@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 SGBM engine (one JSON line on stdout, rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl reference]
+
+A step is one full StereoSGBM computation (cost volume, SGM aggregation, WTA,
+LR check, median) of one seeded synthetic pair, default the 1920x1080,
+maxDisparity=128, SAD + Sobel-x prefilter, 8-path configuration.  ``value`` is
+pixel-disparities per second (W*H*D per step) of the whole job with the inputs
+resident in HBM; ``e2e`` is the same metric through the host-buffer C-ABI
+call (pinned host memory, host<->device copies inside the timed region).
+
+Multi-GPU (torchrun): replicas -- every rank computes its own copy of the
+workload on its own GPU, no collective on the data path; value = all ranks'
+pixel-disparities / max-over-ranks device time.
+
+``--impl reference`` times the reference's algorithm on the host cores (the C
+restatement in oracle/, all threads, a bounded sample of the same workload)
+and, when a GPU and oracle/_ref are present, the reference's own CUDA kernels
+on the GPU as extra information.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from lumenstereo_b200 import MatchingCostMode, StereoParams, StereoSGBM, synth  # noqa: E402
+
+DEFAULT_WORKLOAD = "1920x1080_d128_sad_8path"
+METRIC = "pixel-disparities/s vs HBM roofline"
+UNIT = "pd/s"
+FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(synth.WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--schedule", type=int, default=0, help="aggregation schedule (0 = auto)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def workload_params(wl) -> StereoParams:
+    # StereoParams{} defaults except the configuration's fields and the speckle
+    # filter (off: not one of the measured stages, and racy in the reference).
+    return StereoParams(maxDisparity=wl.max_disparity, numDirections=wl.num_directions,
+                        matchingCostMode=MatchingCostMode.Census if wl.census else MatchingCostMode.SAD,
+                        speckleWindowSize=0)
+
+
+def params_dict(p: StereoParams):
+    return {k: int(v) for k, v in p.__dict__.items()}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(workload: str):
+    """DRAM bytes per pixel-disparity of the aggregation stage from the ncu
+    summary committed under profiles/ (None when absent)."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(workload)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (C restatement of the reference path), all threads
+# ---------------------------------------------------------------------------
+def cpu_port_rate(p: dict, left, right, budget_s: float = 15.0):
+    """pixel-disparities/s of the oracle on a bounded sample of the workload:
+    the full pair when it fits the budget, else a band of full-width rows."""
+    from oracle import oracle
+    H, W = left.shape
+    D = p["maxDisparity"] - p["minDisparity"]
+    probe_rows = max(8, H // 16)
+    t = time.perf_counter()
+    oracle.sgbm(p, left[:probe_rows], right[:probe_rows])
+    t_probe = time.perf_counter() - t
+    est_full = t_probe * H / probe_rows
+    if est_full <= budget_s:
+        rows = H
+        reps = max(1, int(round(budget_s / max(est_full, 1e-3) * 0.6)))
+    else:
+        rows = max(probe_rows, int(H * budget_s / est_full))
+        reps = 1
+    t = time.perf_counter()
+    for _ in range(reps):
+        oracle.sgbm(p, left[:rows], right[:rows])
+    dt = time.perf_counter() - t
+    sample = f"{reps} x {W}x{rows} rows of the {W}x{H} pair (D={D})"
+    return W * rows * D * reps / dt, oracle.max_threads(), sample
+
+
+def opencv_rate(p: dict, left, right, paths: int):
+    """OpenCV StereoSGBM (cv2, host cores) on the same pair: a baseline only
+    (a different SGBM formulation), MODE_HH for 8 paths, MODE_HH4 for 4."""
+    try:
+        import cv2
+    except Exception:
+        return None
+    D = p["maxDisparity"] - p["minDisparity"]
+    nd = ((D + 15) // 16) * 16
+    m = cv2.StereoSGBM_create(minDisparity=0, numDisparities=nd, blockSize=5, P1=200, P2=800,
+                              disp12MaxDiff=1, preFilterCap=31, uniquenessRatio=10,
+                              speckleWindowSize=0, speckleRange=0,
+                              mode=cv2.StereoSGBM_MODE_HH if paths == 8 else cv2.StereoSGBM_MODE_HH4)
+    cv2.setNumThreads(os.cpu_count() or 1)
+    m.compute(left, right)
+    ts = []
+    for _ in range(3):
+        t = time.perf_counter()
+        m.compute(left, right)
+        ts.append(time.perf_counter() - t)
+    H, W = left.shape
+    return {"value": W * H * D / statistics.median(ts), "unit": UNIT,
+            "threads": cv2.getNumThreads(), "numDisparities": nd,
+            "mode": "MODE_HH" if paths == 8 else "MODE_HH4"}
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    wl = synth.WORKLOADS[args.workload]
+    left, right, gt = synth.make_pair(wl.pair)
+    H, W = left.shape
+    D = wl.max_disparity
+    params = workload_params(wl)
+    pd_per_step = W * H * D
+    sgbm = StereoSGBM(params)
+    if args.schedule:
+        sgbm.set_schedule(args.schedule)
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+    dl = torch.from_numpy(left).to(dev)
+    dr = torch.from_numpy(right).to(dev)
+    dout = torch.empty((H, W), dtype=torch.int16, device=dev)
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+
+    def step():
+        sgbm.compute_device(dl.data_ptr(), dr.data_ptr(), W, H, dout.data_ptr(), stream=sptr)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize()
+    check = dout.cpu().numpy()
+    v = check > 0
+    quality = {"valid_frac": float(v.mean()),
+               "bad2_frac": float(np.mean(np.abs(check[v] / 16.0 - gt[v]) > 2)) if v.any() else None}
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    launches0 = sgbm.launch_count()
+    step_ms, agg_ms, cost_ms, sel_ms = [], [], [], []
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()  # L2 flush, outside the step's events
+            ev[k][0].record(stream)
+            step()
+            ev[k][1].record(stream)
+            t = sgbm.timings()  # waits for this step; stage times from the handle's events
+            cost_ms.append(t[1]); agg_ms.append(t[2]); sel_ms.append(t[3])
+        torch.cuda.synchronize()
+        barrier()
+    launches = sgbm.launch_count() - launches0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    value = pd_per_step * args.steps * world / (total_ms / 1e3)
+
+    # e2e: host buffers through the C-ABI call (H2D + compute + D2H per step)
+    lh = torch.from_numpy(left).pin_memory()
+    rh = torch.from_numpy(right).pin_memory()
+    oh = torch.empty((H, W), dtype=torch.int16).pin_memory()
+    from lumenstereo_b200 import _lib, _check
+    lib = _lib.lib()
+
+    def e2e_step():
+        _check(lib.lumen_sgbm_compute(sgbm._h, lh.data_ptr(), rh.data_ptr(), W, H, W, 1,
+                                      oh.data_ptr(), W * 2))
+
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier()
+    e2e_time = 0.0
+    for _ in range(args.steps):
+        flush.zero_()  # L2 flush, outside the timed call
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()     # synchronous: H2D, pipeline, D2H
+        e2e_time += time.perf_counter() - t0
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([e2e_time], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_time = float(tt.item())
+    e2e_value = pd_per_step * args.steps * world / e2e_time
+
+    hbm, peak_kind = measured_peaks()
+    P = wl.num_directions
+    agg_mean = statistics.mean(agg_ms)
+    agg_bytes = (P + 2) * pd_per_step          # cost read once per path + agg written once
+    achieved = agg_bytes / (agg_mean / 1e3) / 1e9
+    traffic_per_pd = profiled_traffic(args.workload)
+    pipe_ms = statistics.mean(step_ms)
+    pipe_bytes = (P + 5) * pd_per_step         # SGM core model: cost w + P reads, agg w + r
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+        "config": {"workload": args.workload, "width": W, "height": H, "max_disparity": D,
+                   "cost": "census" if wl.census else "sad+sobel-x prefilter",
+                   "paths": P, "params": "StereoParams defaults, speckleWindowSize=0",
+                   "l2": "256 MiB buffer written before every timed step, outside its events",
+                   "parallelism": f"replicas x{world}", "schedule": args.schedule or "auto"},
+        "roofline": {"bound": "hbm", "kernel": "sgm aggregation stage",
+                     "achieved": achieved, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": achieved / hbm,
+                     "algorithmic_bytes_per_pd": P + 2,
+                     "traffic": None if traffic_per_pd is None else traffic_per_pd * pd_per_step,
+                     "mean_ms": agg_mean},
+        "pipeline_roofline": {"algorithmic_bytes_per_pd": P + 5, "mean_ms": pipe_ms,
+                              "achieved": pipe_bytes / (pipe_ms / 1e3) / 1e9, "peak": hbm,
+                              "frac": pipe_bytes / (pipe_ms / 1e3) / 1e9 / hbm},
+        "stage_ms": {"cost": statistics.mean(cost_ms), "aggregate": agg_mean,
+                     "select_post": statistics.mean(sel_ms)},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * W * H,
+                "d2h_bytes_per_step": 2 * W * H, "ms_per_step": e2e_time / args.steps * 1e3},
+        "gpu_launches": int(launches),
+        "clocks": clocks.summary(),
+        "quality": quality,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        pdct = params_dict(params)
+        try:
+            rate, cores, sample = cpu_port_rate(pdct, left, right)
+            result["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port",
+                                      "sample": sample}
+        except Exception as e:  # report, never hide
+            result["cpu_baseline"] = {"value": None, "error": repr(e)}
+        ocv = opencv_rate(pdct, left, right, P)
+        if ocv:
+            result["opencv_cpu"] = ocv
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    sgbm.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    wl = synth.WORKLOADS[args.workload]
+    left, right, _ = synth.make_pair(wl.pair)
+    H, W = left.shape
+    D = wl.max_disparity
+    p = params_dict(workload_params(wl))
+    from oracle import oracle
+    # each step: a bounded sample (full-width band of rows) of ~4 s on the host cores
+    probe = max(8, H // 16)
+    t = time.perf_counter()
+    oracle.sgbm(p, left[:probe], right[:probe])
+    est = (time.perf_counter() - t) * H / probe
+    rows = H if est <= 4.0 else max(probe, int(H * 4.0 / est))
+    for _ in range(args.warmup):
+        oracle.sgbm(p, left[:rows], right[:rows])
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.sgbm(p, left[:rows], right[:rows])
+    dt = time.perf_counter() - t
+    value = W * rows * D * args.steps / dt
+    sample = f"{W}x{rows} rows of the {W}x{H} pair (D={D}) per step"
+    res = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+           "config": {"workload": args.workload, "width": W, "height": H, "max_disparity": D,
+                      "paths": wl.num_directions, "cost": "census" if wl.census else "sad"},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": oracle.max_threads(),
+                            "kind": "port", "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    # The reference's own CUDA kernels on this GPU (information only).
+    try:
+        import torch
+        if torch.cuda.is_available() and oracle.ref_available():
+            _, _, ms = oracle.ref_sgbm(p, left, right, repeats=3)
+            res["reference_cuda_gpu"] = {"value": W * H * D / (ms / 1e3), "unit": UNIT,
+                                         "ms_per_pair": ms,
+                                         "what": "LumenStereo src/sgbm_kernels.cu (sm_100, -O3 "
+                                                 "--use_fast_math) with its host sequence; "
+                                                 "getLastComputeTimeMs interval"}
+    except Exception as e:
+        res["reference_cuda_gpu"] = {"error": repr(e)}
+    print(json.dumps(res), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,164 @@
+/*
+ * lumen_sgbm.h -- C ABI of the B200 SGBM stereo engine.
+ *
+ * Plain C: pointers, sizes and POD structs only, so any FFI (ctypes, cgo, JNI,
+ * N-API) can bind it.  Each entry point names the LumenStereo interface it
+ * replaces (paths relative to the LumenStereo source tree).  The header-only
+ * C++ wrapper in include/stereo/sgbm_gpu.h restores the reference's
+ * stereo::StereoSGBM class and exception types on top of these calls.
+ *
+ * Threading: a handle is not thread-safe (like stereo::StereoSGBM); separate
+ * handles may be used from separate threads.  lumen_last_error_string() is
+ * per thread.
+ */
+#ifndef LUMEN_SGBM_H
+#define LUMEN_SGBM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LUMEN_SGBM_ABI_VERSION 1
+
+/* Replaces stereo::kSgbmMaxDisparityRange (include/stereo/sgbm_limits.h:9). */
+#define LUMEN_MAX_DISPARITY_RANGE 512
+
+/* Status codes.  INVALID_ARGUMENT and RANGE_EXCEEDS_LIMIT are the cases in
+ * which the reference throws StereoException (src/sgbm_gpu.cu:148-166);
+ * CUDA_ERROR is the reference's CudaException (include/stereo/common.h:31-84). */
+typedef enum lumen_status {
+    LUMEN_OK = 0,
+    LUMEN_ERR_INVALID_ARGUMENT = 1,   /* empty input, size mismatch, bad disparity range */
+    LUMEN_ERR_RANGE_EXCEEDS_LIMIT = 2, /* maxDisparity - minDisparity > 512 */
+    LUMEN_ERR_CUDA = 3,               /* a CUDA call failed; see lumen_last_error_string() */
+    LUMEN_ERR_OUT_OF_BUDGET = 4,      /* request larger than the device-memory budget */
+    LUMEN_ERR_TIMEOUT = 5,            /* a bounded device-side wait gave up */
+    LUMEN_ERR_NO_DEVICE = 6           /* no CUDA device / kernels not loadable */
+} lumen_status;
+
+/* Field-for-field mirror of stereo::StereoParams (include/stereo/stereo_params.h:57-82,
+ * defaults from the same lines; fill with lumen_stereo_params_default()). */
+typedef struct lumen_stereo_params {
+    int32_t minDisparity;      /* 0 */
+    int32_t maxDisparity;      /* 128 */
+    int32_t blockSize;         /* 5 */
+    int32_t P1;                /* 200 */
+    int32_t P2;                /* 800 */
+    int32_t preFilterCap;      /* 31 */
+    int32_t uniquenessRatio;   /* 10 */
+    int32_t disp12MaxDiff;     /* 1, -1 disables the LR check */
+    int32_t speckleWindowSize; /* 100, 0 disables the speckle filter */
+    int32_t speckleRange;      /* 32 */
+    int32_t useGPU;            /* 1 (read and written, never acted on, as in the reference) */
+    int32_t useSharedMemory;   /* 1 (accepted; every cost kernel here stages through shared memory) */
+    int32_t numDirections;     /* 4, or 8 for the four diagonal paths too */
+    int32_t matchingCostMode;  /* 0 = SAD (Sobel-x prefilter), 1 = Census 5x5 */
+} lumen_stereo_params;
+
+typedef struct lumen_sgbm lumen_sgbm;
+
+/* StereoParams{} (include/stereo/stereo_params.h:57-82). */
+void lumen_stereo_params_default(lumen_stereo_params* out);
+/* StereoParams::isValid (stereo_params.h:96-103): 1 valid, 0 not. */
+int lumen_stereo_params_is_valid(const lumen_stereo_params* p);
+/* StereoParams::autoComputePenalties (stereo_params.h:88-91). */
+void lumen_stereo_params_auto_penalties(lumen_stereo_params* p, int numChannels);
+
+/* StereoSGBM::StereoSGBM (include/stereo/sgbm_gpu.h:31, src/sgbm_gpu.cu:100-107):
+ * binds the current CUDA device, creates the handle's stream and events.
+ * params may be NULL for the defaults. */
+lumen_status lumen_sgbm_create(const lumen_stereo_params* params, lumen_sgbm** out);
+/* StereoSGBM::~StereoSGBM (src/sgbm_gpu.cu:109-113); frees every device buffer. */
+lumen_status lumen_sgbm_destroy(lumen_sgbm* h);
+/* StereoSGBM::setParams / getParams (include/stereo/sgbm_gpu.h:46-47). */
+lumen_status lumen_sgbm_set_params(lumen_sgbm* h, const lumen_stereo_params* params);
+lumen_status lumen_sgbm_get_params(const lumen_sgbm* h, lumen_stereo_params* out);
+
+/* StereoSGBM::compute (include/stereo/sgbm_gpu.h:41, src/sgbm_gpu.cu:147-195) on
+ * HOST buffers, synchronous.  left/right: height rows of width*channels bytes,
+ * row pitch in_stride bytes (0 = tightly packed); channels 1 (gray) or 3 (BGR,
+ * converted with BT.601 15-bit fixed point like cv::cvtColor(COLOR_BGR2GRAY)).
+ * out: height rows of width int16 disparities in 1/16 px (-1 = invalid), row
+ * pitch out_stride bytes (0 = packed). */
+lumen_status lumen_sgbm_compute(lumen_sgbm* h, const uint8_t* left, const uint8_t* right,
+                                int width, int height, size_t in_stride, int channels,
+                                int16_t* out, size_t out_stride);
+
+/* Same computation on DEVICE buffers, asynchronous on `stream` (a
+ * cudaStream_t; NULL = the handle's own stream).  Returns after enqueueing;
+ * the caller synchronises.  No host<->device copies. */
+lumen_status lumen_sgbm_compute_device(lumen_sgbm* h, const uint8_t* d_left,
+                                       const uint8_t* d_right, int width, int height,
+                                       size_t in_stride, int channels, int16_t* d_out,
+                                       size_t out_stride, void* stream);
+
+/* getLastComputeTimeMs / getCostComputeTimeMs / getAggregationTimeMs /
+ * getPostProcessTimeMs (include/stereo/sgbm_gpu.h:52-55), device time in ms of
+ * the last synchronous compute: out[0] total, [1] cost, [2] aggregation,
+ * [3] disparity selection + post-processing.  After lumen_sgbm_compute_device
+ * the first call waits for that compute's last event. */
+lumen_status lumen_sgbm_get_timings(lumen_sgbm* h, float out[4]);
+
+/* Human-readable message of the last failing call on this thread ("" if none). */
+const char* lumen_last_error_string(void);
+
+/* ---- diagnostics (no counterpart in the reference's public API; they expose the
+ * intermediate buffers the parity tests compare stage by stage) ---- */
+
+/* Path-set override for the next computes: bit i selects path i in the order
+ * LR, RL, TB, BT, TLBR, BRTL, TRBL, BLTR (src/sgbm_gpu.cu:321-421); 0 restores
+ * the numDirections default. */
+lumen_status lumen_sgbm_debug_set_paths(lumen_sgbm* h, uint32_t path_mask);
+/* Aggregation schedule: 0 = automatic (autotuner / heuristic), 1 = one kernel
+ * per direction, 2 = two fused wavefront sweeps.  Values, not outputs, are the
+ * same for every schedule. */
+lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule);
+/* Copies one internal buffer of the last compute to host memory `dst`
+ * (capacity dst_bytes).  which: 0 prefiltered left, 1 prefiltered right,
+ * 2 census left (uint32), 3 census right, 4 cost volume (uint8 HxWxD),
+ * 5 aggregated volume (uint16 HxWxD), 6 left WTA disparity, 7 right
+ * disparity, 8 disparity after the LR check (and speckle filter), 9 gray left,
+ * 10 gray right.  Volumes are returned densely packed with D entries per
+ * pixel.  The debug-retain flag must have been set before the compute. */
+lumen_status lumen_sgbm_debug_retain(lumen_sgbm* h, int enable);
+lumen_status lumen_sgbm_debug_copy(lumen_sgbm* h, int which, void* dst, size_t dst_bytes);
+/* Number of kernels this handle has enqueued so far (all computes). */
+unsigned long long lumen_sgbm_debug_launch_count(const lumen_sgbm* h);
+
+/* ---- rectification remap (replaces stereo::StereoRectifier,
+ * include/stereo/rectification.h:41-84, and rectifyImageGPU :92-97) ---- */
+typedef struct lumen_rectifier lumen_rectifier;
+
+/* StereoRectifier(const CameraParams&) (src/rectification.cu:259-284): uploads
+ * the four CV_32FC1 maps (width*height floats each) once; NULL maps mean the
+ * pair is pre-rectified and rectify() copies. */
+lumen_status lumen_rectifier_create(int width, int height, const float* map0x,
+                                    const float* map0y, const float* map1x,
+                                    const float* map1y, lumen_rectifier** out);
+lumen_status lumen_rectifier_destroy(lumen_rectifier* r);
+int lumen_rectifier_is_pre_rectified(const lumen_rectifier* r);
+/* StereoRectifier::rectify (src/rectification.cu:286-345) on host buffers. */
+lumen_status lumen_rectifier_rectify(lumen_rectifier* r, const uint8_t* left_raw,
+                                     const uint8_t* right_raw, int channels,
+                                     uint8_t* left_rect, uint8_t* right_rect);
+/* Device-buffer form, asynchronous on `stream`. */
+lumen_status lumen_rectifier_rectify_device(lumen_rectifier* r, const uint8_t* d_left_raw,
+                                            const uint8_t* d_right_raw, int channels,
+                                            uint8_t* d_left_rect, uint8_t* d_right_rect,
+                                            void* stream);
+/* rectifyImageGPU (src/rectification.cu:354-411): one image, host buffers. */
+lumen_status lumen_remap(const uint8_t* src, const float* map_x, const float* map_y,
+                         uint8_t* dst, int width, int height, int channels);
+
+/* BGR -> gray on the device (the reference calls cv::cvtColor on the host,
+ * src/sgbm_gpu.cu:169-172); host buffers, one image. */
+lumen_status lumen_bgr_to_gray(const uint8_t* bgr, size_t stride, uint8_t* gray, int width,
+                               int height);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LUMEN_SGBM_H */

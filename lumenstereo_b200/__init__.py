@@ -1,0 +1,327 @@
+"""lumenstereo_b200 -- B200-native SGBM stereo matching.
+
+Python mirror of LumenStereo's public C++ API for the stereo path
+(include/stereo/stereo_params.h, sgbm_limits.h, sgbm_gpu.h, rectification.h,
+common.h of the reference), over the C ABI in include/lumen_sgbm.h:
+
+    params = StereoParams(maxDisparity=64, numDirections=8)
+    sgbm = StereoSGBM(params)
+    disparity = sgbm.compute(left, right)      # int16, 1/16 px, -1 invalid
+
+Errors follow the reference: StereoException for empty input, size mismatch
+and bad disparity ranges; CudaException (with ``error_code``) for CUDA
+failures.  Arrays are numpy; device tensors (torch) go through
+``compute_device``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, fields
+from enum import IntEnum
+
+import numpy as np
+
+from . import _lib
+
+__all__ = ["MatchingCostMode", "StereoParams", "StereoSGBM", "StereoRectifier",
+           "StereoException", "CudaException", "kSgbmMaxDisparityRange",
+           "middleburyMatcherMaxDisparity", "rectify_image_gpu", "bgr_to_gray"]
+
+# include/stereo/sgbm_limits.h:9
+kSgbmMaxDisparityRange = 512
+
+
+def middleburyMatcherMaxDisparity(calibNumDisparities: int, fallbackWhenMissing: int = 96) -> int:
+    """include/stereo/sgbm_limits.h:11-22."""
+    ndisp = calibNumDisparities if calibNumDisparities > 0 else fallbackWhenMissing
+    return kSgbmMaxDisparityRange if ndisp > kSgbmMaxDisparityRange else ndisp
+
+
+class MatchingCostMode(IntEnum):
+    """include/stereo/stereo_params.h:20-23."""
+    SAD = 0
+    Census = 1
+
+
+@dataclass
+class StereoParams:
+    """include/stereo/stereo_params.h:57-104 (same fields, defaults and checks)."""
+    minDisparity: int = 0
+    maxDisparity: int = 128
+    blockSize: int = 5
+    P1: int = 200
+    P2: int = 800
+    preFilterCap: int = 31
+    uniquenessRatio: int = 10
+    disp12MaxDiff: int = 1
+    speckleWindowSize: int = 100
+    speckleRange: int = 32
+    useGPU: bool = True
+    useSharedMemory: bool = True
+    numDirections: int = 4
+    matchingCostMode: MatchingCostMode = MatchingCostMode.SAD
+
+    def autoComputePenalties(self, numChannels: int = 1) -> None:
+        self.P1 = 8 * numChannels * self.blockSize * self.blockSize
+        self.P2 = 32 * numChannels * self.blockSize * self.blockSize
+
+    def isValid(self) -> bool:
+        if self.blockSize < 1 or self.blockSize % 2 == 0:
+            return False
+        if self.minDisparity < 0:
+            return False
+        if self.maxDisparity <= self.minDisparity:
+            return False
+        if self.P2 <= self.P1:
+            return False
+        if self.uniquenessRatio < 0 or self.uniquenessRatio > 100:
+            return False
+        return True
+
+    def to_c(self) -> _lib.CParams:
+        return _lib.CParams(*[int(getattr(self, n)) for n in _lib.PARAM_FIELDS])
+
+    @classmethod
+    def from_c(cls, c: _lib.CParams) -> "StereoParams":
+        vals = {n: getattr(c, n) for n in _lib.PARAM_FIELDS}
+        vals["useGPU"] = bool(vals["useGPU"])
+        vals["useSharedMemory"] = bool(vals["useSharedMemory"])
+        vals["matchingCostMode"] = MatchingCostMode(vals["matchingCostMode"])
+        return cls(**vals)
+
+    def replace(self, **kw) -> "StereoParams":
+        d = {f.name: getattr(self, f.name) for f in fields(self)}
+        d.update(kw)
+        return StereoParams(**d)
+
+
+class StereoException(RuntimeError):
+    """include/stereo/common.h:105-110."""
+
+
+class CudaException(RuntimeError):
+    """include/stereo/common.h:31-48 (``error_code`` carries the status)."""
+
+    def __init__(self, msg: str, error_code: int = _lib.ERR_CUDA):
+        super().__init__(msg)
+        self.error_code = error_code
+
+
+class TimeoutException(CudaException):
+    """A bounded device-side wait gave up (LUMEN_ERR_TIMEOUT)."""
+
+
+class OutOfBudgetException(StereoException):
+    """A request does not fit the device-memory budget (LUMEN_ERR_OUT_OF_BUDGET)."""
+
+
+def _check(status: int) -> None:
+    if status == _lib.OK:
+        return
+    msg = _lib.last_error()
+    if status in (_lib.ERR_INVALID_ARGUMENT, _lib.ERR_RANGE_EXCEEDS_LIMIT):
+        raise StereoException(msg)
+    if status == _lib.ERR_OUT_OF_BUDGET:
+        raise OutOfBudgetException(msg)
+    if status == _lib.ERR_TIMEOUT:
+        raise TimeoutException(msg, status)
+    raise CudaException(msg, status)
+
+
+def _image_view(img: np.ndarray):
+    """(array, channels, row stride) for a uint8 HxW or HxWx3 image whose rows
+    are contiguous; copies otherwise."""
+    if img.dtype != np.uint8:
+        raise StereoException("input images must be uint8")
+    if img.ndim == 3 and img.shape[2] == 1:
+        img = img[:, :, 0]
+    if img.ndim == 2:
+        ch = 1
+    elif img.ndim == 3 and img.shape[2] == 3:
+        ch = 3
+    else:
+        raise StereoException("input images must be gray (HxW) or BGR (HxWx3)")
+    inner_ok = (img.strides[-1] == 1) and (ch == 1 or img.strides[1] == 3)
+    if not inner_ok or img.strides[0] < img.shape[1] * ch:
+        img = np.ascontiguousarray(img)
+    return img, ch, img.strides[0]
+
+
+class StereoSGBM:
+    """include/stereo/sgbm_gpu.h:29-91."""
+
+    def __init__(self, params: StereoParams | None = None):
+        self._h = C.c_void_p()
+        p = (params or StereoParams()).to_c()
+        _check(_lib.lib().lumen_sgbm_create(C.byref(p), C.byref(self._h)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.lib().lumen_sgbm_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def setParams(self, params: StereoParams) -> None:
+        p = params.to_c()
+        _check(_lib.lib().lumen_sgbm_set_params(self._h, C.byref(p)))
+
+    def getParams(self) -> StereoParams:
+        c = _lib.CParams()
+        _check(_lib.lib().lumen_sgbm_get_params(self._h, C.byref(c)))
+        return StereoParams.from_c(c)
+
+    def compute(self, left: np.ndarray, right: np.ndarray,
+                disparity: np.ndarray | None = None) -> np.ndarray:
+        """StereoSGBM::compute (src/sgbm_gpu.cu:147-195): returns (or fills)
+        an int16 HxW disparity map in 1/16 px, -1 = invalid."""
+        left = np.asarray(left)
+        right = np.asarray(right)
+        if left.size == 0 or right.size == 0:
+            raise StereoException("Input images are empty")
+        if left.shape[:2] != right.shape[:2]:
+            raise StereoException("Left and right images must have same size")
+        left, ch, stride = _image_view(left)
+        right, chr_, stride_r = _image_view(right)
+        if ch != chr_:
+            raise StereoException("Left and right images must have the same channel count")
+        if stride_r != stride:
+            right = np.ascontiguousarray(right)
+            left = np.ascontiguousarray(left)
+            stride = left.strides[0]
+        h, w = left.shape[:2]
+        if disparity is None or disparity.shape != (h, w) or disparity.dtype != np.int16:
+            disparity = np.empty((h, w), np.int16)
+        elif disparity.strides[1] != 2:
+            raise StereoException("disparity output must have contiguous rows")
+        _check(_lib.lib().lumen_sgbm_compute(
+            self._h, left.ctypes.data, right.ctypes.data, w, h, stride, ch,
+            disparity.ctypes.data, disparity.strides[0]))
+        return disparity
+
+    def compute_device(self, left_ptr: int, right_ptr: int, width: int, height: int,
+                       out_ptr: int, channels: int = 1, in_stride: int = 0, out_stride: int = 0,
+                       stream: int = 0) -> None:
+        """Asynchronous compute on device buffers (raw CUDA pointers, e.g.
+        ``tensor.data_ptr()``) on ``stream`` (a cudaStream_t as int)."""
+        _check(_lib.lib().lumen_sgbm_compute_device(
+            self._h, left_ptr, right_ptr, width, height, in_stride, channels, out_ptr,
+            out_stride, stream or None))
+
+    def _timings(self):
+        t = (C.c_float * 4)()
+        _check(_lib.lib().lumen_sgbm_get_timings(self._h, t))
+        return list(t)
+
+    def getLastComputeTimeMs(self) -> float:
+        return self._timings()[0]
+
+    def getCostComputeTimeMs(self) -> float:
+        return self._timings()[1]
+
+    def getAggregationTimeMs(self) -> float:
+        return self._timings()[2]
+
+    def getPostProcessTimeMs(self) -> float:
+        return self._timings()[3]
+
+    # ---- diagnostics (no counterpart in the reference API) ----
+    def set_debug_paths(self, mask: int) -> None:
+        _check(_lib.lib().lumen_sgbm_debug_set_paths(self._h, mask))
+
+    def set_schedule(self, schedule: int) -> None:
+        _check(_lib.lib().lumen_sgbm_set_schedule(self._h, schedule))
+
+    def launch_count(self) -> int:
+        """Kernels this handle has enqueued so far."""
+        return int(_lib.lib().lumen_sgbm_debug_launch_count(self._h))
+
+    def timings(self):
+        """[total, cost, aggregation, select+post] device ms of the last compute."""
+        return self._timings()
+
+    def retain_intermediates(self, enable: bool = True) -> None:
+        _check(_lib.lib().lumen_sgbm_debug_retain(self._h, 1 if enable else 0))
+
+    def intermediate(self, which: str, shape, dtype) -> np.ndarray:
+        ids = {"pref_left": 0, "pref_right": 1, "census_left": 2, "census_right": 3,
+               "cost": 4, "agg": 5, "disp_wta": 6, "disp_right": 7, "disp_lr": 8,
+               "gray_left": 9, "gray_right": 10}
+        out = np.empty(shape, dtype)
+        _check(_lib.lib().lumen_sgbm_debug_copy(self._h, ids[which], out.ctypes.data, out.nbytes))
+        return out
+
+
+class StereoRectifier:
+    """include/stereo/rectification.h:41-84.  Maps are CV_32FC1 float32 HxW
+    arrays (map0x, map0y for the left camera, map1x, map1y for the right);
+    without maps the pair is treated as pre-rectified."""
+
+    def __init__(self, width: int, height: int, map0x=None, map0y=None, map1x=None, map1y=None):
+        self._h = C.c_void_p()
+        self._maps = [None if m is None else np.ascontiguousarray(m, np.float32)
+                      for m in (map0x, map0y, map1x, map1y)]
+        ptrs = [None if m is None else m.ctypes.data for m in self._maps]
+        _check(_lib.lib().lumen_rectifier_create(width, height, *ptrs, C.byref(self._h)))
+        self.width, self.height = width, height
+
+    def isPreRectified(self) -> bool:
+        return bool(_lib.lib().lumen_rectifier_is_pre_rectified(self._h))
+
+    def rectify(self, left_raw: np.ndarray, right_raw: np.ndarray):
+        l = np.ascontiguousarray(left_raw, np.uint8)
+        r = np.ascontiguousarray(right_raw, np.uint8)
+        ch = 1 if l.ndim == 2 else l.shape[2]
+        ol = np.empty_like(l)
+        orr = np.empty_like(r)
+        _check(_lib.lib().lumen_rectifier_rectify(self._h, l.ctypes.data, r.ctypes.data, ch,
+                                                  ol.ctypes.data, orr.ctypes.data))
+        return ol, orr
+
+    def rectify_device(self, left_ptr: int, right_ptr: int, channels: int, out_left_ptr: int,
+                       out_right_ptr: int, stream: int = 0) -> None:
+        _check(_lib.lib().lumen_rectifier_rectify_device(
+            self._h, left_ptr, right_ptr, channels, out_left_ptr, out_right_ptr, stream or None))
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            _lib.lib().lumen_rectifier_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def rectify_image_gpu(src: np.ndarray, map_x: np.ndarray, map_y: np.ndarray) -> np.ndarray:
+    """rectifyImageGPU (src/rectification.cu:354-411)."""
+    s = np.ascontiguousarray(src, np.uint8)
+    ch = 1 if s.ndim == 2 else s.shape[2]
+    h, w = map_x.shape
+    mx = np.ascontiguousarray(map_x, np.float32)
+    my = np.ascontiguousarray(map_y, np.float32)
+    dst = np.empty_like(s)
+    _check(_lib.lib().lumen_remap(s.ctypes.data, mx.ctypes.data, my.ctypes.data, dst.ctypes.data,
+                                  w, h, ch))
+    return dst
+
+
+def bgr_to_gray(bgr: np.ndarray) -> np.ndarray:
+    """Device BGR -> gray, BT.601 15-bit fixed point (cv::cvtColor semantics)."""
+    b = np.ascontiguousarray(bgr, np.uint8)
+    h, w = b.shape[:2]
+    g = np.empty((h, w), np.uint8)
+    _check(_lib.lib().lumen_bgr_to_gray(b.ctypes.data, b.strides[0], g.ctypes.data, w, h))
+    return g

@@ -1,0 +1,87 @@
+"""ctypes binding of liblumen_sgbm.so (the C ABI in include/lumen_sgbm.h).
+
+The shared library is built in-tree by ``lumenstereo_b200.build``.  There is no
+CPU or Python fallback: if the library cannot be loaded, every entry point
+raises, so a GPU run can never silently measure something else.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblumen_sgbm.so")
+
+_lock = threading.Lock()
+_lib = None
+
+# lumen_status
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_RANGE_EXCEEDS_LIMIT = 2
+ERR_CUDA = 3
+ERR_OUT_OF_BUDGET = 4
+ERR_TIMEOUT = 5
+ERR_NO_DEVICE = 6
+
+PARAM_FIELDS = ("minDisparity", "maxDisparity", "blockSize", "P1", "P2", "preFilterCap",
+                "uniquenessRatio", "disp12MaxDiff", "speckleWindowSize", "speckleRange",
+                "useGPU", "useSharedMemory", "numDirections", "matchingCostMode")
+
+
+class CParams(C.Structure):
+    _fields_ = [(n, C.c_int32) for n in PARAM_FIELDS]
+
+
+def _declare(lib):
+    vp, i, sz = C.c_void_p, C.c_int, C.c_size_t
+    sig = {
+        "lumen_stereo_params_default": (None, [C.POINTER(CParams)]),
+        "lumen_stereo_params_is_valid": (i, [C.POINTER(CParams)]),
+        "lumen_stereo_params_auto_penalties": (None, [C.POINTER(CParams), i]),
+        "lumen_sgbm_create": (i, [C.POINTER(CParams), C.POINTER(vp)]),
+        "lumen_sgbm_destroy": (i, [vp]),
+        "lumen_sgbm_set_params": (i, [vp, C.POINTER(CParams)]),
+        "lumen_sgbm_get_params": (i, [vp, C.POINTER(CParams)]),
+        "lumen_sgbm_compute": (i, [vp, vp, vp, i, i, sz, i, vp, sz]),
+        "lumen_sgbm_compute_device": (i, [vp, vp, vp, i, i, sz, i, vp, sz, vp]),
+        "lumen_sgbm_get_timings": (i, [vp, C.POINTER(C.c_float)]),
+        "lumen_last_error_string": (C.c_char_p, []),
+        "lumen_sgbm_debug_set_paths": (i, [vp, C.c_uint32]),
+        "lumen_sgbm_set_schedule": (i, [vp, i]),
+        "lumen_sgbm_debug_retain": (i, [vp, i]),
+        "lumen_sgbm_debug_copy": (i, [vp, i, vp, sz]),
+        "lumen_sgbm_debug_launch_count": (C.c_ulonglong, [vp]),
+        "lumen_rectifier_create": (i, [i, i, vp, vp, vp, vp, C.POINTER(vp)]),
+        "lumen_rectifier_destroy": (i, [vp]),
+        "lumen_rectifier_is_pre_rectified": (i, [vp]),
+        "lumen_rectifier_rectify": (i, [vp, vp, vp, i, vp, vp]),
+        "lumen_rectifier_rectify_device": (i, [vp, vp, vp, i, vp, vp, vp]),
+        "lumen_remap": (i, [vp, vp, vp, vp, i, i, i]),
+        "lumen_bgr_to_gray": (i, [vp, sz, vp, i, i]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def lib():
+    """The loaded library (raises OSError when it is missing or unloadable)."""
+    global _lib
+    if _lib is None:
+        with _lock:
+            if _lib is None:
+                if not os.path.exists(LIB_PATH):
+                    raise OSError(
+                        f"{LIB_PATH} is missing: build it with `python -m lumenstereo_b200.build`")
+                handle = C.CDLL(LIB_PATH)
+                _declare(handle)
+                _lib = handle
+    return _lib
+
+
+def last_error() -> str:
+    msg = lib().lumen_last_error_string()
+    return msg.decode() if msg else ""

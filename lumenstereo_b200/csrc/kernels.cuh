@@ -1,0 +1,38 @@
+// kernels.cuh -- launchers of the B200 SGBM kernels (host-callable).
+#pragma once
+#include "common.cuh"
+
+namespace lumen {
+
+// Number of path lines of direction dir (LR, RL, TB, BT, TLBR, BRTL, TRBL, BLTR).
+__host__ __device__ inline int num_lines(int dir, int W, int H) {
+    return dir < 2 ? H : (dir < 4 ? W : W + H - 1);
+}
+
+void launch_stage_gray(const uint8_t* l, const uint8_t* r, size_t pitch, int channels, int W,
+                       int H, uint8_t* gl, uint8_t* gr, cudaStream_t s, int nImages = 2);
+void launch_prefilter(const uint8_t* gl, const uint8_t* gr, int W, int H, int cap, uint8_t* pl,
+                      uint8_t* pr, cudaStream_t s);
+void launch_census(const uint8_t* gl, const uint8_t* gr, int W, int H, uint32_t* cl, uint32_t* cr,
+                   cudaStream_t s);
+cudaError_t launch_census_cost(const uint32_t* cl, const uint32_t* cr, int W, int H, int D, int Dp,
+                               int minD, uint8_t* cost, cudaStream_t s);
+size_t sad_cost_smem(int Dp, int r);
+cudaError_t launch_sad_cost(const uint8_t* pl, const uint8_t* pr, int W, int H, int D, int Dp,
+                            int minD, int r, const uint32_t* magic, int wide, uint8_t* cost,
+                            cudaStream_t s);
+
+cudaError_t launch_aggregate_per_direction(const PairView& pv, const SgmConsts& k,
+                                           unsigned pathMask, bool wrap, cudaStream_t s);
+
+cudaError_t launch_select(const uint16_t* agg, int W, int H, int D, int Dp, int minD, int UR,
+                          int16_t* dispL, int16_t* dispR, cudaStream_t s);
+cudaError_t launch_post(const int16_t* dispL, const int16_t* dispR, int W, int H, int lrMaxDiff,
+                        int speckleSize, int speckleDiff, int16_t* out, size_t outPitchElems,
+                        int16_t* dbgLR, cudaStream_t s);
+
+void launch_remap(const uint8_t* srcL, const uint8_t* srcR, const float* mxL, const float* myL,
+                  const float* mxR, const float* myR, uint8_t* dstL, uint8_t* dstR, int W, int H,
+                  int channels, int nImages, cudaStream_t s);
+
+}  // namespace lumen

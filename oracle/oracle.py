@@ -1,0 +1,206 @@
+"""ctypes bindings to the test-only checkers.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline / reference legs of bench.py, never by the product package.
+
+* ``liboracle.so``  -- C restatement of the reference's SGBM path (sgbm_oracle.c)
+* ``_ref/libref_sgbm.so`` -- the reference's own CUDA kernels with a host
+  driver that restates src/sgbm_gpu.cu (needs a GPU; optional).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import astuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF = None
+
+PATH_NAMES = ["LR", "RL", "TB", "BT", "TLBR", "BRTL", "TRBL", "BLTR"]
+
+
+class OracleParams(C.Structure):
+    _fields_ = [(n, C.c_int) for n in (
+        "minDisparity", "maxDisparity", "blockSize", "P1", "P2", "preFilterCap",
+        "uniquenessRatio", "disp12MaxDiff", "speckleWindowSize", "speckleRange", "useGPU",
+        "useSharedMemory", "numDirections", "matchingCostMode")]
+
+
+class OracleIntermediates(C.Structure):
+    _fields_ = [("gray_left", C.c_void_p), ("gray_right", C.c_void_p),
+                ("pref_left", C.c_void_p), ("pref_right", C.c_void_p),
+                ("census_left", C.c_void_p), ("census_right", C.c_void_p),
+                ("cost", C.c_void_p), ("agg", C.c_void_p), ("disp_wta", C.c_void_p),
+                ("disp_right", C.c_void_p), ("disp_lr", C.c_void_p)]
+
+
+class RefDump(C.Structure):
+    _fields_ = [("pref_left", C.c_void_p), ("pref_right", C.c_void_p),
+                ("census_left", C.c_void_p), ("census_right", C.c_void_p),
+                ("cost", C.c_void_p), ("agg", C.c_void_p), ("disp_wta", C.c_void_p),
+                ("disp_right", C.c_void_p), ("disp_lr", C.c_void_p)]
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def build():
+    """Build liboracle.so (and _ref when the reference tree is present)."""
+    import subprocess
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        _LIB = C.CDLL(path)
+        _LIB.oracle_sgbm_compute.restype = C.c_int
+        _LIB.oracle_sgbm_compute.argtypes = [C.POINTER(OracleParams), C.c_void_p, C.c_void_p,
+                                             C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                             C.POINTER(OracleIntermediates), C.c_uint]
+        _LIB.oracle_max_threads.restype = C.c_int
+    return _LIB
+
+
+def ref_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libref_sgbm.so"))
+
+
+def ref():
+    global _REF
+    if _REF is None:
+        _REF = C.CDLL(os.path.join(HERE, "_ref", "libref_sgbm.so"))
+        _REF.ref_sgbm_run.restype = C.c_int
+        _REF.ref_sgbm_run.argtypes = [C.POINTER(OracleParams), C.c_void_p, C.c_void_p, C.c_int,
+                                      C.c_int, C.c_void_p, C.POINTER(RefDump), C.c_uint, C.c_int,
+                                      C.POINTER(C.c_float)]
+        _REF.ref_remap_run.restype = C.c_int
+        _REF.ref_last_error.restype = C.c_char_p
+    return _REF
+
+
+def to_params(p) -> OracleParams:
+    """From any object with the StereoParams field names (or a dict)."""
+    get = (lambda k: p[k]) if isinstance(p, dict) else (lambda k: getattr(p, k))
+    vals = []
+    for name, _ in OracleParams._fields_:
+        v = get(name)
+        vals.append(int(v))
+    return OracleParams(*vals)
+
+
+def set_threads(n: int):
+    lib().oracle_set_threads(int(n))
+
+
+def max_threads() -> int:
+    return lib().oracle_max_threads()
+
+
+def sgbm(params, left: np.ndarray, right: np.ndarray, intermediates: bool = False,
+         path_mask: int = 0):
+    """Full pipeline. Returns disparity (int16 HxW), or (disparity, dict)."""
+    left = np.ascontiguousarray(left)
+    right = np.ascontiguousarray(right)
+    h, w = left.shape[:2]
+    ch = 1 if left.ndim == 2 else left.shape[2]
+    p = to_params(params)
+    D = p.maxDisparity - p.minDisparity
+    out = np.zeros((h, w), np.int16)
+    inter = None
+    arrs = {}
+    if intermediates:
+        arrs = dict(
+            gray_left=np.zeros((h, w), np.uint8), gray_right=np.zeros((h, w), np.uint8),
+            pref_left=np.zeros((h, w), np.uint8), pref_right=np.zeros((h, w), np.uint8),
+            census_left=np.zeros((h, w), np.uint32), census_right=np.zeros((h, w), np.uint32),
+            cost=np.zeros((h, w, max(D, 1)), np.uint8), agg=np.zeros((h, w, max(D, 1)), np.uint16),
+            disp_wta=np.zeros((h, w), np.int16), disp_right=np.zeros((h, w), np.int16),
+            disp_lr=np.zeros((h, w), np.int16))
+        inter = OracleIntermediates(*[_ptr(arrs[f]) for f, _ in OracleIntermediates._fields_])
+    rc = lib().oracle_sgbm_compute(C.byref(p), _ptr(left), _ptr(right), w, h, ch, _ptr(out),
+                                   C.byref(inter) if inter is not None else None, path_mask)
+    if rc != 0:
+        raise RuntimeError(f"oracle_sgbm_compute failed with status {rc}")
+    return (out, arrs) if intermediates else out
+
+
+def remap(src: np.ndarray, mapx: np.ndarray, mapy: np.ndarray) -> np.ndarray:
+    src = np.ascontiguousarray(src)
+    h, w = mapx.shape
+    ch = 1 if src.ndim == 2 else src.shape[2]
+    dst = np.zeros_like(src)
+    lib().oracle_remap(_ptr(src), _ptr(np.ascontiguousarray(mapx, np.float32)),
+                       _ptr(np.ascontiguousarray(mapy, np.float32)), _ptr(dst), w, h, ch)
+    return dst
+
+
+def bgr2gray(bgr: np.ndarray) -> np.ndarray:
+    bgr = np.ascontiguousarray(bgr)
+    h, w = bgr.shape[:2]
+    g = np.zeros((h, w), np.uint8)
+    lib().oracle_bgr2gray(_ptr(bgr), _ptr(g), w, h, C.c_size_t(w * 3))
+    return g
+
+
+def median3x3(disp: np.ndarray) -> np.ndarray:
+    disp = np.ascontiguousarray(disp, np.int16)
+    h, w = disp.shape
+    out = np.zeros_like(disp)
+    lib().oracle_median3x3(_ptr(disp), _ptr(out), w, h)
+    return out
+
+
+def speckle(disp: np.ndarray, max_speckle: int, max_diff: int) -> np.ndarray:
+    disp = np.array(disp, np.int16, copy=True)
+    h, w = disp.shape
+    lib().oracle_speckle(_ptr(disp), w, h, int(max_speckle), int(max_diff))
+    return disp
+
+
+def ref_sgbm(params, left: np.ndarray, right: np.ndarray, intermediates: bool = False,
+             path_mask: int = 0, repeats: int = 1):
+    """The reference's CUDA pipeline on the GPU (gray input).  Returns
+    (disparity, dict of intermediates, best device ms)."""
+    left = np.ascontiguousarray(left, np.uint8)
+    right = np.ascontiguousarray(right, np.uint8)
+    h, w = left.shape
+    p = to_params(params)
+    D = p.maxDisparity - p.minDisparity
+    out = np.zeros((h, w), np.int16)
+    arrs = {}
+    dump = None
+    if intermediates:
+        arrs = dict(pref_left=np.zeros((h, w), np.uint8), pref_right=np.zeros((h, w), np.uint8),
+                    census_left=np.zeros((h, w), np.uint32),
+                    census_right=np.zeros((h, w), np.uint32),
+                    cost=np.zeros((h, w, D), np.uint8), agg=np.zeros((h, w, D), np.uint16),
+                    disp_wta=np.zeros((h, w), np.int16), disp_right=np.zeros((h, w), np.int16),
+                    disp_lr=np.zeros((h, w), np.int16))
+        dump = RefDump(*[_ptr(arrs[f]) for f, _ in RefDump._fields_])
+    ms = C.c_float(0.0)
+    rc = ref().ref_sgbm_run(C.byref(p), _ptr(left), _ptr(right), w, h, _ptr(out),
+                            C.byref(dump) if dump is not None else None, path_mask, repeats,
+                            C.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"ref_sgbm_run failed ({rc}): {ref().ref_last_error()!r}")
+    return out, arrs, ms.value
+
+
+def ref_remap(src: np.ndarray, mapx: np.ndarray, mapy: np.ndarray) -> np.ndarray:
+    src = np.ascontiguousarray(src)
+    h, w = mapx.shape
+    ch = 1 if src.ndim == 2 else src.shape[2]
+    dst = np.zeros_like(src)
+    rc = ref().ref_remap_run(_ptr(src), _ptr(np.ascontiguousarray(mapx, np.float32)),
+                             _ptr(np.ascontiguousarray(mapy, np.float32)), _ptr(dst), w, h, ch)
+    if rc != 0:
+        raise RuntimeError(f"ref_remap_run failed ({rc})")
+    return dst

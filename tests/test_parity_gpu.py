@@ -1,0 +1,302 @@
+"""CUDA path vs the oracle (bit-exact integer stages, 1/16-px subpixel
+tolerance), through the C ABI.  Mirrors the reference's SGBM tests
+(tests/test_sgbm.cpp:163-406) and adds the value checks they lack.
+
+Tolerance for 1/16-px maps: the CUDA path divides with --use_fast_math like
+the reference; the oracle divides in IEEE single precision, so a pixel may
+differ by 1 (= 1/16 px) on at most 0.01% of pixels (one pixel for tiny maps).
+Against the reference's own kernels (oracle/_ref) the maps must be identical.
+"""
+import os
+import zlib
+
+import numpy as np
+import pytest
+
+from lumenstereo_b200 import (MatchingCostMode, StereoException, StereoParams, StereoSGBM,
+                              bgr_to_gray, kSgbmMaxDisparityRange, rectify_image_gpu, synth)
+from tests.conftest import params_dict
+
+pytestmark = pytest.mark.gpu
+
+SUBPIX_FRAC = 1e-4
+
+
+def assert_subpix_close(ours, ref, what=""):
+    bad = ours != ref
+    assert np.all(np.abs(ours.astype(int) - ref.astype(int))[bad] <= 1), what
+    assert bad.sum() <= max(1, int(SUBPIX_FRAC * bad.size)), (what, int(bad.sum()))
+
+
+def to_params(d):
+    d = dict(d)
+    d["matchingCostMode"] = MatchingCostMode(d["matchingCostMode"])
+    return StereoParams(**d)
+
+
+def run_ours(pdict, left, right, path_mask=0, schedule=0):
+    p = to_params(pdict)
+    h, w = left.shape[:2]
+    D = p.maxDisparity - p.minDisparity
+    with StereoSGBM(p) as s:
+        s.retain_intermediates(True)
+        if path_mask:
+            s.set_debug_paths(path_mask)
+        if schedule:
+            s.set_schedule(schedule)
+        disp = s.compute(left, right)
+        inter = dict(cost=s.intermediate("cost", (h, w, D), np.uint8),
+                     agg=s.intermediate("agg", (h, w, D), np.uint16),
+                     disp_wta=s.intermediate("disp_wta", (h, w), np.int16),
+                     disp_right=s.intermediate("disp_right", (h, w), np.int16),
+                     disp_lr=s.intermediate("disp_lr", (h, w), np.int16))
+        if p.matchingCostMode == MatchingCostMode.Census:
+            inter["census_left"] = s.intermediate("census_left", (h, w), np.uint32)
+            inter["census_right"] = s.intermediate("census_right", (h, w), np.uint32)
+        else:
+            inter["pref_left"] = s.intermediate("pref_left", (h, w), np.uint8)
+            inter["pref_right"] = s.intermediate("pref_right", (h, w), np.uint8)
+    return disp, inter
+
+
+def compare_all(pdict, left, right, oracle_mod, path_mask=0, schedule=0):
+    disp, ours = run_ours(pdict, left, right, path_mask, schedule)
+    ref_disp, ref = oracle_mod.sgbm(pdict, left, right, intermediates=True, path_mask=path_mask)
+    for key in ("census_left", "census_right", "pref_left", "pref_right", "cost", "agg"):
+        if key in ours:
+            assert np.array_equal(ours[key], ref[key]), key
+    # integer WTA (first strict minimum) from the bit-exact volume
+    assert np.array_equal(np.argmin(ours["agg"], axis=2), np.argmin(ref["agg"], axis=2))
+    assert_subpix_close(ours["disp_wta"], ref["disp_wta"], "disp_wta")
+    assert_subpix_close(ours["disp_right"], ref["disp_right"], "disp_right")
+    assert_subpix_close(ours["disp_lr"], ref["disp_lr"], "disp_lr")
+    assert_subpix_close(disp, ref_disp, "disp")
+    return disp
+
+
+CASES = {
+    "census_4path_d32": (64, 48, dict(maxDisparity=32, matchingCostMode=1)),
+    "sad_8path_d64": (96, 64, dict(maxDisparity=64, numDirections=8)),
+    "census_8path_d45_min3": (72, 40, dict(minDisparity=3, maxDisparity=48, matchingCostMode=1,
+                                           numDirections=8)),
+    "sad_4path_bs3_ur0_nolr": (60, 44, dict(maxDisparity=24, blockSize=3, uniquenessRatio=0,
+                                            disp12MaxDiff=-1)),
+    "sad_8path_bs7_speckle": (80, 36, dict(maxDisparity=40, blockSize=7, numDirections=8,
+                                           speckleWindowSize=100, speckleRange=2)),
+    "census_d290_tail": (330, 20, dict(maxDisparity=290, matchingCostMode=1, numDirections=8)),
+    "sad_d512": (600, 10, dict(maxDisparity=512, numDirections=8)),
+    "census_d192": (260, 30, dict(maxDisparity=192, matchingCostMode=1, numDirections=8)),
+    "sad_d1": (30, 20, dict(maxDisparity=1)),
+    "sad_d2_odd_w": (31, 17, dict(maxDisparity=2, numDirections=8)),
+    "census_wrap_bs21": (40, 30, dict(maxDisparity=16, matchingCostMode=1, blockSize=21,
+                                      preFilterCap=63, P1=30000, P2=60000, numDirections=8)),
+    "sad_wrap_bs19": (48, 32, dict(maxDisparity=16, blockSize=19, numDirections=8)),
+    "sad_wide_bs11_cap127": (64, 40, dict(maxDisparity=24, blockSize=11, preFilterCap=127,
+                                          numDirections=8)),
+    "sad_bs0": (40, 20, dict(maxDisparity=8, blockSize=0)),
+    "census_tiny_5x3": (5, 3, dict(maxDisparity=4, matchingCostMode=1, numDirections=8)),
+    "sad_tiny_2x2": (2, 2, dict(maxDisparity=3, numDirections=8)),
+    "sad_minD20_ur15": (90, 30, dict(minDisparity=20, maxDisparity=52, uniquenessRatio=15,
+                                     numDirections=8)),
+    "census_minD100_wide": (120, 16, dict(minDisparity=100, maxDisparity=164,
+                                          matchingCostMode=1)),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_parity_small(name, oracle_mod):
+    w, h, over = CASES[name]
+    if w * h >= 2048:
+        left, right, _ = synth.make_pair(synth.PairSpec(w, h, 4, 1, max(2, 0.3 * min(w, 300)), 2.0,
+                                                        zlib.crc32(name.encode()) % 1000))
+    else:
+        left, right = synth.random_pair(w, h, seed=zlib.crc32(name.encode()) % 1000, shift=1)
+    compare_all(params_dict(speckleWindowSize=0, **over) if "speckle" not in name
+                else params_dict(**over), left, right, oracle_mod)
+
+
+@pytest.mark.parametrize("k", range(8))
+def test_parity_single_path(k, oracle_mod):
+    left, right = synth.random_pair(70, 45, seed=40 + k, shift=4)
+    for mode in (0, 1):
+        compare_all(params_dict(maxDisparity=40, numDirections=8, matchingCostMode=mode,
+                                speckleWindowSize=0), left, right, oracle_mod, path_mask=1 << k)
+
+
+def test_parity_color_input(oracle_mod):
+    """SGBMTest.ColorInput (tests/test_sgbm.cpp:194-218) plus values: BGR is
+    converted on the device like cv::cvtColor(COLOR_BGR2GRAY)."""
+    rng = np.random.default_rng(7)
+    left = rng.integers(0, 256, (48, 64, 3), dtype=np.uint8)
+    right = np.roll(left, -3, axis=1)
+    p = params_dict(maxDisparity=32, speckleWindowSize=0)
+    disp, _ = run_ours(p, left, right)
+    ref = oracle_mod.sgbm(p, left, right)
+    assert disp.dtype == np.int16 and disp.shape == (48, 64)
+    assert_subpix_close(disp, ref, "color")
+
+
+def test_bgr_to_gray_matches_oracle(oracle_mod):
+    rng = np.random.default_rng(8)
+    img = rng.integers(0, 256, (123, 77, 3), dtype=np.uint8)
+    assert np.array_equal(bgr_to_gray(img), oracle_mod.bgr2gray(img))
+
+
+def test_compute_basic_shifted_rectangles():
+    """SGBMTest.ComputeBasic (tests/test_sgbm.cpp:163-192)."""
+    left = np.zeros((100, 100), np.uint8)
+    right = np.zeros((100, 100), np.uint8)
+    left[30:71, 30:71] = 128
+    right[30:71, 25:66] = 128
+    with StereoSGBM(StereoParams(maxDisparity=32, blockSize=5, numDirections=4)) as s:
+        disp = s.compute(left, right)
+        assert disp.shape == left.shape and disp.dtype == np.int16
+        assert s.getLastComputeTimeMs() > 0
+
+
+def test_different_sizes_and_disparities(oracle_mod):
+    """SGBMTest.DifferentSizes / DifferentDisparities (tests/test_sgbm.cpp:220-281),
+    one handle reused across sizes (buffers grow)."""
+    rng = np.random.default_rng(3)
+    with StereoSGBM(StereoParams(maxDisparity=32, numDirections=4, speckleWindowSize=0)) as s:
+        for (h, w) in [(48, 64), (96, 128), (240, 320), (480, 640), (48, 64)]:
+            left = rng.integers(0, 255, (h, w), dtype=np.uint8)
+            right = rng.integers(0, 255, (h, w), dtype=np.uint8)
+            disp = s.compute(left, right)
+            assert disp.shape == (h, w)
+            if h <= 96:
+                assert_subpix_close(disp, oracle_mod.sgbm(params_dict(maxDisparity=32,
+                                                                      speckleWindowSize=0),
+                                                          left, right))
+    left = rng.integers(0, 255, (240, 320), dtype=np.uint8)
+    right = rng.integers(0, 255, (240, 320), dtype=np.uint8)
+    for md in (32, 64, 96, 128):
+        with StereoSGBM(StereoParams(maxDisparity=md, numDirections=4)) as s:
+            assert s.compute(left, right).shape == (240, 320)
+
+
+def test_empty_input():
+    with StereoSGBM(StereoParams()) as s:
+        with pytest.raises(StereoException):
+            s.compute(np.zeros((0, 0), np.uint8), np.zeros((0, 0), np.uint8))
+
+
+def test_size_mismatch():
+    with StereoSGBM(StereoParams()) as s:
+        with pytest.raises(StereoException):
+            s.compute(np.zeros((100, 100), np.uint8), np.zeros((100, 200), np.uint8))
+
+
+def test_disparity_range_exceeds_gpu_limit():
+    rng = np.random.default_rng(0)
+    img = rng.integers(0, 255, (64, 64), dtype=np.uint8)
+    with StereoSGBM(StereoParams(minDisparity=0, maxDisparity=kSgbmMaxDisparityRange + 32)) as s:
+        with pytest.raises(StereoException):
+            s.compute(img, img)
+    with StereoSGBM(StereoParams(minDisparity=10, maxDisparity=10)) as s:
+        with pytest.raises(StereoException):
+            s.compute(img, img)
+
+
+def test_deterministic_and_handle_reuse():
+    left, right, _ = synth.make_pair(synth.PairSpec(200, 120, 5, 4, 40, 2.0, 77))
+    p = StereoParams(maxDisparity=48, numDirections=8, matchingCostMode=MatchingCostMode.Census)
+    with StereoSGBM(p) as s:
+        a = s.compute(left, right).copy()
+        b = s.compute(left, right).copy()
+    with StereoSGBM(p) as s2:
+        c = s2.compute(left, right)
+    assert np.array_equal(a, b) and np.array_equal(a, c)
+
+
+def test_compute_device_matches_host():
+    torch = pytest.importorskip("torch")
+    left, right, _ = synth.make_pair(synth.PairSpec(256, 96, 5, 4, 40, 2.0, 78))
+    p = StereoParams(maxDisparity=64, numDirections=8)
+    with StereoSGBM(p) as s:
+        host = s.compute(left, right)
+        dl = torch.from_numpy(left).cuda()
+        dr = torch.from_numpy(right).cuda()
+        out = torch.empty((96, 256), dtype=torch.int16, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        s.compute_device(dl.data_ptr(), dr.data_ptr(), 256, 96, out.data_ptr(), stream=stream)
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), host)
+
+
+def test_remap_known_answers(oracle_mod):
+    """RectificationTest.GPUvsOpenCV / BilinearInterpolation
+    (tests/test_rectification.cpp:189-265) and bit-exactness vs the oracle."""
+    cv2 = pytest.importorskip("cv2")
+    rng = np.random.default_rng(1)
+    src = rng.integers(0, 255, (480, 640), dtype=np.uint8)
+    my, mx = np.mgrid[0:480, 0:640].astype(np.float32)
+    assert np.array_equal(rectify_image_gpu(src, mx, my), cv2.remap(src, mx, my, cv2.INTER_LINEAR))
+    g = np.tile((np.arange(100) * 255 // 100).astype(np.uint8), (100, 1))
+    my2, mx2 = np.mgrid[0:100, 0:100].astype(np.float32)
+    mx2 += 0.5
+    my2 += 0.5
+    ours = rectify_image_gpu(g, mx2, my2)
+    assert np.abs(ours.astype(int) - cv2.remap(g, mx2, my2, cv2.INTER_LINEAR).astype(int)).max() <= 1
+    # random sub-pixel maps, gray and BGR: identical to the oracle
+    for ch in (1, 3):
+        img = rng.integers(0, 256, (90, 120) if ch == 1 else (90, 120, 3), dtype=np.uint8)
+        mxr = (rng.random((90, 120)) * 130 - 5).astype(np.float32)
+        myr = (rng.random((90, 120)) * 100 - 5).astype(np.float32)
+        assert np.array_equal(rectify_image_gpu(img, mxr, myr), oracle_mod.remap(img, mxr, myr))
+
+
+# ---------------------------------------------------------------------------
+# The reference's own CUDA pipeline (oracle/_ref) at the benchmark sizes.
+# ---------------------------------------------------------------------------
+def _ref_or_skip(oracle_mod):
+    if not oracle_mod.ref_available():
+        pytest.skip("oracle/_ref not built (needs the reference tree at build time)")
+
+
+@pytest.mark.parametrize("wl", ["640x480_d64_census_4path", "1920x1080_d128_sad_8path",
+                                "1920x1080_d128_census_8path", "2880x1988_d290_census_8path"])
+def test_parity_vs_reference_kernels_full_size(wl, oracle_mod):
+    _ref_or_skip(oracle_mod)
+    w = synth.WORKLOADS[wl]
+    left, right, gt = synth.make_pair(w.pair)
+    p = params_dict(maxDisparity=w.max_disparity, matchingCostMode=int(w.census),
+                    numDirections=w.num_directions, speckleWindowSize=0)
+    ref_disp, ref, _ = oracle_mod.ref_sgbm(p, left, right, intermediates=False)
+    ours, inter = run_ours_light(p, left, right)
+    assert np.array_equal(ours, ref_disp)
+    # sanity: the scene's disparities are recovered
+    v = ours > 0
+    assert v.mean() > 0.5
+    assert np.median(np.abs(ours[v] / 16.0 - gt[v])) < 1.0
+
+
+def run_ours_light(pdict, left, right):
+    p = to_params(pdict)
+    with StereoSGBM(p) as s:
+        return s.compute(left, right), None
+
+
+def test_parity_vs_reference_kernels_intermediates(oracle_mod):
+    """Every checkpoint against the reference kernels on the 640x480 workload."""
+    _ref_or_skip(oracle_mod)
+    w = synth.WORKLOADS["640x480_d64_census_4path"]
+    left, right, _ = synth.make_pair(w.pair)
+    for mode, nd, ur in ((1, 4, 10), (0, 8, 0), (1, 8, 0)):
+        p = params_dict(maxDisparity=64, matchingCostMode=mode, numDirections=nd,
+                        uniquenessRatio=ur, speckleWindowSize=0)
+        ref_disp, ref, _ = oracle_mod.ref_sgbm(p, left, right, intermediates=True)
+        disp, ours = run_ours(p, left, right)
+        for key in ("cost", "agg", "disp_wta", "disp_right", "disp_lr"):
+            assert np.array_equal(ours[key], ref[key]), (mode, nd, key)
+        assert np.array_equal(disp, ref_disp)
+
+
+def test_remap_vs_reference_kernel(oracle_mod):
+    _ref_or_skip(oracle_mod)
+    rng = np.random.default_rng(2)
+    for ch in (1, 3):
+        img = rng.integers(0, 256, (200, 300) if ch == 1 else (200, 300, 3), dtype=np.uint8)
+        mx = (rng.random((200, 300)) * 320 - 10).astype(np.float32)
+        my = (rng.random((200, 300)) * 220 - 10).astype(np.float32)
+        assert np.array_equal(rectify_image_gpu(img, mx, my), oracle_mod.ref_remap(img, mx, my))
