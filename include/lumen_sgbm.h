@@ -88,8 +88,8 @@ lumen_status lumen_sgbm_compute(lumen_sgbm* h, const uint8_t* left, const uint8_
                                 int16_t* out, size_t out_stride);
 
 /* Same computation on DEVICE buffers, asynchronous on `stream` (a
- * cudaStream_t; NULL = the handle's own stream).  Returns after enqueueing;
- * the caller synchronises.  No host<->device copies. */
+ * cudaStream_t; NULL = the default stream, as in every CUDA API).  Returns
+ * after enqueueing; the caller synchronises.  No host<->device copies. */
 lumen_status lumen_sgbm_compute_device(lumen_sgbm* h, const uint8_t* d_left,
                                        const uint8_t* d_right, int width, int height,
                                        size_t in_stride, int channels, int16_t* d_out,
@@ -144,7 +144,7 @@ int lumen_rectifier_is_pre_rectified(const lumen_rectifier* r);
 lumen_status lumen_rectifier_rectify(lumen_rectifier* r, const uint8_t* left_raw,
                                      const uint8_t* right_raw, int channels,
                                      uint8_t* left_rect, uint8_t* right_rect);
-/* Device-buffer form, asynchronous on `stream`. */
+/* Device-buffer form, asynchronous on `stream` (NULL = the default stream). */
 lumen_status lumen_rectifier_rectify_device(lumen_rectifier* r, const uint8_t* d_left_raw,
                                             const uint8_t* d_right_raw, int channels,
                                             uint8_t* d_left_rect, uint8_t* d_right_rect,

@@ -216,7 +216,7 @@ class StereoSGBM:
         ``tensor.data_ptr()``) on ``stream`` (a cudaStream_t as int)."""
         _check(_lib.lib().lumen_sgbm_compute_device(
             self._h, left_ptr, right_ptr, width, height, in_stride, channels, out_ptr,
-            out_stride, stream or None))
+            out_stride, stream or None))  # 0 / None: the default stream
 
     def _timings(self):
         t = (C.c_float * 4)()

@@ -36,7 +36,20 @@ __device__ __forceinline__ void fill_p2_lut(int* lut, int P1, int P2) {
     for (int g = threadIdx.x; g < 256; g += blockDim.x) lut[g] = max(P1 + 1, P2 * 8 / max(8, g));
 }
 
-template <int KW, bool WRAP, bool FULL>
+// Number of pixels on the line that starts at (x, y) with step (sx, sy).
+__device__ __forceinline__ int line_length(int x, int y, int sx, int sy, int W, int H) {
+    int n = 1 << 30;
+    if (sx > 0) n = min(n, W - x);
+    if (sx < 0) n = min(n, x + 1);
+    if (sy > 0) n = min(n, H - y);
+    if (sy < 0) n = min(n, y + 1);
+    return n;
+}
+
+// One warp per path line.  Loads of the cost and aggregated words (and the
+// image byte) for pixel i+PF are issued while pixel i is computed: the
+// recurrence's step chain never waits on DRAM latency.
+template <int KW, bool WRAP, bool FULL, int PF>
 __global__ void __launch_bounds__(128)
 agg_dir_kernel(PairView pv, SgmConsts k, int dir, int first) {
     __shared__ int p2lut[256];
@@ -45,54 +58,67 @@ agg_dir_kernel(PairView pv, SgmConsts k, int dir, int first) {
     const int lane = threadIdx.x & 31;
     const int li = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (li >= num_lines(dir, k.W, k.H)) return;
-    int x, y, sx, sy;
-    line_start(dir, li, k.W, k.H, x, y, sx, sy);
+    int x0, y0, sx, sy;
+    line_start(dir, li, k.W, k.H, x0, y0, sx, sy);
+    const int len = line_length(x0, y0, sx, sy, k.W, k.H);
     LaneMasks<KW> mk;
     make_lane_masks<KW>(lane, k.D, mk);
     const size_t Dp = (size_t)k.Dp;
     const int off = lane * 2 * KW;
+    const long long pstep = (long long)sy * k.W + sx;  // pixel index step along the line
+    const long long p0 = (long long)y0 * k.W + x0;
 
-    uint32_t Lp[KW], Cw[KW], Ln[KW];
-    size_t p = (size_t)y * k.W + x;
-    load_cost_words<KW>(pv.cost + p * Dp + off, Cw);
+    uint32_t cb[PF][KW], ab[PF][KW];
+    int ib[PF];
 #pragma unroll
-    for (int i = 0; i < KW; ++i) Lp[i] = scale_cost<WRAP>(Cw[i], k.costScale) | mk.padMask[i];
-    {
-        uint16_t* ap = pv.agg + p * Dp + off;
-        if (first) {
-            store_words<KW>(ap, Lp);
-        } else {
-            uint32_t a[KW];
-            load_words<KW>(ap, a);
-#pragma unroll
-            for (int i = 0; i < KW; ++i) a[i] = WRAP ? __vadd2(a[i], Lp[i]) : a[i] + Lp[i];
-            store_words<KW>(ap, a);
+    for (int j = 0; j < PF; ++j) {
+        if (j < len) {
+            const size_t p = (size_t)(p0 + j * pstep);
+            load_cost_words<KW>(pv.cost + p * Dp + off, cb[j]);
+            if (!first) load_words<KW>(pv.agg + p * Dp + off, ab[j]);
+            ib[j] = pv.img[p];
         }
     }
-    uint32_t minPrev = warp_min_u16<KW>(Lp);
-    int prevI = pv.img[p];
-    for (x += sx, y += sy; x >= 0 && x < k.W && y >= 0 && y < k.H; x += sx, y += sy) {
-        p = (size_t)y * k.W + x;
-        const int curI = pv.img[p];
-        const int p2 = p2lut[abs(curI - prevI)];
-        prevI = curI;
-        load_cost_words<KW>(pv.cost + p * Dp + off, Cw);
+    uint32_t Lp[KW], Ln[KW], Cw[KW];
+    uint32_t minPrev = 0;
+    int prevI = 0;
+    for (int base = 0; base < len; base += PF) {
 #pragma unroll
-        for (int i = 0; i < KW; ++i) Cw[i] = scale_cost<WRAP>(Cw[i], k.costScale);
-        sgm_step<KW, WRAP, FULL>(Lp, Cw, minPrev, p2, k.p1x2, k.bsub, mk, Ln);
-        uint16_t* ap = pv.agg + p * Dp + off;
-        if (first) {
-            store_words<KW>(ap, Ln);
-        } else {
-            uint32_t a[KW];
-            load_words<KW>(ap, a);
+        for (int j = 0; j < PF; ++j) {
+            const int i = base + j;
+            if (i >= len) break;
+            const size_t p = (size_t)(p0 + (long long)i * pstep);
 #pragma unroll
-            for (int i = 0; i < KW; ++i) a[i] = WRAP ? __vadd2(a[i], Ln[i]) : a[i] + Ln[i];
-            store_words<KW>(ap, a);
+            for (int w = 0; w < KW; ++w) Cw[w] = scale_cost<WRAP>(cb[j][w], k.costScale);
+            const int curI = ib[j];
+            if (i == 0) {
+#pragma unroll
+                for (int w = 0; w < KW; ++w) Ln[w] = Cw[w] | mk.padMask[w];
+            } else {
+                const int p2 = p2lut[abs(curI - prevI)];
+                sgm_step<KW, WRAP, FULL>(Lp, Cw, minPrev, p2, k.p1x2, k.bsub, mk, Ln);
+            }
+            prevI = curI;
+            uint16_t* ap = pv.agg + p * Dp + off;
+            if (first) {
+                store_words<KW>(ap, Ln);
+            } else {
+                uint32_t a[KW];
+#pragma unroll
+                for (int w = 0; w < KW; ++w) a[w] = WRAP ? __vadd2(ab[j][w], Ln[w]) : ab[j][w] + Ln[w];
+                store_words<KW>(ap, a);
+            }
+            // prefetch pixel i + PF into this slot
+            if (i + PF < len) {
+                const size_t q = (size_t)(p0 + (long long)(i + PF) * pstep);
+                load_cost_words<KW>(pv.cost + q * Dp + off, cb[j]);
+                if (!first) load_words<KW>(pv.agg + q * Dp + off, ab[j]);
+                ib[j] = pv.img[q];
+            }
+#pragma unroll
+            for (int w = 0; w < KW; ++w) Lp[w] = Ln[w];
+            minPrev = warp_min_u16<KW>(Lp);
         }
-#pragma unroll
-        for (int i = 0; i < KW; ++i) Lp[i] = Ln[i];
-        minPrev = warp_min_u16<KW>(Lp);
     }
 }
 
@@ -102,7 +128,8 @@ static cudaError_t launch_dir_t(const PairView& pv, const SgmConsts& k, int dir,
     const int lines = num_lines(dir, k.W, k.H);
     const int warpsPerBlock = 4;
     const int grid = (lines + warpsPerBlock - 1) / warpsPerBlock;
-    agg_dir_kernel<KW, WRAP, FULL><<<grid, 32 * warpsPerBlock, 0, s>>>(pv, k, dir, first);
+    constexpr int PF = KW <= 4 ? 4 : 2;
+    agg_dir_kernel<KW, WRAP, FULL, PF><<<grid, 32 * warpsPerBlock, 0, s>>>(pv, k, dir, first);
     return cudaGetLastError();
 }
 

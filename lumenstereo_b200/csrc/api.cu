@@ -415,7 +415,7 @@ extern "C" lumen_status lumen_sgbm_compute_device(lumen_sgbm* h, const uint8_t* 
     if (!out_stride) out_stride = (size_t)width * 2;
     if (out_stride < (size_t)width * 2 || out_stride % 2)
         return fail(LUMEN_ERR_INVALID_ARGUMENT, "out_stride must be an even byte count >= 2*width");
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : h->stream;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the default stream
     LCU(cudaEventRecord(h->ev[0], s));
     st = run_pipeline(h, d_left, d_right, in_stride, channels, width, height, d_out,
                       out_stride / 2, s, true);
@@ -511,7 +511,7 @@ extern "C" lumen_status lumen_rectifier_rectify_device(lumen_rectifier* r, const
                                                        uint8_t* ol, uint8_t* orr, void* stream) {
     if (!r || !dl || !dr || !ol || !orr) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL argument");
     if (channels < 1) return fail(LUMEN_ERR_INVALID_ARGUMENT, "channels must be >= 1");
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : r->stream;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);  // NULL: the default stream
     const size_t n = (size_t)r->W * r->H * channels;
     if (r->pre) {
         LCU(cudaMemcpyAsync(ol, dl, n, cudaMemcpyDeviceToDevice, s));

@@ -39,7 +39,7 @@ struct LaneMasks {
     uint32_t padMask[KW];     // halves of word i with d >= D
 };
 
-// Per-lane masks for a warp whose lane `lane` holds d = 2*KW*lane + (0..2KW-1).
+// Per-lane masks for a team lane `lane` holding d = 2*KW*lane + (0..2KW-1).
 template <int KW>
 __device__ __forceinline__ void make_lane_masks(int lane, int D, LaneMasks<KW>& m) {
     const int base = 2 * KW * lane;
@@ -48,8 +48,8 @@ __device__ __forceinline__ void make_lane_masks(int lane, int D, LaneMasks<KW>& 
         // nb[j] = (L'[base+2j-1], L'[base+2j])
         uint32_t mk = 0;
         if (base + 2 * j - 1 == -1) mk |= 0x0000FFFFu;         // left of d = 0
-        if (base + 2 * j - 1 == D) mk |= 0x0000FFFFu;          // right of d = D-1 (odd D-1... )
-        if (base + 2 * j == D) mk |= 0xFFFF0000u;              // right of d = D-1
+        if (base + 2 * j - 1 == D) mk |= 0x0000FFFFu;          // right of d = D-1 (D-1 even)
+        if (base + 2 * j == D) mk |= 0xFFFF0000u;              // right of d = D-1 (D-1 odd)
         m.nbMask[j] = mk;
     }
 #pragma unroll
@@ -70,32 +70,41 @@ __device__ __forceinline__ uint32_t scale_cost(uint32_t pk, int costScale) {
     return lo | hi;
 }
 
-// min over the lane's words and both halves, then across the warp.
-template <int KW>
+// min over the lane's words and both halves, then across the team of T lanes
+// (T = 32: one redux.sync; T < 32: xor butterfly inside the T-lane segment).
+template <int KW, int T = 32>
 __device__ __forceinline__ uint32_t warp_min_u16(const uint32_t (&L)[KW]) {
     uint32_t m = L[0];
 #pragma unroll
     for (int i = 1; i < KW; ++i) m = __vminu2(m, L[i]);
     m = min(m & 0xFFFFu, m >> 16);
-    return __reduce_min_sync(kFull, m);
+    if constexpr (T == 32) {
+        return __reduce_min_sync(kFull, m);
+    } else {
+#pragma unroll
+        for (int o = T / 2; o > 0; o >>= 1) m = min(m, __shfl_xor_sync(kFull, m, o));
+        return m;
+    }
 }
 
 // One recurrence step.  Lp: previous path costs; Cw: scaled matching costs of
 // the current pixel; minPrev: min over d of Lp; p2: P2adj of this step;
 // bsub: (0xFFFF - P1) in both halves (mod 2^16); p1x2: P1 in both halves.
-template <int KW, bool WRAP, bool FULL>
+// T: lanes per pixel (the team); lanes of a team are a contiguous, aligned
+// segment of the warp and every lane of the warp executes the step.
+template <int KW, bool WRAP, bool FULL, int T = 32>
 __device__ __forceinline__ void sgm_step(const uint32_t (&Lp)[KW], const uint32_t (&Cw)[KW],
                                          uint32_t minPrev, int p2, uint32_t p1x2, uint32_t bsub,
                                          const LaneMasks<KW>& mk, uint32_t (&Ln)[KW]) {
-    const uint32_t up = __shfl_up_sync(kFull, Lp[KW - 1], 1);
-    const uint32_t dn = __shfl_down_sync(kFull, Lp[0], 1);
+    const uint32_t up = __shfl_up_sync(kFull, Lp[KW - 1], 1, T);
+    const uint32_t dn = __shfl_down_sync(kFull, Lp[0], 1, T);
     uint32_t nb[KW + 1];
     nb[0] = __byte_perm(up, Lp[0], 0x5432);
 #pragma unroll
     for (int j = 1; j < KW; ++j) nb[j] = __byte_perm(Lp[j - 1], Lp[j], 0x5432);
     nb[KW] = __byte_perm(Lp[KW - 1], dn, 0x5432);
     if (FULL) {
-        // Only L'[-1] (lane 0, nb[0] low) and L'[D] (lane 31, nb[KW] high) occur.
+        // Only L'[-1] (team lane 0, nb[0] low) and L'[D] (last team lane, nb[KW] high) occur.
         nb[0] = (nb[0] & ~mk.nbMask[0]) | (bsub & mk.nbMask[0]);
         nb[KW] = (nb[KW] & ~mk.nbMask[KW]) | (bsub & mk.nbMask[KW]);
     } else {

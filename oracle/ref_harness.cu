@@ -37,8 +37,8 @@ __global__ void speckleFilter(int16_t*, int, int, int, int);
 __global__ void remapKernelSimple(const unsigned char*, const float*, const float*, unsigned char*, int, int, int);
 }  // namespace stereo
 
-namespace {
-
+// Field order of oracle_params / lumen_stereo_params; external linkage so the
+// extern "C" entry points below are exported.
 struct RefParams {  // field order of oracle_params / lumen_stereo_params
     int minDisparity, maxDisparity, blockSize, P1, P2, preFilterCap, uniquenessRatio,
         disp12MaxDiff, speckleWindowSize, speckleRange, useGPU, useSharedMemory, numDirections,
@@ -56,6 +56,8 @@ struct RefDump {  // host pointers, any may be null
     int16_t* disp_right;
     int16_t* disp_lr;
 };
+
+namespace {
 
 inline int divUp(int a, int b) { return (a + b - 1) / b; }
 
