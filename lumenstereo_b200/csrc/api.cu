@@ -72,6 +72,10 @@ struct lumen_sgbm {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     DevBuf inL, inR, gray[2], pref[2], census[2], cost, agg, dispL, dispR, out, dbgLR, magic;
+    DevBuf partB, xring, counters, status;  // sweep schedule: backward partial, exchange rings
+    int numSMs = 148;
+    long long spinMax = 1ll << 22;          // bounded device-side waits
+    bool statusPending = false;
     int magicR = -1;
     float timings[4] = {0, 0, 0, 0};
     unsigned pathOverride = 0;
@@ -144,7 +148,10 @@ extern "C" lumen_status lumen_sgbm_create(const lumen_stereo_params* params, lum
     if (params) h->params = *params;
     else lumen_stereo_params_default(&h->params);
     cudaGetDevice(&h->device);
+    cudaDeviceGetAttribute(&h->numSMs, cudaDevAttrMultiProcessorCount, h->device);
     cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = h->status.ensure(sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(h->status.p, 0, sizeof(int));
     for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaEventCreate(&h->ev[i]);
     if (e != cudaSuccess) {
         lumen_sgbm_destroy(h);
@@ -159,7 +166,8 @@ extern "C" lumen_status lumen_sgbm_destroy(lumen_sgbm* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (DevBuf* b : {&h->inL, &h->inR, &h->gray[0], &h->gray[1], &h->pref[0], &h->pref[1],
                       &h->census[0], &h->census[1], &h->cost, &h->agg, &h->dispL, &h->dispR,
-                      &h->out, &h->dbgLR, &h->magic})
+                      &h->out, &h->dbgLR, &h->magic, &h->partB, &h->xring, &h->counters,
+                      &h->status})
         b->release();
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
@@ -180,8 +188,26 @@ extern "C" lumen_status lumen_sgbm_get_params(const lumen_sgbm* h, lumen_stereo_
     return LUMEN_OK;
 }
 
+// Device-side waits report through a status word; read it once the work is done.
+static lumen_status check_status(lumen_sgbm* h) {
+    if (!h->statusPending) return LUMEN_OK;
+    int st = 0;
+    LCU(cudaMemcpy(&st, h->status.p, sizeof(int), cudaMemcpyDeviceToHost));
+    h->statusPending = false;
+    if (st != 0) {
+        cudaMemset(h->status.p, 0, sizeof(int));
+        return fail(static_cast<lumen_status>(st),
+                    "a bounded device-side wait timed out in the aggregation sweep");
+    }
+    return LUMEN_OK;
+}
+
 static lumen_status read_timings(lumen_sgbm* h) {
     LCU(cudaEventSynchronize(h->ev[4]));
+    {
+        lumen_status st = check_status(h);
+        if (st != LUMEN_OK) return st;
+    }
     float t = 0;
     LCU(cudaEventElapsedTime(&t, h->ev[0], h->ev[4]));
     h->timings[0] = t;
@@ -353,12 +379,37 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
     k.bsub = ((uint32_t)(0xFFFF - p.P1) & 0xFFFFu) * 0x10001u;
     const bool wrap = !no_wrap(p, k.costScale, __builtin_popcount(mask));
     PairView pv{h->cost.as<uint8_t>(), gl, h->agg.as<uint16_t>()};
-    LCU(launch_aggregate_per_direction(pv, k, mask, wrap, s));
-    nl += __builtin_popcount(mask);
+    const bool sweepable = (mask == 0xFFu || mask == 0x0Fu);
+    int sched = h->schedule ? h->schedule : (sweepable ? 2 : 1);
+    if (sched == 2 && !sweepable) sched = 1;  // single-path debug masks: per-direction kernels
+    if (sched == 2 && !sweep_fits(W, Dp)) sched = 1;  // very wide images: per-direction kernels
+    const uint16_t* aggB = nullptr;
+    if (sched == 2) {
+        const int R = sweep_rows_per_band(Dp);
+        const int nBands = (H + R - 1) / R;
+        LCU(h->partB.ensure(ND * 2));
+        LCU(h->xring.ensure(sweep_ring_bytes(W, Dp, nBands)));
+        LCU(h->counters.ensure(sizeof(unsigned) * 4 * (size_t)nBands));
+        LCU(launch_aggregate_sweep(pv, h->partB.as<uint16_t>(), k, wrap, mask == 0xFFu,
+                                   h->xring.as<uint8_t>(), h->counters.as<unsigned>(),
+                                   h->status.as<int>(), h->spinMax, s, h->numSMs));
+        h->statusPending = true;
+        nl += 1;  // the sweep kernel (the counter reset is a memset, not a kernel)
+        aggB = h->partB.as<uint16_t>();
+        if (h->retain || select_needs_summed_volume(D, Dp)) {
+            launch_sum_volumes(h->agg.as<uint16_t>(), aggB, h->agg.as<uint16_t>(), ND, s);
+            LCU(cudaGetLastError());
+            nl += 1;
+            aggB = nullptr;
+        }
+    } else {
+        LCU(launch_aggregate_per_direction(pv, k, mask, wrap, s));
+        nl += __builtin_popcount(mask);
+    }
     if (timed) LCU(cudaEventRecord(h->ev[3], s));
     // selection + post-processing
-    LCU(launch_select(h->agg.as<uint16_t>(), W, H, D, Dp, p.minDisparity, p.uniquenessRatio,
-                      h->dispL.as<int16_t>(), h->dispR.as<int16_t>(), s));
+    LCU(launch_select(h->agg.as<uint16_t>(), aggB, wrap, W, H, D, Dp, p.minDisparity,
+                      p.uniquenessRatio, h->dispL.as<int16_t>(), h->dispR.as<int16_t>(), s));
     const int lr = p.disp12MaxDiff >= 0 ? p.disp12MaxDiff * 16 : -1;
     const int spk = p.speckleWindowSize > 0 ? std::min(p.speckleWindowSize, 25) : 0;
     LCU(launch_post(h->dispL.as<int16_t>(), h->dispR.as<int16_t>(), W, H, lr, spk,
@@ -399,7 +450,7 @@ extern "C" lumen_status lumen_sgbm_compute(lumen_sgbm* h, const uint8_t* left,
     LCU(cudaMemcpy2DAsync(out, out_stride, h->out.p, (size_t)width * 2, (size_t)width * 2, height,
                           cudaMemcpyDeviceToHost, s));
     LCU(cudaStreamSynchronize(s));
-    return read_timings(h);
+    return read_timings(h);  // also reports a device-side timeout
 }
 
 extern "C" lumen_status lumen_sgbm_compute_device(lumen_sgbm* h, const uint8_t* d_left,

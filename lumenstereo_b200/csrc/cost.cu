@@ -109,12 +109,15 @@ census_cost_kernel(const uint32_t* __restrict__ cl, const uint32_t* __restrict__
     }
     __syncthreads();
     const int chunks = Dp / 16;
-    const int items = kCensusTile * chunks;
     const bool rowOk = (y >= 2 && y < H - 2);
-    for (int it = threadIdx.x; it < items; it += blockDim.x) {
-        const int px = it / chunks, ch = it - px * chunks;
+    // thread -> one 16-disparity chunk, striding over the tile's pixels
+    const int ch = threadIdx.x % chunks;
+    const int pxStep = blockDim.x / chunks;
+    const int px0 = threadIdx.x / chunks;
+    if (px0 >= pxStep) return;  // no barrier below
+    for (int px = px0; px < kCensusTile; px += pxStep) {
         const int x = x0 + px;
-        if (x >= W) continue;
+        if (x >= W) break;
         const bool leftOk = rowOk && x >= 2 && x < W - 2;
         const int dlo = ch * 16;
         const int rxHi = x - minD - dlo, rxLo = rxHi - 15;  // right columns of this chunk
@@ -156,153 +159,225 @@ census_cost_kernel(const uint32_t* __restrict__ cl, const uint32_t* __restrict__
 }
 
 // ---------------------------------------------------------------------------
-// SAD cost (src/sgbm_kernels.cu:70-212).  One CTA per (row y, 64-pixel tile).
-// Shared memory holds the prefiltered rows y-r..y+r of both images (right rows
-// reversed, so that four consecutive disparities of one column are four
-// consecutive bytes), then the column sums
-//   cs[x'][d] = sum over valid rows of |Lf(x',row) - Rf(x'-ad,row)|
-// (0 for a column whose left or right pixel lies outside the image), four
-// disparities per __vabsdiffu4.  The window sum adds 2r+1 column sums; the
-// count is (#valid rows) x (#valid columns) and sum/count is
-// umulhi(sum, ceil(2^32/count)), exact because sum*count < 2^32 here.
-// `wide` selects 32-bit window sums when (2r+1)^2 * 2*cap can exceed 65535.
+// SAD cost (src/sgbm_kernels.cu:70-212).
+//
+// One CTA per (64-pixel column tile, band of kSadBand rows), sliding down the
+// band.  Shared memory keeps, per column x' of the tile plus an r-pixel apron
+// and per 4-disparity quad, the column sums
+//   cs[x'][d] = sum over the window's valid rows of A(x', row, d),
+//   A = |Lf(x',row) - Rf(x'-ad,row)| (0 when x' or x'-ad is outside the image),
+// four disparities per __vabsdiffu4, stored as two uint16x2 words holding
+// (d0,d2) and (d1,d3).  Moving one row down adds the entering row and
+// subtracts the leaving one (rows are kept in a small ring), so every A value
+// is computed twice instead of 2r+1 times.  Window sums then slide along x
+// (add the entering column, subtract the leaving one).  The count is
+// (#valid rows) x (#valid columns) and sum/count = umulhi(sum, ceil(2^32/count)),
+// exact for every reachable sum.  WIDE keeps 32-bit window sums when
+// (2r+1)^2 * 2*cap can exceed 65535.
 // ---------------------------------------------------------------------------
-constexpr int kSadTile = 64;
+constexpr int kSadTile = 64;   // output columns per CTA
+constexpr int kSadBand = 32;   // output rows per CTA
+constexpr int kSadRun = 8;     // consecutive output pixels per thread (window sliding)
+
+struct SadGeom {
+    int nrow;   // 2r+1
+    int ncol;   // kSadTile + 2r
+    int ncolp;  // ncol rounded up to 4
+    int rw;     // reversed right-row span (bytes), multiple of 4
+    int ring;   // rows kept: 2r+2
+};
+
+__host__ __device__ inline SadGeom sad_geom(int Dp, int r) {
+    SadGeom g;
+    g.nrow = 2 * r + 1;
+    g.ncol = kSadTile + 2 * r;
+    g.ncolp = (g.ncol + 3) & ~3;
+    g.rw = (g.ncol + Dp - 1 + 3 + 4) & ~3;
+    g.ring = 2 * r + 2;
+    return g;
+}
 
 __device__ __forceinline__ uint32_t load_u32_unaligned(const uint8_t* base, int i) {
     const uint32_t* w = reinterpret_cast<const uint32_t*>(base + (i & ~3));
     return __byte_perm(w[0], w[1], (uint32_t)(0x3210 + 0x1111 * (i & 3)));
 }
 
+// abs differences of one row for column c and the quad d0..d0+3, split as
+// (d0,d2) / (d1,d3) uint16x2 words.
+__device__ __forceinline__ void sad_row_quad(const uint8_t* sLrow, const uint8_t* sRrow, int c,
+                                             int j0, uint32_t mask, uint32_t& ev, uint32_t& od) {
+    const uint32_t l4 = __byte_perm((uint32_t)sLrow[c], 0u, 0x0000);
+    const uint32_t r4 = load_u32_unaligned(sRrow, j0);
+    const uint32_t v = __vabsdiffu4(l4, r4) & mask;
+    ev = v & 0x00FF00FFu;
+    od = (v >> 8) & 0x00FF00FFu;
+}
+
+template <bool WIDE>
 __global__ void __launch_bounds__(256)
 sad_cost_kernel(const uint8_t* __restrict__ pl, const uint8_t* __restrict__ pr, int W, int H,
-                int D, int Dp, int minD, int r, const uint32_t* __restrict__ magic, int wide,
+                int D, int Dp, int minD, int r, const uint32_t* __restrict__ magic,
                 uint8_t* __restrict__ cost) {
     extern __shared__ __align__(16) uint8_t sm[];
-    const int y = blockIdx.y;
+    const SadGeom g = sad_geom(Dp, r);
     const int x0 = blockIdx.x * kSadTile;
-    const int nrow = 2 * r + 1;
-    const int ncol = kSadTile + 2 * r;             // columns x' of the column sums
-    const int lx0 = x0 - r;                        // first column x'
-    // Right row span, stored reversed: index j holds Rf(rtop - j).
-    const int rtop = lx0 + ncol - 1 - minD;        // rightmost right column reached
-    const int rw = (ncol + Dp - 1 + 3 + 4) & ~3;   // padded span (+4 slack for unaligned reads)
-    uint8_t* sL = sm;                              // [nrow][ncolp]
-    const int ncolp = (ncol + 3) & ~3;
-    uint8_t* sR = sL + nrow * ncolp;               // [nrow][rw]
-    uint32_t* cs = reinterpret_cast<uint32_t*>(
-        sm + ((nrow * (ncolp + rw) + 15) & ~15));  // [ncol][Dp/2] packed pairs
-    const int ylo = max(0, y - r), yhi = min(H - 1, y + r);
-    const int cy = yhi - ylo + 1;
-    for (int i = threadIdx.x; i < nrow * ncolp; i += blockDim.x) {
-        const int rr = i / ncolp, c = i - rr * ncolp;
-        const int gy = y - r + rr, gx = lx0 + c;
-        sL[i] = (gy >= 0 && gy < H && gx >= 0 && gx < W && c < ncol) ? pl[(size_t)gy * W + gx] : 0;
-    }
-    for (int i = threadIdx.x; i < nrow * rw; i += blockDim.x) {
-        const int rr = i / rw, j = i - rr * rw;
-        const int gy = y - r + rr, gx = rtop - j;
-        sR[i] = (gy >= 0 && gy < H && gx >= 0 && gx < W) ? pr[(size_t)gy * W + gx] : 0;
-    }
-    __syncthreads();
-    // Column sums: 4 disparities per item.
+    const int yb = blockIdx.y * kSadBand;
+    const int yEnd = min(H, yb + kSadBand);
+    const int lx0 = x0 - r;                        // column of cs index 0
+    const int rtop = lx0 + g.ncol - 1 - minD;      // right column at reversed index 0
     const int quads = Dp / 4;
-    for (int it = threadIdx.x; it < ncol * quads; it += blockDim.x) {
-        const int c = it / quads, q = it - c * quads;
+    uint8_t* sL = sm;                              // [ring][ncolp]
+    uint8_t* sR = sL + g.ring * g.ncolp;           // [ring][rw]
+    uint2* cs = reinterpret_cast<uint2*>(sm + ((g.ring * (g.ncolp + g.rw) + 15) & ~15));  // [ncol][quads]
+
+    auto load_row = [&](int gy) {  // row gy into ring slot gy % ring
+        const int slot = gy % g.ring;
+        for (int i = threadIdx.x; i < g.ncolp; i += blockDim.x) {
+            const int gx = lx0 + i;
+            sL[slot * g.ncolp + i] = (gx >= 0 && gx < W && i < g.ncol) ? pl[(size_t)gy * W + gx] : 0;
+        }
+        for (int j = threadIdx.x; j < g.rw; j += blockDim.x) {
+            const int gx = rtop - j;
+            sR[slot * g.rw + j] = (gx >= 0 && gx < W) ? pr[(size_t)gy * W + gx] : 0;
+        }
+    };
+    // validity mask of (column c, quad q): bytes whose column and right pixel are in the image
+    auto quad_mask = [&](int c, int q) -> uint32_t {
         const int xg = lx0 + c;
+        if (xg < 0 || xg >= W) return 0u;
         const int d0 = 4 * q;
-        // byte b of the quad is disparity d0+b: right column xg - minD - d0 - b,
-        // reversed index j = rtop - (xg - minD - d0 - b) = j0 + b.
-        const int j0 = rtop - (xg - minD - d0);
-        uint32_t mask = 0;
+        const int rx0 = xg - minD - d0;  // right column of byte 0; byte b: rx0 - b
+        if (rx0 - 3 >= 0 && rx0 < W && d0 + 4 <= D) return 0xFFFFFFFFu;
+        uint32_t m = 0;
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int rx = xg - minD - d0 - b;
-            if (xg >= 0 && xg < W && rx >= 0 && rx < W && d0 + b < D) mask |= 0xFFu << (8 * b);
-        }
-        uint32_t ev = 0, od = 0;  // (d0, d0+2) and (d0+1, d0+3) as u16 pairs
-        if (mask) {
-            for (int gy = ylo; gy <= yhi; ++gy) {
-                const int rr = gy - (y - r);
-                const uint32_t l4 = (uint32_t)sL[rr * ncolp + c] * 0x01010101u;
-                const uint32_t r4 = load_u32_unaligned(sR + rr * rw, j0);
-                const uint32_t v = __vabsdiffu4(l4, r4) & mask;
-                ev += v & 0x00FF00FFu;
-                od += (v >> 8) & 0x00FF00FFu;
-            }
-        }
-        cs[c * (Dp / 2) + 2 * q] = __byte_perm(ev, od, 0x5410);
-        cs[c * (Dp / 2) + 2 * q + 1] = __byte_perm(ev, od, 0x7632);
-    }
+        for (int b = 0; b < 4; ++b)
+            if (rx0 - b >= 0 && rx0 - b < W && d0 + b < D) m |= 0xFFu << (8 * b);
+        return m;
+    };
+
+    // initial window rows of the first output row
+    for (int gy = max(0, yb - r); gy <= min(H - 1, yb + r); ++gy) load_row(gy);
     __syncthreads();
-    // Window sums, 16 disparities per item (one 16-byte store).
-    const int chunks = Dp / 16;
-    for (int it = threadIdx.x; it < kSadTile * chunks; it += blockDim.x) {
-        const int px = it / chunks, ch = it - px * chunks;
-        const int x = x0 + px;
-        if (x >= W) continue;
-        uint32_t s[16];
-        if (!wide) {
-            uint32_t sums[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) sums[k] = 0;
-            for (int dx = -r; dx <= r; ++dx) {
-                const uint4* src = reinterpret_cast<const uint4*>(cs + (size_t)(px + r + dx) * (Dp / 2) + ch * 8);
-                const uint4 a = src[0], b = src[1];
-                sums[0] += a.x; sums[1] += a.y; sums[2] += a.z; sums[3] += a.w;
-                sums[4] += b.x; sums[5] += b.y; sums[6] += b.z; sums[7] += b.w;
-            }
-#pragma unroll
-            for (int k = 0; k < 8; ++k) { s[2 * k] = sums[k] & 0xFFFFu; s[2 * k + 1] = sums[k] >> 16; }
-        } else {
-#pragma unroll
-            for (int k = 0; k < 16; ++k) s[k] = 0;
-            for (int dx = -r; dx <= r; ++dx) {
-                const uint32_t* src = cs + (size_t)(px + r + dx) * (Dp / 2) + ch * 8;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) { s[2 * k] += src[k] & 0xFFFFu; s[2 * k + 1] += src[k] >> 16; }
-            }
-        }
-        const int dlo = ch * 16;
-        uint32_t outw[4];
-        const int full = (2 * r + 1) * cy;
-        const bool interior = (x - r >= 0) && (x + r <= W - 1) && (x - r - minD - (dlo + 15) >= 0) &&
-                              (x + r - minD - dlo <= W - 1) && (dlo + 16 <= D);
-        if (interior) {
-            const uint32_t m = magic[full];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                uint32_t packed = 0;
-#pragma unroll
-                for (int b = 0; b < 4; ++b)
-                    packed |= (full == 1 ? s[4 * q + b] : __umulhi(s[4 * q + b], m)) << (8 * b);
-                outw[q] = packed;
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                uint32_t packed = 0;
-#pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    const int d = dlo + 4 * q + b;
-                    uint32_t v;
-                    if (d >= D) {
-                        v = 0;
-                    } else {
-                        // valid columns: x+dx in [0,W) and x+dx-ad in [0,W)
-                        const int ad = minD + d;
-                        const int clo = max(max(-r, -x), ad - x);
-                        const int chi = min(min(r, W - 1 - x), W - 1 - x + ad);
-                        const int cnt = cy * max(0, chi - clo + 1);
-                        v = cnt > 0 ? (cnt == 1 ? s[4 * q + b] : __umulhi(s[4 * q + b], magic[cnt])) : 255u;
-                    }
-                    packed |= v << (8 * b);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int c = warp; c < g.ncol; c += nw) {
+        for (int q = lane; q < quads; q += 32) {
+            const uint32_t mask = quad_mask(c, q);
+            const int j0 = rtop - (lx0 + c - minD - 4 * q);
+            uint32_t ev = 0, od = 0;
+            if (mask)
+                for (int gy = max(0, yb - r); gy <= min(H - 1, yb + r); ++gy) {
+                    uint32_t e, o;
+                    const int slot = gy % g.ring;
+                    sad_row_quad(sL + slot * g.ncolp, sR + slot * g.rw, c, j0, mask, e, o);
+                    ev += e;
+                    od += o;
                 }
-                outw[q] = packed;
+            cs[c * quads + q] = make_uint2(ev, od);
+        }
+    }
+    for (int y = yb; y < yEnd; ++y) {
+        if (y > yb) {
+            // slide: add row y+r, remove row y-r-1
+            const int yin = y + r, yout = y - r - 1;
+            if (yin < H) load_row(yin);
+            __syncthreads();
+            for (int c = warp; c < g.ncol; c += nw) {
+                for (int q = lane; q < quads; q += 32) {
+                    const uint32_t mask = quad_mask(c, q);
+                    if (!mask) continue;
+                    const int j0 = rtop - (lx0 + c - minD - 4 * q);
+                    uint2 v = cs[c * quads + q];
+                    uint32_t e, o;
+                    if (yin < H) {
+                        const int slot = yin % g.ring;
+                        sad_row_quad(sL + slot * g.ncolp, sR + slot * g.rw, c, j0, mask, e, o);
+                        v.x += e;
+                        v.y += o;
+                    }
+                    if (yout >= 0) {
+                        const int slot = yout % g.ring;
+                        sad_row_quad(sL + slot * g.ncolp, sR + slot * g.rw, c, j0, mask, e, o);
+                        v.x -= e;
+                        v.y -= o;
+                    }
+                    cs[c * quads + q] = v;
+                }
             }
         }
-        *reinterpret_cast<uint4*>(cost + ((size_t)y * W + x) * Dp + dlo) =
-            make_uint4(outw[0], outw[1], outw[2], outw[3]);
+        __syncthreads();
+        // window sums: thread -> (quad, run of kSadRun pixels)
+        const int cy = min(H - 1, y + r) - max(0, y - r) + 1;
+        const int full = cy * (2 * r + 1);
+        const uint32_t mfull = magic[full];
+        const int runs = kSadTile / kSadRun;
+        for (int item = threadIdx.x; item < quads * runs; item += blockDim.x) {
+            const int q = item % quads, run = item / quads;  // quads is 16..128: shifts when a power of 2
+            const int px0 = run * kSadRun;
+            const int d0 = 4 * q;
+            uint32_t s0, s1, s2, s3;  // window sums of d0..d0+3 (WIDE) or packed pairs
+            uint32_t pe = 0, po = 0;
+            uint32_t w0 = 0, w1 = 0, w2 = 0, w3 = 0;
+            // columns of pixel px: cs index px .. px + 2r
+            for (int k = 0; k < 2 * r + 1; ++k) {
+                const uint2 v = cs[(px0 + k) * quads + q];
+                if (WIDE) {
+                    w0 += v.x & 0xFFFFu; w2 += v.x >> 16; w1 += v.y & 0xFFFFu; w3 += v.y >> 16;
+                } else {
+                    pe += v.x;
+                    po += v.y;
+                }
+            }
+            for (int t = 0; t < kSadRun; ++t) {
+                const int px = px0 + t;
+                const int x = x0 + px;
+                if (t > 0) {
+                    const uint2 vin = cs[(px + 2 * r) * quads + q];
+                    const uint2 vout = cs[(px - 1) * quads + q];
+                    if (WIDE) {
+                        w0 += (vin.x & 0xFFFFu) - (vout.x & 0xFFFFu);
+                        w2 += (vin.x >> 16) - (vout.x >> 16);
+                        w1 += (vin.y & 0xFFFFu) - (vout.y & 0xFFFFu);
+                        w3 += (vin.y >> 16) - (vout.y >> 16);
+                    } else {
+                        pe += vin.x - vout.x;
+                        po += vin.y - vout.y;
+                    }
+                }
+                if (x >= W) break;
+                if (WIDE) { s0 = w0; s1 = w1; s2 = w2; s3 = w3; }
+                else { s0 = pe & 0xFFFFu; s2 = pe >> 16; s1 = po & 0xFFFFu; s3 = po >> 16; }
+                uint32_t outw;
+                const bool interior = (x - r >= 0) && (x + r <= W - 1) && (x - r - minD - d0 - 3 >= 0) &&
+                                      (d0 + 4 <= D);
+                if (interior) {
+                    const uint32_t q0 = full == 1 ? s0 : __umulhi(s0, mfull);
+                    const uint32_t q1 = full == 1 ? s1 : __umulhi(s1, mfull);
+                    const uint32_t q2 = full == 1 ? s2 : __umulhi(s2, mfull);
+                    const uint32_t q3 = full == 1 ? s3 : __umulhi(s3, mfull);
+                    outw = q0 | (q1 << 8) | (q2 << 16) | (q3 << 24);
+                } else {
+                    const uint32_t sv[4] = {s0, s1, s2, s3};
+                    outw = 0;
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const int d = d0 + b;
+                        uint32_t v;
+                        if (d >= D) {
+                            v = 0;
+                        } else {
+                            const int ad = minD + d;
+                            const int clo = max(max(-r, -x), ad - x);
+                            const int chi = min(min(r, W - 1 - x), W - 1 - x + ad);
+                            const int cnt = cy * max(0, chi - clo + 1);
+                            v = cnt > 0 ? (cnt == 1 ? sv[b] : __umulhi(sv[b], magic[cnt])) : 255u;
+                        }
+                        outw |= v << (8 * b);
+                    }
+                }
+                *reinterpret_cast<uint32_t*>(cost + ((size_t)y * W + x) * Dp + d0) = outw;
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -341,20 +416,19 @@ cudaError_t launch_census_cost(const uint32_t* cl, const uint32_t* cr, int W, in
 }
 
 size_t sad_cost_smem(int Dp, int r) {
-    const int nrow = 2 * r + 1, ncol = kSadTile + 2 * r;
-    const int ncolp = (ncol + 3) & ~3, rw = (ncol + Dp - 1 + 3 + 4) & ~3;
-    return (size_t)((nrow * (ncolp + rw) + 15) & ~15) + (size_t)ncol * Dp * 2;
+    const SadGeom g = sad_geom(Dp, r);
+    return (size_t)((g.ring * (g.ncolp + g.rw) + 15) & ~15) + (size_t)g.ncol * (Dp / 4) * 8;
 }
 
 cudaError_t launch_sad_cost(const uint8_t* pl, const uint8_t* pr, int W, int H, int D, int Dp,
                             int minD, int r, const uint32_t* magic, int wide, uint8_t* cost,
                             cudaStream_t s) {
     const size_t smem = sad_cost_smem(Dp, r);
-    cudaError_t e = cudaFuncSetAttribute(sad_cost_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    auto kern = wide ? sad_cost_kernel<true> : sad_cost_kernel<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    dim3 g((W + kSadTile - 1) / kSadTile, H);
-    sad_cost_kernel<<<g, 256, smem, s>>>(pl, pr, W, H, D, Dp, minD, r, magic, wide, cost);
+    dim3 g((W + kSadTile - 1) / kSadTile, (H + kSadBand - 1) / kSadBand);
+    kern<<<g, 256, smem, s>>>(pl, pr, W, H, D, Dp, minD, r, magic, cost);
     return cudaGetLastError();
 }
 

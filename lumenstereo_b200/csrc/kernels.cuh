@@ -25,8 +25,22 @@ cudaError_t launch_sad_cost(const uint8_t* pl, const uint8_t* pr, int W, int H, 
 cudaError_t launch_aggregate_per_direction(const PairView& pv, const SgmConsts& k,
                                            unsigned pathMask, bool wrap, cudaStream_t s);
 
-cudaError_t launch_select(const uint16_t* agg, int W, int H, int D, int Dp, int minD, int UR,
-                          int16_t* dispL, int16_t* dispR, cudaStream_t s);
+// Sweep schedule: forward partial into pv.agg, backward partial into partB.
+size_t sweep_ring_bytes(int W, int Dp, int nBandsMax);
+int sweep_rows_per_band(int Dp);
+bool sweep_fits(int W, int Dp);  // shared memory of the sweep kernel fits this device
+cudaError_t launch_aggregate_sweep(const PairView& pv, uint16_t* partB, const SgmConsts& k,
+                                   bool wrap, bool diag, uint8_t* xring, unsigned* counters,
+                                   int* status, long long spinMax, cudaStream_t s, int numSMs);
+
+// aggB (nullable): second partial volume summed with agg (mod 2^16 when wrap).
+cudaError_t launch_select(const uint16_t* agg, const uint16_t* aggB, bool wrap, int W, int H,
+                          int D, int Dp, int minD, int UR, int16_t* dispL, int16_t* dispR,
+                          cudaStream_t s);
+bool select_needs_summed_volume(int D, int Dp);
+// dst = a + b (mod 2^16 per element), n uint16 elements (n even).
+void launch_sum_volumes(const uint16_t* a, const uint16_t* b, uint16_t* dst, size_t n,
+                        cudaStream_t s);
 cudaError_t launch_post(const int16_t* dispL, const int16_t* dispR, int W, int H, int lrMaxDiff,
                         int speckleSize, int speckleDiff, int16_t* out, size_t outPitchElems,
                         int16_t* dbgLR, cudaStream_t s);

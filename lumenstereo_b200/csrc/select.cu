@@ -12,6 +12,8 @@
 // This file is compiled with --use_fast_math like the reference (its
 // CMakeLists.txt:32), so the parabola's (c0 - c2) / denom is the same
 // approximate division and the 1/16-px outputs match bit for bit.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -36,8 +38,9 @@ __device__ __forceinline__ int16_t subpixel_disp(float c0, float c1, float c2, i
 // SMEM: serve the right view from the staged tile (else gather from global).
 template <int KW, bool SMEM>
 __global__ void __launch_bounds__(256)
-select_kernel(const uint16_t* __restrict__ agg, int W, int H, int D, int Dp, int minD, int UR,
-              int T, int16_t* __restrict__ dispL, int16_t* __restrict__ dispR) {
+select_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict__ aggB, int wrap, int W,
+              int H, int D, int Dp, int minD, int UR, int T, int16_t* __restrict__ dispL,
+              int16_t* __restrict__ dispR) {
     extern __shared__ __align__(16) uint16_t sa[];
     const int y = blockIdx.y;
     const int x0 = blockIdx.x * T;
@@ -49,7 +52,16 @@ select_kernel(const uint16_t* __restrict__ agg, int W, int H, int D, int Dp, int
         const uint4* src = reinterpret_cast<const uint4*>(row + (size_t)x0 * Dp);
         uint4* dst = reinterpret_cast<uint4*>(sa);
         const int n16 = nload * Dp / 8;
-        for (int i = threadIdx.x; i < n16; i += blockDim.x) dst[i] = src[i];
+        if (aggB) {  // two partial volumes (sweep schedule): sum while staging
+            const uint4* srcB = reinterpret_cast<const uint4*>(aggB + (size_t)y * W * Dp + (size_t)x0 * Dp);
+            for (int i = threadIdx.x; i < n16; i += blockDim.x) {
+                const uint4 p = src[i], q = srcB[i];
+                dst[i] = wrap ? make_uint4(__vadd2(p.x, q.x), __vadd2(p.y, q.y), __vadd2(p.z, q.z), __vadd2(p.w, q.w))
+                              : make_uint4(p.x + q.x, p.y + q.y, p.z + q.z, p.w + q.w);
+            }
+        } else {
+            for (int i = threadIdx.x; i < n16; i += blockDim.x) dst[i] = src[i];
+        }
         __syncthreads();
     }
     const int dBase = 2 * KW * lane;
@@ -127,9 +139,168 @@ select_kernel(const uint16_t* __restrict__ agg, int W, int H, int D, int Dp, int
     }
 }
 
+// ---------------------------------------------------------------------------
+// select_team_kernel: the same two selections with teams of 8 lanes per pixel
+// (4 pixels per warp); a lane owns KS packed uint16x2 words (2*KS
+// disparities).  The left view takes the min with __vminu2, the first index
+// of the min with __vcmpeq2, and the second order statistic as the min with
+// that one element removed (the multiset statistic the reference's running
+// second-minimum computes, src/sgbm_kernels.cu:764-777); team reductions are
+// 3-step xor butterflies.  The right view gathers agg[y][xr+minD+d][d] from
+// the staged tile, rows padded to Dp+2 elements so that the diagonal spreads
+// over the shared-memory banks.
+// ---------------------------------------------------------------------------
+template <int KS>
+__global__ void __launch_bounds__(256)
+select_team_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict__ aggB, int wrap,
+                   int W, int D, int Dp, int minD, int UR, int T, int16_t* __restrict__ dispL,
+                   int16_t* __restrict__ dispR) {
+    extern __shared__ __align__(16) uint16_t sa[];
+    const int pitch = Dp + 2;
+    const int y = blockIdx.y;
+    const int x0 = blockIdx.x * T;
+    const int loadHi = min(W, x0 + T + D - 1);
+    const int nload = max(0, loadHi - x0);
+    {
+        const uint4* srcA = reinterpret_cast<const uint4*>(agg + ((size_t)y * W + x0) * Dp);
+        const uint4* srcB = aggB ? reinterpret_cast<const uint4*>(aggB + ((size_t)y * W + x0) * Dp) : nullptr;
+        const int per = Dp / 8;  // uint4 per pixel
+        for (int i = threadIdx.x; i < nload * per; i += blockDim.x) {
+            const int px = i / per, q = i - px * per;
+            uint4 v = srcA[i];
+            if (srcB) {
+                const uint4 w = srcB[i];
+                v = wrap ? make_uint4(__vadd2(v.x, w.x), __vadd2(v.y, w.y), __vadd2(v.z, w.z), __vadd2(v.w, w.w))
+                         : make_uint4(v.x + w.x, v.y + w.y, v.z + w.z, v.w + w.w);
+            }
+            uint32_t* d = reinterpret_cast<uint32_t*>(sa + (size_t)px * pitch + q * 8);
+            d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+        }
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, tl = lane & 7;
+    const int tteam = (threadIdx.x >> 5) * 4 + (lane >> 3);
+    const int nTeams = blockDim.x >> 3;
+    const int d0 = tl * 2 * KS;
+    const int Tr = (T + nTeams - 1) / nTeams * nTeams;  // uniform trip count for all teams
+    // ---------------- left view ----------------
+    for (int px = tteam; px < Tr; px += nTeams) {
+        const int x = x0 + px;
+        const bool ok = px < T && x < W;
+        const int pxc = ok ? px : 0;
+        const uint32_t* v32 = reinterpret_cast<const uint32_t*>(sa + (size_t)pxc * pitch) + tl * KS;
+        uint32_t w[KS];
+#pragma unroll
+        for (int k = 0; k < KS; ++k) {
+            uint32_t val = ok && nload > 0 ? v32[k] : 0xFFFFFFFFu;
+            if (d0 + 2 * k >= D) val |= 0x0000FFFFu;
+            if (d0 + 2 * k + 1 >= D) val |= 0xFFFF0000u;
+            w[k] = val;
+        }
+        uint32_t m = w[0];
+#pragma unroll
+        for (int k = 1; k < KS; ++k) m = __vminu2(m, w[k]);
+        m = min(m & 0xFFFFu, m >> 16);
+        m = min(m, __shfl_xor_sync(kFullMask, m, 4));
+        m = min(m, __shfl_xor_sync(kFullMask, m, 2));
+        m = min(m, __shfl_xor_sync(kFullMask, m, 1));
+        const uint32_t best = m, bx2 = best * 0x10001u;
+        uint32_t first = 0xFFFFu;
+#pragma unroll
+        for (int k = KS - 1; k >= 0; --k) {
+            const uint32_t eq = __vcmpeq2(w[k], bx2);
+            const uint32_t idx = (eq & 0xFFFFu) ? (uint32_t)(d0 + 2 * k)
+                                                : ((eq >> 16) ? (uint32_t)(d0 + 2 * k + 1) : 0xFFFFu);
+            first = min(first, idx);
+        }
+        first = min(first, __shfl_xor_sync(kFullMask, first, 4));
+        first = min(first, __shfl_xor_sync(kFullMask, first, 2));
+        first = min(first, __shfl_xor_sync(kFullMask, first, 1));
+        const int bestD = (int)first;
+        // second order statistic: min with the element at bestD removed
+        uint32_t m2 = 0xFFFFFFFFu;
+#pragma unroll
+        for (int k = 0; k < KS; ++k) {
+            uint32_t val = w[k];
+            if (d0 + 2 * k == bestD) val |= 0x0000FFFFu;
+            if (d0 + 2 * k + 1 == bestD) val |= 0xFFFF0000u;
+            m2 = __vminu2(m2, val);
+        }
+        m2 = min(m2 & 0xFFFFu, m2 >> 16);
+        m2 = min(m2, __shfl_xor_sync(kFullMask, m2, 4));
+        m2 = min(m2, __shfl_xor_sync(kFullMask, m2, 2));
+        m2 = min(m2, __shfl_xor_sync(kFullMask, m2, 1));
+        if (ok && tl == 0) {
+            const uint16_t* v = sa + (size_t)px * pitch;
+            int16_t out;
+            if (UR > 0 && m2 != 0xFFFFu && m2 <= best + (best * (uint32_t)UR) / 100u) {
+                out = -1;
+            } else if (bestD > 0 && bestD < D - 1) {
+                out = subpixel_disp((float)v[bestD - 1], (float)v[bestD], (float)v[bestD + 1],
+                                    bestD, D, minD);
+            } else {
+                out = subpixel_disp(0.f, 0.f, 0.f, bestD, D, minD);
+            }
+            dispL[(size_t)y * W + x] = out;
+        }
+    }
+    // ---------------- right view ----------------
+    for (int px = tteam; px < Tr; px += nTeams) {
+        const int xr = x0 - minD + px;
+        const bool ok = px < T && xr >= 0 && xr < W;
+        uint32_t key = 0xFFFFFFFFu;
+#pragma unroll
+        for (int j = 0; j < 2 * KS; ++j) {
+            const int d = d0 + j;
+            const int lx = x0 + px + d;
+            if (ok && d < D && lx < W) {
+                const uint32_t c = sa[(size_t)(px + d) * pitch + d];
+                key = min(key, (c << 16) | (uint32_t)d);
+            }
+        }
+        key = min(key, __shfl_xor_sync(kFullMask, key, 4));
+        key = min(key, __shfl_xor_sync(kFullMask, key, 2));
+        key = min(key, __shfl_xor_sync(kFullMask, key, 1));
+        if (ok && tl == 0) {
+            const int bestD = key == 0xFFFFFFFFu ? 0 : (int)(key & 0xFFFFu);
+            int16_t out;
+            if (bestD > 0 && bestD < D - 1) {
+                const uint16_t* v = sa + (size_t)(px + bestD) * pitch;
+                out = subpixel_disp((float)v[bestD - 1], (float)v[bestD], (float)v[bestD + 1],
+                                    bestD, D, minD);
+            } else {
+                out = subpixel_disp(0.f, 0.f, 0.f, bestD, D, minD);
+            }
+            dispR[(size_t)y * W + xr] = out;
+        }
+    }
+}
+
+template <int KS>
+static cudaError_t launch_select_team(const uint16_t* agg, const uint16_t* aggB, bool wrap, int W,
+                                      int H, int D, int Dp, int minD, int UR, int16_t* dispL,
+                                      int16_t* dispR, cudaStream_t s, bool* launched) {
+    int T = 0;
+    size_t smem = 0;
+    for (int t : {128, 64, 32}) {
+        const size_t b = (size_t)(t + D - 1) * (Dp + 2) * 2;
+        if (b <= 200 * 1024) { T = t; smem = b; break; }
+    }
+    *launched = false;
+    if (T == 0) return cudaSuccess;
+    cudaError_t e = cudaFuncSetAttribute(select_team_kernel<KS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 g((W + minD + T - 1) / T, H);
+    select_team_kernel<KS><<<g, 256, smem, s>>>(agg, aggB, wrap, W, D, Dp, minD, UR, T, dispL, dispR);
+    *launched = true;
+    return cudaGetLastError();
+}
+
 template <int KW>
-static cudaError_t launch_select_kw(const uint16_t* agg, int W, int H, int D, int Dp, int minD,
-                                    int UR, int16_t* dispL, int16_t* dispR, cudaStream_t s) {
+static cudaError_t launch_select_kw(const uint16_t* agg, const uint16_t* aggB, bool wrap, int W,
+                                    int H, int D, int Dp, int minD, int UR, int16_t* dispL,
+                                    int16_t* dispR, cudaStream_t s) {
     // Largest tile whose staged rows fit in shared memory.
     int T = 0;
     size_t smem = 0;
@@ -142,26 +313,66 @@ static cudaError_t launch_select_kw(const uint16_t* agg, int W, int H, int D, in
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         dim3 g((W + minD + T - 1) / T, H);
-        select_kernel<KW, true><<<g, 256, smem, s>>>(agg, W, H, D, Dp, minD, UR, T, dispL, dispR);
+        select_kernel<KW, true><<<g, 256, smem, s>>>(agg, aggB, wrap, W, H, D, Dp, minD, UR, T,
+                                                     dispL, dispR);
     } else {
+        if (aggB) return cudaErrorInvalidValue;  // the caller sums the partials first
         T = 32;
         dim3 g((W + minD + T - 1) / T, H);
-        select_kernel<KW, false><<<g, 256, 0, s>>>(agg, W, H, D, Dp, minD, UR, T, dispL, dispR);
+        select_kernel<KW, false><<<g, 256, 0, s>>>(agg, nullptr, 0, W, H, D, Dp, minD, UR, T,
+                                                   dispL, dispR);
     }
     return cudaGetLastError();
 }
 
-cudaError_t launch_select(const uint16_t* agg, int W, int H, int D, int Dp, int minD, int UR,
-                          int16_t* dispL, int16_t* dispR, cudaStream_t s) {
+bool select_needs_summed_volume(int D, int Dp) {
+    if (Dp <= 320)
+        for (int t : {128, 64, 32})
+            if ((size_t)(t + D - 1) * (Dp + 2) * 2 <= 200 * 1024) return false;
+    for (int t : {128, 64, 32, 16})
+        if ((size_t)(t + D - 1) * Dp * 2 <= 200 * 1024) return false;
+    return true;
+}
+
+__global__ void sum_volumes_kernel(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
+                                   uint32_t* __restrict__ dst, size_t n2) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n2;
+         i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = __vadd2(a[i], b[i]);
+}
+
+void launch_sum_volumes(const uint16_t* a, const uint16_t* b, uint16_t* dst, size_t n,
+                        cudaStream_t s) {
+    const size_t n2 = n / 2;
+    const int blocks = (int)std::min<size_t>((n2 + 255) / 256, 148 * 16);
+    sum_volumes_kernel<<<blocks, 256, 0, s>>>(reinterpret_cast<const uint32_t*>(a),
+                                              reinterpret_cast<const uint32_t*>(b),
+                                              reinterpret_cast<uint32_t*>(dst), n2);
+}
+
+cudaError_t launch_select(const uint16_t* agg, const uint16_t* aggB, bool wrap, int W, int H,
+                          int D, int Dp, int minD, int UR, int16_t* dispL, int16_t* dispR,
+                          cudaStream_t s) {
+    bool launched = false;
+    cudaError_t e = cudaSuccess;
+    switch (Dp / 16) {
+    case 4: e = launch_select_team<4>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, &launched); break;
+    case 8: e = launch_select_team<8>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, &launched); break;
+    case 12: e = launch_select_team<12>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, &launched); break;
+    case 16: e = launch_select_team<16>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, &launched); break;
+    case 20: e = launch_select_team<20>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, &launched); break;
+    default: break;
+    }
+    if (e != cudaSuccess || launched) return e;
     switch (Dp / 64) {
-    case 1: return launch_select_kw<1>(agg, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 2: return launch_select_kw<2>(agg, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 3: return launch_select_kw<3>(agg, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 4: return launch_select_kw<4>(agg, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 5: return launch_select_kw<5>(agg, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 6: return launch_select_kw<6>(agg, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 7: return launch_select_kw<7>(agg, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 8: return launch_select_kw<8>(agg, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 1: return launch_select_kw<1>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 2: return launch_select_kw<2>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 3: return launch_select_kw<3>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 4: return launch_select_kw<4>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 5: return launch_select_kw<5>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 6: return launch_select_kw<6>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 7: return launch_select_kw<7>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 8: return launch_select_kw<8>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -103,8 +103,9 @@ CASES = {
 }
 
 
+@pytest.mark.parametrize("schedule", [1, 2])
 @pytest.mark.parametrize("name", sorted(CASES))
-def test_parity_small(name, oracle_mod):
+def test_parity_small(name, schedule, oracle_mod):
     w, h, over = CASES[name]
     if w * h >= 2048:
         left, right, _ = synth.make_pair(synth.PairSpec(w, h, 4, 1, max(2, 0.3 * min(w, 300)), 2.0,
@@ -112,7 +113,7 @@ def test_parity_small(name, oracle_mod):
     else:
         left, right = synth.random_pair(w, h, seed=zlib.crc32(name.encode()) % 1000, shift=1)
     compare_all(params_dict(speckleWindowSize=0, **over) if "speckle" not in name
-                else params_dict(**over), left, right, oracle_mod)
+                else params_dict(**over), left, right, oracle_mod, schedule=schedule)
 
 
 @pytest.mark.parametrize("k", range(8))
@@ -198,6 +199,26 @@ def test_disparity_range_exceeds_gpu_limit():
             s.compute(img, img)
 
 
+@pytest.mark.parametrize("wl", ["640x480_d64_census_4path", "1920x1080_d128_census_8path"])
+def test_schedules_agree_full_size(wl):
+    """Per-direction kernels and the fused sweeps give identical volumes and maps."""
+    w = synth.WORKLOADS[wl]
+    left, right, _ = synth.make_pair(w.pair)
+    p = StereoParams(maxDisparity=w.max_disparity, numDirections=w.num_directions,
+                     matchingCostMode=MatchingCostMode.Census if w.census else MatchingCostMode.SAD,
+                     speckleWindowSize=0)
+    outs = []
+    for schedule in (1, 2):
+        with StereoSGBM(p) as s:
+            s.set_schedule(schedule)
+            s.retain_intermediates(True)
+            d = s.compute(left, right)
+            agg = s.intermediate("agg", left.shape + (w.max_disparity,), np.uint16)
+            outs.append((d, agg))
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert np.array_equal(outs[0][0], outs[1][0])
+
+
 def test_deterministic_and_handle_reuse():
     left, right, _ = synth.make_pair(synth.PairSpec(200, 120, 5, 4, 40, 2.0, 77))
     p = StereoParams(maxDisparity=48, numDirections=8, matchingCostMode=MatchingCostMode.Census)
@@ -263,17 +284,20 @@ def test_parity_vs_reference_kernels_full_size(wl, oracle_mod):
     p = params_dict(maxDisparity=w.max_disparity, matchingCostMode=int(w.census),
                     numDirections=w.num_directions, speckleWindowSize=0)
     ref_disp, ref, _ = oracle_mod.ref_sgbm(p, left, right, intermediates=False)
-    ours, inter = run_ours_light(p, left, right)
-    assert np.array_equal(ours, ref_disp)
+    for schedule in (1, 2):
+        ours, inter = run_ours_light(p, left, right, schedule)
+        assert np.array_equal(ours, ref_disp), schedule
     # sanity: the scene's disparities are recovered
     v = ours > 0
     assert v.mean() > 0.5
     assert np.median(np.abs(ours[v] / 16.0 - gt[v])) < 1.0
 
 
-def run_ours_light(pdict, left, right):
+def run_ours_light(pdict, left, right, schedule=0):
     p = to_params(pdict)
     with StereoSGBM(p) as s:
+        if schedule:
+            s.set_schedule(schedule)
         return s.compute(left, right), None
 
 
@@ -286,10 +310,11 @@ def test_parity_vs_reference_kernels_intermediates(oracle_mod):
         p = params_dict(maxDisparity=64, matchingCostMode=mode, numDirections=nd,
                         uniquenessRatio=ur, speckleWindowSize=0)
         ref_disp, ref, _ = oracle_mod.ref_sgbm(p, left, right, intermediates=True)
-        disp, ours = run_ours(p, left, right)
-        for key in ("cost", "agg", "disp_wta", "disp_right", "disp_lr"):
-            assert np.array_equal(ours[key], ref[key]), (mode, nd, key)
-        assert np.array_equal(disp, ref_disp)
+        for schedule in (1, 2):
+            disp, ours = run_ours(p, left, right, schedule=schedule)
+            for key in ("cost", "agg", "disp_wta", "disp_right", "disp_lr"):
+                assert np.array_equal(ours[key], ref[key]), (mode, nd, key, schedule)
+            assert np.array_equal(disp, ref_disp)
 
 
 def test_remap_vs_reference_kernel(oracle_mod):
