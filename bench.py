@@ -230,10 +230,15 @@ def run_ours(args):
     def step():
         sgbm.compute_device(dl.data_ptr(), dr.data_ptr(), W, H, dout.data_ptr(), stream=sptr)
 
+    tune_report = None
+    if not args.schedule:
+        # autotuner: every schedule / sweep configuration on this pair, outside the timed region
+        tune_report = sgbm.autotune(dl.data_ptr(), dr.data_ptr(), W, H, repeats=2)
     for _ in range(args.warmup):
         flush.zero_()
         step()
     torch.cuda.synchronize()
+    tuning = sgbm.get_tuning()
     check = dout.cpu().numpy()
     v = check > 0
     quality = {"valid_frac": float(v.mean()),
@@ -314,7 +319,9 @@ def run_ours(args):
                    "cost": "census" if wl.census else "sad+sobel-x prefilter",
                    "paths": P, "params": "StereoParams defaults, speckleWindowSize=0",
                    "l2": "256 MiB buffer written before every timed step, outside its events",
-                   "parallelism": f"replicas x{world}", "schedule": args.schedule or "auto"},
+                   "parallelism": f"replicas x{world}",
+                   "schedule": {"requested": args.schedule or "auto", "used": tuning[0],
+                                "lanes_per_pixel": tuning[1], "warps_per_block": tuning[2]}},
         "roofline": {"bound": "hbm", "kernel": "sgm aggregation stage",
                      "achieved": achieved, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / hbm,
@@ -331,6 +338,7 @@ def run_ours(args):
         "gpu_launches": int(launches),
         "clocks": clocks.summary(),
         "quality": quality,
+        "autotune": tune_report.strip().splitlines() if tune_report else None,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         pdct = params_dict(params)

@@ -116,6 +116,22 @@ lumen_status lumen_sgbm_debug_set_paths(lumen_sgbm* h, uint32_t path_mask);
  * per direction, 2 = two fused wavefront sweeps.  Values, not outputs, are the
  * same for every schedule. */
 lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule);
+/* Pin the fused-sweep configuration: lanes per pixel (8, 16 or 32) and warps
+ * per thread block (2, 4 or 8; rows per band = warps * 32 / lanes).  0, 0
+ * restores the automatic choice.  Values are identical for every setting. */
+lumen_status lumen_sgbm_set_tuning(lumen_sgbm* h, int lanes_per_pixel, int warps_per_block);
+/* The schedule and configuration the last compute used: {schedule, lanes, warps}. */
+lumen_status lumen_sgbm_get_tuning(const lumen_sgbm* h, int out[3]);
+/* Autotuner (no counterpart in the reference): runs every aggregation schedule
+ * and sweep configuration `repeats` times on the given DEVICE pair, keeps the
+ * fastest for this (size, disparity range, cost mode, path set) key, and
+ * writes one line per candidate into `report`.  Synchronous. */
+lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left, const uint8_t* d_right,
+                                 int width, int height, size_t in_stride, int channels,
+                                 int repeats, char* report, size_t report_bytes);
+/* Persist / restore the autotuner's decisions (text, one key per line). */
+lumen_status lumen_sgbm_tuning_save(const lumen_sgbm* h, const char* path);
+lumen_status lumen_sgbm_tuning_load(lumen_sgbm* h, const char* path);
 /* Copies one internal buffer of the last compute to host memory `dst`
  * (capacity dst_bytes).  which: 0 prefiltered left, 1 prefiltered right,
  * 2 census left (uint32), 3 census right, 4 cost volume (uint8 HxWxD),

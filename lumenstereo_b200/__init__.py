@@ -242,6 +242,31 @@ class StereoSGBM:
     def set_schedule(self, schedule: int) -> None:
         _check(_lib.lib().lumen_sgbm_set_schedule(self._h, schedule))
 
+    def set_tuning(self, lanes_per_pixel: int = 0, warps_per_block: int = 0) -> None:
+        """Pin the fused-sweep configuration (0, 0 = automatic)."""
+        _check(_lib.lib().lumen_sgbm_set_tuning(self._h, lanes_per_pixel, warps_per_block))
+
+    def get_tuning(self):
+        """(schedule, lanes per pixel, warps per block) the last compute used."""
+        out = (C.c_int * 3)()
+        _check(_lib.lib().lumen_sgbm_get_tuning(self._h, out))
+        return tuple(out)
+
+    def autotune(self, left_ptr: int, right_ptr: int, width: int, height: int,
+                 channels: int = 1, in_stride: int = 0, repeats: int = 2) -> str:
+        """Time every aggregation schedule/configuration on device buffers and
+        keep the fastest for this workload; returns the per-candidate report."""
+        buf = C.create_string_buffer(4096)
+        _check(_lib.lib().lumen_sgbm_autotune(self._h, left_ptr, right_ptr, width, height,
+                                              in_stride, channels, repeats, buf, 4096))
+        return buf.value.decode()
+
+    def save_tuning(self, path: str) -> None:
+        _check(_lib.lib().lumen_sgbm_tuning_save(self._h, path.encode()))
+
+    def load_tuning(self, path: str) -> None:
+        _check(_lib.lib().lumen_sgbm_tuning_load(self._h, path.encode()))
+
     def launch_count(self) -> int:
         """Kernels this handle has enqueued so far."""
         return int(_lib.lib().lumen_sgbm_debug_launch_count(self._h))

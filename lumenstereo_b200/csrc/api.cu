@@ -11,6 +11,11 @@
 #include <cstring>
 #include <string>
 #include <algorithm>
+#include <map>
+#include <fstream>
+#include <sstream>
+#include <cstdlib>
+#include <vector>
 
 #include "../../include/lumen_sgbm.h"
 #include "common.cuh"
@@ -76,6 +81,10 @@ struct lumen_sgbm {
     int numSMs = 148;
     long long spinMax = 1ll << 22;          // bounded device-side waits
     bool statusPending = false;
+    SweepConfig forced{0, 0};               // lumen_sgbm_set_tuning (0 = automatic)
+    std::map<std::string, std::pair<int, SweepConfig>> tuned;  // key -> (schedule, config)
+    int lastSchedule = 0;
+    SweepConfig lastConfig{0, 0};
     int magicR = -1;
     float timings[4] = {0, 0, 0, 0};
     unsigned pathOverride = 0;
@@ -248,6 +257,26 @@ extern "C" lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule) {
     return LUMEN_OK;
 }
 
+extern "C" lumen_status lumen_sgbm_set_tuning(lumen_sgbm* h, int lanes, int warps) {
+    if (!h) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL handle");
+    if (lanes == 0 && warps == 0) {
+        h->forced = SweepConfig{0, 0};
+        return LUMEN_OK;
+    }
+    if (!(lanes == 8 || lanes == 16 || lanes == 32) || !(warps == 2 || warps == 4 || warps == 8))
+        return fail(LUMEN_ERR_INVALID_ARGUMENT, "lanes must be 8/16/32 and warps 2/4/8");
+    h->forced = SweepConfig{lanes, warps};
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_sgbm_get_tuning(const lumen_sgbm* h, int out[3]) {
+    if (!h || !out) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL argument");
+    out[0] = h->lastSchedule;
+    out[1] = h->lastConfig.T;
+    out[2] = h->lastConfig.NW;
+    return LUMEN_OK;
+}
+
 extern "C" lumen_status lumen_sgbm_debug_retain(lumen_sgbm* h, int enable) {
     if (!h) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL handle");
     h->retain = enable ? 1 : 0;
@@ -306,6 +335,14 @@ static bool no_wrap(const lumen_stereo_params& p, int cs, int nPaths) {
     if (lmax + p2max > 65535) return false;
     if (lmax * nPaths > 65535) return false;
     return true;
+}
+
+// Autotuner key: geometry, disparity range, cost mode, path set, arithmetic mode.
+static std::string tune_key(int W, int H, const lumen_stereo_params& p, unsigned mask, bool wrap) {
+    std::ostringstream o;
+    o << W << "x" << H << ":D" << (p.maxDisparity - p.minDisparity) << ":m" << p.matchingCostMode
+      << ":p" << mask << ":w" << (wrap ? 1 : 0);
+    return o.str();
 }
 
 // ---------------------------------------------------------------------------
@@ -380,17 +417,30 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
     const bool wrap = !no_wrap(p, k.costScale, __builtin_popcount(mask));
     PairView pv{h->cost.as<uint8_t>(), gl, h->agg.as<uint16_t>()};
     const bool sweepable = (mask == 0xFFu || mask == 0x0Fu);
-    int sched = h->schedule ? h->schedule : (sweepable ? 2 : 1);
-    if (sched == 2 && !sweepable) sched = 1;  // single-path debug masks: per-direction kernels
-    if (sched == 2 && !sweep_fits(W, Dp)) sched = 1;  // very wide images: per-direction kernels
+    int sched = h->schedule;
+    SweepConfig cfg = h->forced.T ? h->forced : sweep_default_config(Dp, wrap);
+    if (!h->forced.T && sched == 0) {
+        auto it = h->tuned.find(tune_key(W, H, p, mask, wrap));
+        if (it != h->tuned.end()) {
+            sched = it->second.first;
+            cfg = it->second.second;
+        }
+    }
+    if (sched == 0) sched = sweepable ? 2 : 1;
+    if (sched == 2 && !sweepable) sched = 1;          // single-path debug masks: per-direction kernels
+    if (sched == 2 && !sweep_fits(W, Dp, cfg)) sched = 1;  // very wide images: per-direction kernels
     const uint16_t* aggB = nullptr;
     if (sched == 2) {
-        const int R = sweep_rows_per_band(Dp);
-        const int nBands = (H + R - 1) / R;
+        SweepPlan plan;
+        cudaError_t pe = sweep_plan(pv, k, cfg, wrap, mask == 0xFFu, h->numSMs, &plan);
+        if (pe != cudaSuccess) {  // this configuration cannot serve these parameters
+            cfg = sweep_default_config(Dp, wrap);
+            LCU(sweep_plan(pv, k, cfg, wrap, mask == 0xFFu, h->numSMs, &plan));
+        }
         LCU(h->partB.ensure(ND * 2));
-        LCU(h->xring.ensure(sweep_ring_bytes(W, Dp, nBands)));
-        LCU(h->counters.ensure(sizeof(unsigned) * 4 * (size_t)nBands));
-        LCU(launch_aggregate_sweep(pv, h->partB.as<uint16_t>(), k, wrap, mask == 0xFFu,
+        LCU(h->xring.ensure(plan.ringBytes));
+        LCU(h->counters.ensure(sizeof(unsigned) * plan.counterWords));
+        LCU(launch_aggregate_sweep(pv, h->partB.as<uint16_t>(), k, wrap, mask == 0xFFu, cfg, plan,
                                    h->xring.as<uint8_t>(), h->counters.as<unsigned>(),
                                    h->status.as<int>(), h->spinMax, s, h->numSMs));
         h->statusPending = true;
@@ -406,6 +456,8 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
         LCU(launch_aggregate_per_direction(pv, k, mask, wrap, s));
         nl += __builtin_popcount(mask);
     }
+    h->lastSchedule = sched;
+    h->lastConfig = sched == 2 ? cfg : SweepConfig{0, 0};
     if (timed) LCU(cudaEventRecord(h->ev[3], s));
     // selection + post-processing
     LCU(launch_select(h->agg.as<uint16_t>(), aggB, wrap, W, H, D, Dp, p.minDisparity,
@@ -472,6 +524,94 @@ extern "C" lumen_status lumen_sgbm_compute_device(lumen_sgbm* h, const uint8_t* 
                       out_stride / 2, s, true);
     if (st == LUMEN_OK) h->timingsPending = true;
     return st;
+}
+
+// Autotuner: every aggregation schedule / sweep configuration runs `repeats`
+// times on the caller's device pair; the fastest whole-pipeline device time
+// is kept for this workload key (lumen_sgbm_compute_device then uses it).
+extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left,
+                                            const uint8_t* d_right, int width, int height,
+                                            size_t in_stride, int channels, int repeats,
+                                            char* report, size_t report_bytes) {
+    if (!h) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL handle");
+    lumen_status st = validate(h->params, d_left, d_right, width, height, in_stride, channels);
+    if (st != LUMEN_OK) return st;
+    if (repeats < 1) repeats = 1;
+    const size_t row = (size_t)width * channels;
+    if (!in_stride) in_stride = row;
+    LCU(h->out.ensure((size_t)width * height * 2));
+    const lumen_stereo_params& p = h->params;
+    const int D = p.maxDisparity - p.minDisparity, Dp = padded_d(D);
+    const unsigned mask = path_mask(h);
+    const bool wrap = !no_wrap(p, cost_scale(p), __builtin_popcount(mask));
+    const std::string key = tune_key(width, height, p, mask, wrap);
+    std::vector<std::pair<int, SweepConfig>> cands;
+    cands.push_back({1, SweepConfig{0, 0}});
+    if (mask == 0xFFu || mask == 0x0Fu) {
+        SweepConfig cs[8];
+        const int n = sweep_configs(Dp, cs, 8);
+        for (int i = 0; i < n; ++i) {
+            if (wrap && !(cs[i].T == 32 && cs[i].NW == 4)) continue;
+            if (!sweep_fits(width, Dp, cs[i])) continue;
+            cands.push_back({2, cs[i]});
+        }
+    }
+    const SweepConfig savedForced = h->forced;
+    const int savedSched = h->schedule;
+    std::ostringstream rep;
+    float bestMs = 1e30f;
+    std::pair<int, SweepConfig> best = cands[0];
+    for (auto& c : cands) {
+        h->schedule = c.first;
+        h->forced = c.second;
+        float acc = 0.f;
+        bool ok = true;
+        for (int r = 0; r <= repeats; ++r) {  // first run warms up
+            LCU(cudaEventRecord(h->ev[0], h->stream));
+            st = run_pipeline(h, d_left, d_right, in_stride, channels, width, height,
+                              h->out.as<int16_t>(), (size_t)width, h->stream, true);
+            if (st != LUMEN_OK) { ok = false; break; }
+            LCU(cudaStreamSynchronize(h->stream));
+            st = read_timings(h);
+            if (st != LUMEN_OK) { ok = false; break; }
+            if (r > 0) acc += h->timings[0];
+        }
+        if (!ok || h->lastSchedule != c.first) continue;
+        const float ms = acc / repeats;
+        rep << "schedule=" << c.first << " lanes=" << c.second.T << " warps=" << c.second.NW
+            << " ms=" << ms << "\n";
+        if (ms < bestMs) { bestMs = ms; best = c; }
+    }
+    h->schedule = savedSched;
+    h->forced = savedForced;
+    h->tuned[key] = best;
+    rep << "best schedule=" << best.first << " lanes=" << best.second.T << " warps="
+        << best.second.NW << " key=" << key << "\n";
+    if (report && report_bytes) {
+        const std::string r = rep.str();
+        std::snprintf(report, report_bytes, "%s", r.c_str());
+    }
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_sgbm_tuning_save(const lumen_sgbm* h, const char* path) {
+    if (!h || !path) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::ofstream f(path);
+    if (!f) return fail(LUMEN_ERR_INVALID_ARGUMENT, std::string("cannot write ") + path);
+    for (auto& kv : h->tuned)
+        f << kv.first << " " << kv.second.first << " " << kv.second.second.T << " "
+          << kv.second.second.NW << "\n";
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_sgbm_tuning_load(lumen_sgbm* h, const char* path) {
+    if (!h || !path) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::ifstream f(path);
+    if (!f) return fail(LUMEN_ERR_INVALID_ARGUMENT, std::string("cannot read ") + path);
+    std::string key;
+    int sched, T, NW;
+    while (f >> key >> sched >> T >> NW) h->tuned[key] = {sched, SweepConfig{T, NW}};
+    return LUMEN_OK;
 }
 
 extern "C" lumen_status lumen_sgbm_debug_copy(lumen_sgbm* h, int which, void* dst,

@@ -25,13 +25,29 @@ cudaError_t launch_sad_cost(const uint8_t* pl, const uint8_t* pr, int W, int H, 
 cudaError_t launch_aggregate_per_direction(const PairView& pv, const SgmConsts& k,
                                            unsigned pathMask, bool wrap, cudaStream_t s);
 
-// Sweep schedule: forward partial into pv.agg, backward partial into partB.
-size_t sweep_ring_bytes(int W, int Dp, int nBandsMax);
-int sweep_rows_per_band(int Dp);
-bool sweep_fits(int W, int Dp);  // shared memory of the sweep kernel fits this device
+// Sweep schedule (two fused wavefront sweeps): forward partial into pv.agg,
+// backward partial into partB.  A configuration is T lanes per pixel and NW
+// warps per CTA (rows per band = NW * 32 / T).
+struct SweepConfig {
+    int T;
+    int NW;
+};
+struct SweepPlan {
+    int G;                 // CTAs per sweep
+    int nBands;            // bands per sweep
+    int K;                 // exchange ring capacity (pixels)
+    size_t ringBytes;      // bytes of exchange rings
+    size_t counterWords;   // progress counters (uint32)
+};
+int sweep_configs(int Dp, SweepConfig* out, int max);
+SweepConfig sweep_default_config(int Dp, bool wrap);
+bool sweep_fits(int W, int Dp, SweepConfig c);
+cudaError_t sweep_plan(const PairView& pv, const SgmConsts& k, SweepConfig c, bool wrap, bool diag,
+                       int numSMs, SweepPlan* plan);
 cudaError_t launch_aggregate_sweep(const PairView& pv, uint16_t* partB, const SgmConsts& k,
-                                   bool wrap, bool diag, uint8_t* xring, unsigned* counters,
-                                   int* status, long long spinMax, cudaStream_t s, int numSMs);
+                                   bool wrap, bool diag, SweepConfig c, const SweepPlan& plan,
+                                   uint8_t* xring, unsigned* counters, int* status,
+                                   long long spinMax, cudaStream_t s, int numSMs);
 
 // aggB (nullable): second partial volume summed with agg (mod 2^16 when wrap).
 cudaError_t launch_select(const uint16_t* agg, const uint16_t* aggB, bool wrap, int W, int H,

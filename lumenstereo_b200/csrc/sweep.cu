@@ -1,399 +1,115 @@
-// sweep.cu -- SGM aggregation as two fused wavefront sweeps (schedule 2).
-//
-// The eight path recurrences of the reference (src/sgbm_kernels.cu:315-742)
-// are regrouped by the neighbour they read:
-//   forward sweep  F: LR (x-1,y)  TB (x,y-1)  TLBR (x-1,y-1)  TRBL (x+1,y-1)
-//   backward sweep B: RL (x+1,y)  BT (x,y+1)  BRTL (x+1,y+1)  BLTR (x-1,y+1)
-// B is F with the image mirrored in both axes, so one kernel body runs both in
-// "sweep coordinates" (u, v): x = u or W-1-u, y = v or H-1-v.  A pixel needs
-// its own row's previous pixel and the previous row's pixels u-1, u, u+1, so
-// rows advance as a wavefront with row v+1 two pixels behind row v.
-//
-// Work decomposition: a CTA owns a band of R consecutive sweep rows and walks
-// them in lockstep (one __syncthreads per step), teams of T lanes per row
-// (T = 32, 16 or 8; lane holds 2*KW disparities, sgm_step.cuh).  Row r hands
-// its TB/TLBR/TRBL vectors to row r+1 through a 4-slot shared-memory ring; the
-// band's last row hands them to the next band (another CTA) through a global
-// ring with release/acquire progress counters, and the next band prefetches
-// them with cp.async.  Cost vectors are prefetched the same way.  The four
-// path vectors of a pixel are summed in registers and stored once: each sweep
-// writes one uint16 partial volume, no read-modify-write of the aggregate.
-//
-// All CTAs are co-resident (cooperative launch); a CTA that runs out of bands
-// exits.  Every wait is a bounded spin: on timeout the CTA records
-// LUMEN_ERR_TIMEOUT in *status and leaves its band (all its warps together).
+// sweep.cu -- host side of the fused two-sweep aggregation (schedule 2):
+// configuration choice, exchange-ring sizing and dispatch to the compiled
+// instances in sweep_cfg_*.cu (kernel in sweep_kernel.cuh).
 #include <algorithm>
 
-#include "../../include/lumen_sgbm.h"
 #include "common.cuh"
 #include "kernels.cuh"
-#include "sgm_step.cuh"
+#include "sweep_kernel.cuh"
 
 namespace lumen {
 
-constexpr int kLag = 4;        // prefetch distance (steps) of cost / exchange copies
-constexpr int kRowSlots = 4;   // smem ring slots per band row
-constexpr int kXSlots = 8;     // smem ring slots of the incoming (previous band's) row
-constexpr int kCostSlots = 8;  // smem cost slots per row
-constexpr int kPublish = 8;    // publish progress every kPublish steps
+#define LUMEN_SWEEP_DISPATCH(dp)                                                           \
+    cudaError_t sweep_dispatch_##dp(SweepArgs a, int T, int NW, bool wrap, bool diag,     \
+                                    cudaStream_t s, int numSMs, int* g);
+LUMEN_SWEEP_DISPATCH(64)
+LUMEN_SWEEP_DISPATCH(128)
+LUMEN_SWEEP_DISPATCH(192)
+LUMEN_SWEEP_DISPATCH(256)
+LUMEN_SWEEP_DISPATCH(320)
+LUMEN_SWEEP_DISPATCH(384)
+LUMEN_SWEEP_DISPATCH(448)
+LUMEN_SWEEP_DISPATCH(512)
 
-struct SweepArgs {
-    const uint8_t* cost;
-    const uint8_t* img;
-    uint16_t* part[2];       // per-sweep partial sums, [H][W][Dp]
-    uint8_t* xring;          // [2][G][W][3][slotBytes]
-    unsigned* prod;          // [2][G] pixels published (monotonic over the launch)
-    unsigned* cons;          // [2][G] pixels consumed
-    int* status;
-    int W, H, D, Dp;
-    int P1, P2, costScale;
-    uint32_t p1x2, bsub;
-    int R;                   // rows per band
-    int nBands;              // per sweep
-    int G;                   // CTAs per sweep
-    int slotBytes;           // 2*Dp + 16
-    long long spinMax;
-};
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
-
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+int sweep_configs(int Dp, SweepConfig* out, int max) {
+    static const SweepConfig small[] = {{32, 4}, {32, 8}, {16, 4}, {8, 4}, {8, 2}};
+    static const SweepConfig mid[] = {{32, 4}, {32, 8}, {16, 4}};
+    static const SweepConfig big[] = {{32, 4}, {32, 8}};
+    const SweepConfig* src = Dp <= 128 ? small : (Dp <= 256 ? mid : big);
+    const int n = Dp <= 128 ? 5 : (Dp <= 256 ? 3 : 2);
+    for (int i = 0; i < n && i < max; ++i) out[i] = src[i];
+    return std::min(n, max);
 }
 
-// Shared memory carve-up (bytes), identical on host and device.
-struct SweepSmem {
-    int imgOff, ringOff, xOff, costOff, lutOff, total;
-    int Wp, slotBytes;
-};
-__host__ __device__ inline SweepSmem sweep_smem(int W, int Dp, int R) {
-    SweepSmem s;
-    s.Wp = (W + 15) & ~15;
-    s.slotBytes = 2 * Dp + 16;
-    s.imgOff = 0;
-    int o = (R + 1) * s.Wp;
-    o = (o + 15) & ~15;
-    s.ringOff = o;
-    o += R * 3 * kRowSlots * s.slotBytes;
-    s.xOff = o;
-    o += 3 * kXSlots * s.slotBytes;
-    s.costOff = o;
-    o += R * kCostSlots * Dp;
-    s.lutOff = o;
-    o += 256 * 4;
-    s.total = o;
-    return s;
+SweepConfig sweep_default_config(int Dp, bool wrap) {
+    (void)Dp;
+    (void)wrap;
+    return SweepConfig{32, 4};
 }
 
-template <int T, int KW, bool WRAP, bool FULL, int NW, int NP>
-__global__ void __launch_bounds__(NW * 32)
-sweep_kernel(SweepArgs a) {
-    constexpr int RPW = 32 / T;  // rows per warp
-    extern __shared__ __align__(16) uint8_t sm[];
-    const SweepSmem L = sweep_smem(a.W, a.Dp, a.R);
-    uint8_t* simg = sm + L.imgOff;
-    uint8_t* sring = sm + L.ringOff;
-    uint8_t* sx = sm + L.xOff;
-    uint8_t* scost = sm + L.costOff;
-    int* p2lut = reinterpret_cast<int*>(sm + L.lutOff);
-    __shared__ int abortFlag;
-
-    const int sw = blockIdx.x & 1;   // 0 forward, 1 backward
-    const int c = blockIdx.x >> 1;   // CTA index within the sweep
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int team = lane / T, tl = lane & (T - 1);
-    const int r = warp * RPW + team;  // band row of this team
-    const int W = a.W, H = a.H, Dp = a.Dp;
-    const int off = tl * 2 * KW;      // first disparity of this lane
-    const int SB = L.slotBytes;
-
-    for (int g = threadIdx.x; g < 256; g += blockDim.x)
-        p2lut[g] = max(a.P1 + 1, a.P2 * 8 / max(8, g));
-    if (threadIdx.x == 0) abortFlag = 0;
-
-    LaneMasks<KW> mk;
-    make_lane_masks<KW>(tl, a.D, mk);
-    uint16_t* part = sw ? a.part[1] : a.part[0];
-    const size_t ringStride = (size_t)W * 3 * SB;
-
-    for (int b = c; b < a.nBands; b += a.G) {
-        const int it = b / a.G;
-        const int v0 = b * a.R;
-        const int v = v0 + r;
-        const bool rowOk = r < a.R && v < H;
-        // ---- stage sweep-oriented image rows v0-1 .. v0+R-1 ----
-        __syncthreads();
-        for (int i = threadIdx.x; i < (a.R + 1) * W; i += blockDim.x) {
-            const int rr = i / W, u = i - rr * W;
-            const int vv = v0 - 1 + rr;
-            uint8_t val = 0;
-            if (vv >= 0 && vv < H) {
-                const int x = sw ? W - 1 - u : u, y = sw ? H - 1 - vv : vv;
-                val = a.img[(size_t)y * W + x];
-            }
-            simg[rr * L.Wp + u] = val;
-        }
-        __syncthreads();
-        // incoming ring of the previous band (produced by CTA (b-1) % G, iteration (b-1) / G)
-        const bool hasPrev = b > 0;
-        const int pc = (b - 1 + a.G) % a.G;
-        const unsigned pBase = hasPrev ? (unsigned)((b - 1) / a.G) * (unsigned)W : 0u;
-        const uint8_t* pring = a.xring + ((size_t)sw * a.G + pc) * ringStride;
-        unsigned* pProd = a.prod + sw * a.G + pc;
-        unsigned* pCons = a.cons + sw * a.G + pc;
-        // outgoing ring (this CTA, iteration it)
-        const bool hasNext = b + 1 < a.nBands;
-        uint8_t* oring = a.xring + ((size_t)sw * a.G + c) * ringStride;
-        unsigned* oProd = a.prod + sw * a.G + c;
-        unsigned* oCons = a.cons + sw * a.G + c;
-        const unsigned oBase = (unsigned)it * (unsigned)W;
-        unsigned seenProd = 0, seenCons = 0;
-        const bool lastRow = (r == a.R - 1) || (v == H - 1);
-        const bool firstRow = (r == 0);
-
-        uint32_t LH[KW];
-#pragma unroll
-        for (int w = 0; w < KW; ++w) LH[w] = 0;
-        uint32_t minH = 0;
-        const int sEnd = W - 1 + 2 * (a.R - 1);
-        for (int s = -kLag - 1; s <= sEnd; ++s) {
-            const int u = s - 2 * r;
-            // ---- prefetch: cost of pixel u+kLag for this row ----
-            {
-                const int pu = u + kLag;
-                if (rowOk && pu >= 0 && pu < W) {
-                    const int x = sw ? W - 1 - pu : pu, y = sw ? H - 1 - v : v;
-                    const uint8_t* src = a.cost + ((size_t)y * W + x) * Dp;
-                    uint8_t* dst = scost + (r * kCostSlots + (pu & (kCostSlots - 1))) * Dp;
-                    for (int k = tl; k < Dp / 16; k += T) cp_async16(dst + 16 * k, src + 16 * k);
-                }
-            }
-            // ---- prefetch: previous band's row, pixel s+kLag+1 (warp 0) ----
-            if (warp == 0 && hasPrev) {
-                const int pu = s + kLag + 1;
-                if (pu >= 0 && pu < W) {
-                    const unsigned need = pBase + (unsigned)pu + 1u;
-                    if (seenProd < need) {
-                        long long spins = 0;
-                        unsigned pv = ld_acquire(pProd);
-                        while (pv < need && ++spins < a.spinMax) pv = ld_acquire(pProd);
-                        if (pv < need) {
-                            if (lane == 0) { atomicExch(a.status, (int)LUMEN_ERR_TIMEOUT); abortFlag = 1; }
-                            pv = need;  // leave the loop; abortFlag stops the band below
-                        }
-                        seenProd = pv;
-                    }
-                    const uint8_t* src = pring + (size_t)pu * 3 * SB;
-                    uint8_t* dst = sx + (pu & (kXSlots - 1)) * 3 * SB;
-                    for (int k = lane; k < 3 * SB / 16; k += 32) cp_async16(dst + 16 * k, src + 16 * k);
-                }
-            }
-            cp_async_commit();
-
-            // ---- back-pressure: the outgoing slot of pixel u was last used one
-            //      iteration ago; wait until that pixel was consumed ----
-            const bool active = rowOk && u >= 0 && u < W;
-            const unsigned teamMask = T == 32 ? 0xFFFFFFFFu : (((1u << T) - 1u) << (team * T));
-            if (it > 0 && hasNext && active && lastRow) {
-                const unsigned need = oBase - (unsigned)W + (unsigned)u + 1u;
-                if (seenCons < need) {
-                    unsigned cv = 0;
-                    if (tl == 0) {
-                        long long spins = 0;
-                        cv = ld_acquire(oCons);
-                        while (cv < need && ++spins < a.spinMax) cv = ld_acquire(oCons);
-                        if (cv < need) { atomicExch(a.status, (int)LUMEN_ERR_TIMEOUT); abortFlag = 1; cv = need; }
-                    }
-                    seenCons = __shfl_sync(teamMask, cv, 0, T);
-                }
-            }
-            // ---- compute pixel u of row r: every lane of the warp runs the math
-            //      (teams of one warp sit at different u), stores are predicated ----
-            {
-                const int uc = min(max(u, 0), W - 1);
-                const int x = sw ? W - 1 - uc : uc, y = sw ? H - 1 - min(v, H - 1) : min(v, H - 1);
-                uint32_t Cw[KW], Ln[KW], S[KW], Lp[KW];
-                load_cost_words<KW>(scost + (r * kCostSlots + (uc & (kCostSlots - 1))) * Dp + off, Cw);
-#pragma unroll
-                for (int w = 0; w < KW; ++w) Cw[w] = scale_cost<WRAP>(Cw[w], a.costScale);
-                const uint8_t* irow = simg + (r + 1) * L.Wp;
-                const uint8_t* iprev = simg + r * L.Wp;
-                const int cur = irow[uc];
-                // H path (LR / RL).  The step runs on every lane of the warp (its
-                // shuffles need the whole warp; teams of one warp sit at different
-                // u); a path start only selects C instead of the step's result.
-                sgm_step<KW, WRAP, FULL, T>(LH, Cw, minH, p2lut[abs(cur - irow[max(uc - 1, 0)])],
-                                            a.p1x2, a.bsub, mk, Ln);
-                if (uc == 0) {
-#pragma unroll
-                    for (int w = 0; w < KW; ++w) Ln[w] = Cw[w] | mk.padMask[w];
-                }
-                const uint32_t mnH = warp_min_u16<KW, T>(Ln);
-                if (active) {
-#pragma unroll
-                    for (int w = 0; w < KW; ++w) LH[w] = Ln[w];
-                    minH = mnH;
-                }
-#pragma unroll
-                for (int w = 0; w < KW; ++w) S[w] = Ln[w];
-                // vertical-ish paths: 0 = V (u), 1 = D1 (u-1), 2 = D2 (u+1); NP = 1
-                // (4-path mode) runs V only
-                uint8_t* outSlot = sring + ((r * 3) * kRowSlots + (uc & (kRowSlots - 1))) * SB;
-                uint8_t* xout = oring + ((size_t)uc * 3) * SB;
-#pragma unroll
-                for (int pth = 0; pth < NP; ++pth) {
-                    const int pu = pth == 0 ? uc : (pth == 1 ? uc - 1 : uc + 1);
-                    const bool start = (v == 0) || pu < 0 || pu >= W;
-                    const int puc = min(max(pu, 0), W - 1);
-                    {
-                        // firstRow reads the previous band's row, other rows row r-1
-                        // (row 0 of band 0 starts every path: its slot is not read)
-                        const uint8_t* slot;
-                        if (firstRow) slot = sx + ((puc & (kXSlots - 1)) * 3 + pth) * SB;
-                        else slot = sring + (((max(r - 1, 0)) * 3 + pth) * kRowSlots + (puc & (kRowSlots - 1))) * SB;
-                        load_words<KW>(reinterpret_cast<const uint16_t*>(slot) + off, Lp);
-                        const uint32_t mp = *reinterpret_cast<const uint32_t*>(slot + 2 * Dp) & 0xFFFFu;
-                        sgm_step<KW, WRAP, FULL, T>(Lp, Cw, mp, p2lut[abs(cur - iprev[puc])], a.p1x2,
-                                                    a.bsub, mk, Ln);
-                    }
-                    if (start) {
-#pragma unroll
-                        for (int w = 0; w < KW; ++w) Ln[w] = Cw[w] | mk.padMask[w];
-                    }
-                    const uint32_t mn = warp_min_u16<KW, T>(Ln);
-                    if (active) {
-                        uint8_t* myslot = outSlot + pth * kRowSlots * SB;
-                        store_words<KW>(reinterpret_cast<uint16_t*>(myslot) + off, Ln);
-                        if (tl == 0) *reinterpret_cast<uint32_t*>(myslot + 2 * Dp) = mn;
-                        if (lastRow && hasNext) {
-                            uint8_t* xs = xout + pth * SB;
-                            store_words<KW>(reinterpret_cast<uint16_t*>(xs) + off, Ln);
-                            if (tl == 0) *reinterpret_cast<uint32_t*>(xs + 2 * Dp) = mn;
-                        }
-                    }
-#pragma unroll
-                    for (int w = 0; w < KW; ++w) S[w] = WRAP ? __vadd2(S[w], Ln[w]) : S[w] + Ln[w];
-                }
-                if (active) store_words<KW>(part + ((size_t)y * W + x) * Dp + off, S);
-            }
-            // ---- publish the band's last row to the next band ----
-            if (hasNext && active && lastRow && ((u % kPublish) == kPublish - 1 || u == W - 1)) {
-                __threadfence();
-                __syncwarp(teamMask);
-                if (tl == 0) st_release(oProd, oBase + (unsigned)u + 1u);
-            }
-            cp_async_wait<kLag - 1>();
-            __syncthreads();
-            // ---- consumer progress (copies of pixel s-kLag+1+kLag+1 = s+2 are complete) ----
-            if (warp == 0 && lane == 0 && hasPrev) {
-                const int done = s + 2;  // exchange pixels < done are in shared memory
-                if (done > 0 && ((done % kPublish) == 0 || done >= W)) st_release(pCons, pBase + (unsigned)min(done, W));
-            }
-            if (abortFlag) break;
-        }
-        cp_async_wait<0>();
-        __syncthreads();
-        if (abortFlag) return;
+static cudaError_t dispatch(const SweepArgs& a, SweepConfig c, bool wrap, bool diag, cudaStream_t s,
+                            int numSMs, int* g) {
+    switch (a.Dp) {
+    case 64: return sweep_dispatch_64(a, c.T, c.NW, wrap, diag, s, numSMs, g);
+    case 128: return sweep_dispatch_128(a, c.T, c.NW, wrap, diag, s, numSMs, g);
+    case 192: return sweep_dispatch_192(a, c.T, c.NW, wrap, diag, s, numSMs, g);
+    case 256: return sweep_dispatch_256(a, c.T, c.NW, wrap, diag, s, numSMs, g);
+    case 320: return sweep_dispatch_320(a, c.T, c.NW, wrap, diag, s, numSMs, g);
+    case 384: return sweep_dispatch_384(a, c.T, c.NW, wrap, diag, s, numSMs, g);
+    case 448: return sweep_dispatch_448(a, c.T, c.NW, wrap, diag, s, numSMs, g);
+    case 512: return sweep_dispatch_512(a, c.T, c.NW, wrap, diag, s, numSMs, g);
+    default: return cudaErrorInvalidValue;
     }
 }
 
-// ---------------------------------------------------------------------------
-// host side
-// ---------------------------------------------------------------------------
-template <int T, int KW, bool WRAP, bool FULL, int NW, int NP>
-static cudaError_t sweep_launch_t(SweepArgs a, cudaStream_t s, int numSMs, int* gridOut) {
-    auto kern = sweep_kernel<T, KW, WRAP, FULL, NW, NP>;
-    const SweepSmem L = sweep_smem(a.W, a.Dp, a.R);
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L.total);
-    if (e != cudaSuccess) return e;
-    int perSM = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kern, NW * 32, L.total);
-    if (e != cudaSuccess) return e;
-    if (perSM < 1) return cudaErrorInvalidConfiguration;
-    const int maxG = perSM * numSMs / 2;
-    a.G = std::min(a.nBands, maxG);
-    if (a.G < 1) return cudaErrorInvalidConfiguration;
-    *gridOut = 2 * a.G;
-    void* args[] = {&a};
-    return cudaLaunchCooperativeKernel((const void*)kern, dim3(2 * a.G), dim3(NW * 32), args,
-                                       (size_t)L.total, s);
-}
-
-// Lanes per pixel T and words per lane KW = Dp/(2T); NW warps per CTA.
-template <int T, int KW, int NW, int NP>
-static cudaError_t sweep_launch_np(SweepArgs a, bool wrap, cudaStream_t s, int numSMs, int* g) {
-    const bool full = (a.D == a.Dp);
-    if (wrap) return full ? sweep_launch_t<T, KW, true, true, NW, NP>(a, s, numSMs, g)
-                          : sweep_launch_t<T, KW, true, false, NW, NP>(a, s, numSMs, g);
-    return full ? sweep_launch_t<T, KW, false, true, NW, NP>(a, s, numSMs, g)
-                : sweep_launch_t<T, KW, false, false, NW, NP>(a, s, numSMs, g);
-}
-
-template <int T, int KW, int NW>
-static cudaError_t sweep_launch_kw(SweepArgs a, bool wrap, bool diag, cudaStream_t s, int numSMs,
-                                   int* g) {
-    return diag ? sweep_launch_np<T, KW, NW, 3>(a, wrap, s, numSMs, g)
-                : sweep_launch_np<T, KW, NW, 1>(a, wrap, s, numSMs, g);
-}
-
-size_t sweep_ring_bytes(int W, int Dp, int nBandsMax) {
-    return (size_t)2 * nBandsMax * W * 3 * (2 * Dp + 16);
-}
-
-int sweep_rows_per_band(int Dp) { return Dp <= 128 ? 16 : 8; }
-
-bool sweep_fits(int W, int Dp) {
-    int dev = 0, maxSmem = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&maxSmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    return sweep_smem(W, Dp, sweep_rows_per_band(Dp)).total + 1024 <= maxSmem;
-}
-
-cudaError_t launch_aggregate_sweep(const PairView& pv, uint16_t* partB, const SgmConsts& k,
-                                   bool wrap, bool diag, uint8_t* xring, unsigned* counters,
-                                   int* status, long long spinMax, cudaStream_t s, int numSMs) {
-    SweepArgs a;
+static SweepArgs make_args(const PairView& pv, uint16_t* partB, const SgmConsts& k, SweepConfig c) {
+    SweepArgs a{};
     a.cost = pv.cost;
     a.img = pv.img;
     a.part[0] = pv.agg;
     a.part[1] = partB;
-    a.xring = xring;
     a.W = k.W; a.H = k.H; a.D = k.D; a.Dp = k.Dp;
     a.P1 = k.P1; a.P2 = k.P2; a.costScale = k.costScale;
     a.p1x2 = k.p1x2; a.bsub = k.bsub;
-    a.R = sweep_rows_per_band(k.Dp);
+    a.R = c.NW * 32 / c.T;
     a.nBands = (k.H + a.R - 1) / a.R;
     a.G = a.nBands;
-    a.prod = counters;
-    a.cons = counters + 2 * a.nBands;
-    a.status = status;
     a.slotBytes = 2 * k.Dp + 16;
-    a.spinMax = spinMax;
-    cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned) * 4 * a.nBands, s);
+    return a;
+}
+
+bool sweep_fits(int W, int Dp, SweepConfig c) {
+    int dev = 0, maxSmem = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&maxSmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return sweep_smem(W, Dp, c.NW * 32 / c.T).total + 1024 <= maxSmem;
+}
+
+cudaError_t sweep_plan(const PairView& pv, const SgmConsts& k, SweepConfig c, bool wrap, bool diag,
+                       int numSMs, SweepPlan* plan) {
+    SweepArgs a = make_args(pv, nullptr, k, c);
+    a.plan = 1;
+    int G = 0;
+    cudaError_t e = dispatch(a, c, wrap, diag, nullptr, numSMs, &G);
     if (e != cudaSuccess) return e;
-    int grid = 0;
-    switch (k.Dp) {
-    case 64: return sweep_launch_kw<8, 4, 4>(a, wrap, diag, s, numSMs, &grid);    // R = 16
-    case 128: return sweep_launch_kw<8, 8, 4>(a, wrap, diag, s, numSMs, &grid);   // R = 16
-    case 192: return sweep_launch_kw<16, 6, 4>(a, wrap, diag, s, numSMs, &grid);  // R = 8
-    case 256: return sweep_launch_kw<16, 8, 4>(a, wrap, diag, s, numSMs, &grid);  // R = 8
-    case 320: return sweep_launch_kw<32, 5, 8>(a, wrap, diag, s, numSMs, &grid);  // R = 8
-    case 384: return sweep_launch_kw<32, 6, 8>(a, wrap, diag, s, numSMs, &grid);
-    case 448: return sweep_launch_kw<32, 7, 8>(a, wrap, diag, s, numSMs, &grid);
-    case 512: return sweep_launch_kw<32, 8, 8>(a, wrap, diag, s, numSMs, &grid);
-    default: return cudaErrorInvalidValue;
-    }
+    plan->G = G;
+    plan->nBands = a.nBands;
+    // one wave (every band resident): small rings with back-pressure; otherwise
+    // a full row per ring so that a producer never waits inside its band
+    plan->K = (G == a.nBands) ? std::min(k.W, 128) : k.W;
+    plan->ringBytes = (size_t)2 * G * plan->K * 3 * (2 * k.Dp + 16);
+    plan->counterWords = (size_t)4 * G;
+    return cudaSuccess;
+}
+
+cudaError_t launch_aggregate_sweep(const PairView& pv, uint16_t* partB, const SgmConsts& k,
+                                   bool wrap, bool diag, SweepConfig c, const SweepPlan& plan,
+                                   uint8_t* xring, unsigned* counters, int* status,
+                                   long long spinMax, cudaStream_t s, int numSMs) {
+    SweepArgs a = make_args(pv, partB, k, c);
+    a.xring = xring;
+    a.prod = counters;
+    a.cons = counters + 2 * plan.G;
+    a.status = status;
+    a.K = plan.K;
+    a.spinMax = spinMax;
+    a.plan = 0;
+    cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned) * plan.counterWords, s);
+    if (e != cudaSuccess) return e;
+    int G = 0;
+    e = dispatch(a, c, wrap, diag, s, numSMs, &G);
+    if (e == cudaSuccess && G != plan.G) return cudaErrorInvalidConfiguration;
+    return e;
 }
 
 }  // namespace lumen

@@ -116,6 +116,52 @@ def test_parity_small(name, schedule, oracle_mod):
                 else params_dict(**over), left, right, oracle_mod, schedule=schedule)
 
 
+SWEEP_CONFIGS = {64: [(32, 4), (32, 8), (16, 4), (8, 4), (8, 2)],
+                 128: [(32, 4), (32, 8), (16, 4), (8, 4), (8, 2)],
+                 192: [(32, 4), (32, 8), (16, 4)], 320: [(32, 4), (32, 8)]}
+
+
+@pytest.mark.parametrize("D,cfg", [(d, c) for d in (40, 128, 150, 290) for c in
+                                   SWEEP_CONFIGS[(d + 63) // 64 * 64]])
+def test_parity_sweep_configs(D, cfg, oracle_mod):
+    """Every compiled sweep configuration (lanes per pixel, warps per block)
+    reproduces the oracle bit for bit, both cost modes, 4 and 8 paths."""
+    left, right, _ = synth.make_pair(synth.PairSpec(150, 70, 4, 1, min(D - 1, 40), 2.0, 60 + D))
+    for mode, nd in ((0, 8), (1, 4)):
+        pd = params_dict(maxDisparity=D, numDirections=nd, matchingCostMode=mode,
+                         speckleWindowSize=0)
+        p = to_params(pd)
+        with StereoSGBM(p) as s:
+            s.set_schedule(2)
+            s.set_tuning(*cfg)
+            s.retain_intermediates(True)
+            disp = s.compute(left, right)
+            agg = s.intermediate("agg", (70, 150, D), np.uint16)
+            assert s.get_tuning() == (2, cfg[0], cfg[1])
+        ref_disp, ref = oracle_mod.sgbm(pd, left, right, intermediates=True)
+        assert np.array_equal(agg, ref["agg"]), (mode, nd)
+        assert_subpix_close(disp, ref_disp)
+
+
+def test_autotune_and_cache(tmp_path):
+    torch = pytest.importorskip("torch")
+    left, right, _ = synth.make_pair(synth.PairSpec(320, 180, 5, 4, 40, 2.0, 90))
+    p = StereoParams(maxDisparity=64, numDirections=8, speckleWindowSize=0)
+    dl = torch.from_numpy(left).cuda()
+    dr = torch.from_numpy(right).cuda()
+    with StereoSGBM(p) as s:
+        ref = s.compute(left, right).copy()
+        rep = s.autotune(dl.data_ptr(), dr.data_ptr(), 320, 180)
+        assert "best schedule=" in rep
+        assert np.array_equal(s.compute(left, right), ref)  # uses the tuned choice
+        path = str(tmp_path / "tune.txt")
+        s.save_tuning(path)
+    with StereoSGBM(p) as s2:
+        s2.load_tuning(path)
+        assert np.array_equal(s2.compute(left, right), ref)
+    assert open(path).read().strip()
+
+
 @pytest.mark.parametrize("k", range(8))
 def test_parity_single_path(k, oracle_mod):
     left, right = synth.random_pair(70, 45, seed=40 + k, shift=4)
