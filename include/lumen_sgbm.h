@@ -113,11 +113,13 @@ const char* lumen_last_error_string(void);
  * the numDirections default. */
 lumen_status lumen_sgbm_debug_set_paths(lumen_sgbm* h, uint32_t path_mask);
 /* Aggregation schedule: 0 = automatic (autotuner / heuristic), 1 = one kernel
- * per direction, 2 = two fused wavefront sweeps.  Values, not outputs, are the
- * same for every schedule. */
+ * per direction, 2 = two fused wavefront sweeps (rows of a band in lockstep),
+ * 3 = two fused wavefront sweeps with decoupled row warps and ticket-ordered
+ * bands.  Outputs are identical for every schedule. */
 lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule);
 /* Pin the fused-sweep configuration: lanes per pixel (8, 16 or 32) and warps
- * per thread block (2, 4 or 8; rows per band = warps * 32 / lanes).  0, 0
+ * per thread block (2, 4 or 8; rows per band = warps * 32 / lanes).  Schedule 3
+ * uses 32 lanes and takes `warps` (4 or 8) as its rows per band.  0, 0
  * restores the automatic choice.  Values are identical for every setting. */
 lumen_status lumen_sgbm_set_tuning(lumen_sgbm* h, int lanes_per_pixel, int warps_per_block);
 /* The schedule and configuration the last compute used: {schedule, lanes, warps}. */
@@ -143,6 +145,12 @@ lumen_status lumen_sgbm_debug_retain(lumen_sgbm* h, int enable);
 lumen_status lumen_sgbm_debug_copy(lumen_sgbm* h, int which, void* dst, size_t dst_bytes);
 /* Number of kernels this handle has enqueued so far (all computes). */
 unsigned long long lumen_sgbm_debug_launch_count(const lumen_sgbm* h);
+/* Iteration limit of every device-side wait (0 restores the default, 2^22). */
+lumen_status lumen_sgbm_debug_set_wait_limit(lumen_sgbm* h, long long spins);
+/* Failure-path self test of schedule 3: while enabled, one wait of the first
+ * band can never be satisfied, so it runs out after the wait limit and the
+ * compute returns LUMEN_ERR_TIMEOUT (no fault, no hang; the handle stays usable). */
+lumen_status lumen_sgbm_debug_stall_test(lumen_sgbm* h, int enable);
 
 /* ---- rectification remap (replaces stereo::StereoRectifier,
  * include/stereo/rectification.h:41-84, and rectifyImageGPU :92-97) ---- */

@@ -242,6 +242,14 @@ class StereoSGBM:
     def set_schedule(self, schedule: int) -> None:
         _check(_lib.lib().lumen_sgbm_set_schedule(self._h, schedule))
 
+    def set_wait_limit(self, spins: int = 0) -> None:
+        """Iteration limit of the device-side waits (0 = default)."""
+        _check(_lib.lib().lumen_sgbm_debug_set_wait_limit(self._h, spins))
+
+    def stall_test(self, enable: bool = True) -> None:
+        """Make one device-side wait of schedule 3 unsatisfiable (failure-path test)."""
+        _check(_lib.lib().lumen_sgbm_debug_stall_test(self._h, 1 if enable else 0))
+
     def set_tuning(self, lanes_per_pixel: int = 0, warps_per_block: int = 0) -> None:
         """Pin the fused-sweep configuration (0, 0 = automatic)."""
         _check(_lib.lib().lumen_sgbm_set_tuning(self._h, lanes_per_pixel, warps_per_block))

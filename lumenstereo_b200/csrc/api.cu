@@ -80,6 +80,7 @@ struct lumen_sgbm {
     DevBuf partB, xring, counters, status;  // sweep schedule: backward partial, exchange rings
     int numSMs = 148;
     long long spinMax = 1ll << 22;          // bounded device-side waits
+    int stallTest = 0;                      // lumen_sgbm_debug_stall_test
     bool statusPending = false;
     SweepConfig forced{0, 0};               // lumen_sgbm_set_tuning (0 = automatic)
     std::map<std::string, std::pair<int, SweepConfig>> tuned;  // key -> (schedule, config)
@@ -240,6 +241,19 @@ extern "C" lumen_status lumen_sgbm_get_timings(lumen_sgbm* h, float out[4]) {
     return LUMEN_OK;
 }
 
+extern "C" lumen_status lumen_sgbm_debug_set_wait_limit(lumen_sgbm* h, long long spins) {
+    if (!h) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL handle");
+    if (spins < 0) return fail(LUMEN_ERR_INVALID_ARGUMENT, "wait limit must be >= 0");
+    h->spinMax = spins ? spins : (1ll << 22);
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_sgbm_debug_stall_test(lumen_sgbm* h, int enable) {
+    if (!h) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL handle");
+    h->stallTest = enable ? 1 : 0;
+    return LUMEN_OK;
+}
+
 extern "C" unsigned long long lumen_sgbm_debug_launch_count(const lumen_sgbm* h) {
     return h ? h->launches : 0ull;
 }
@@ -252,7 +266,8 @@ extern "C" lumen_status lumen_sgbm_debug_set_paths(lumen_sgbm* h, uint32_t mask)
 
 extern "C" lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule) {
     if (!h) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL handle");
-    if (schedule < 0 || schedule > 2) return fail(LUMEN_ERR_INVALID_ARGUMENT, "schedule must be 0, 1 or 2");
+    if (schedule < 0 || schedule > 3)
+        return fail(LUMEN_ERR_INVALID_ARGUMENT, "schedule must be 0, 1, 2 or 3");
     h->schedule = schedule;
     return LUMEN_OK;
 }
@@ -427,10 +442,36 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
         }
     }
     if (sched == 0) sched = sweepable ? 2 : 1;
-    if (sched == 2 && !sweepable) sched = 1;          // single-path debug masks: per-direction kernels
+    if (sched >= 2 && !sweepable) sched = 1;          // single-path debug masks: per-direction kernels
+    Sweep2Plan plan2{};
+    if (sched == 3) {
+        const int R = (cfg.T == 32 && (cfg.NW == 4 || cfg.NW == 8)) ? cfg.NW : 8;
+        if (sweep2_plan(k, R, wrap, mask == 0xFFu, h->numSMs, &plan2) == cudaSuccess) {
+            cfg = SweepConfig{32, R};
+        } else {
+            sched = 2;
+            cfg = sweep_default_config(Dp, wrap);
+        }
+    }
     if (sched == 2 && !sweep_fits(W, Dp, cfg)) sched = 1;  // very wide images: per-direction kernels
     const uint16_t* aggB = nullptr;
-    if (sched == 2) {
+    if (sched == 3) {
+        LCU(h->partB.ensure(ND * 2));
+        LCU(h->xring.ensure(plan2.ringBytes));
+        LCU(h->counters.ensure(sizeof(unsigned) * plan2.counterWords));
+        LCU(launch_aggregate_sweep2(pv, h->partB.as<uint16_t>(), k, wrap, mask == 0xFFu, plan2,
+                                    h->xring.as<uint8_t>(), h->counters.as<unsigned>(),
+                                    h->status.as<int>(), h->spinMax, s, h->stallTest));
+        h->statusPending = true;
+        nl += 1;
+        aggB = h->partB.as<uint16_t>();
+        if (h->retain || select_needs_summed_volume(D, Dp)) {
+            launch_sum_volumes(h->agg.as<uint16_t>(), aggB, h->agg.as<uint16_t>(), ND, s);
+            LCU(cudaGetLastError());
+            nl += 1;
+            aggB = nullptr;
+        }
+    } else if (sched == 2) {
         SweepPlan plan;
         cudaError_t pe = sweep_plan(pv, k, cfg, wrap, mask == 0xFFu, h->numSMs, &plan);
         if (pe != cudaSuccess) {  // this configuration cannot serve these parameters
@@ -457,7 +498,7 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
         nl += __builtin_popcount(mask);
     }
     h->lastSchedule = sched;
-    h->lastConfig = sched == 2 ? cfg : SweepConfig{0, 0};
+    h->lastConfig = sched >= 2 ? cfg : SweepConfig{0, 0};
     if (timed) LCU(cudaEventRecord(h->ev[3], s));
     // selection + post-processing
     LCU(launch_select(h->agg.as<uint16_t>(), aggB, wrap, W, H, D, Dp, p.minDisparity,
@@ -555,6 +596,9 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
             if (!sweep_fits(width, Dp, cs[i])) continue;
             cands.push_back({2, cs[i]});
         }
+        int rs[4];
+        const int nr = sweep2_rows_options(Dp, rs, 4);
+        for (int i = 0; i < nr; ++i) cands.push_back({3, SweepConfig{32, rs[i]}});
     }
     const SweepConfig savedForced = h->forced;
     const int savedSched = h->schedule;

@@ -49,6 +49,24 @@ cudaError_t launch_aggregate_sweep(const PairView& pv, uint16_t* partB, const Sg
                                    uint8_t* xring, unsigned* counters, int* status,
                                    long long spinMax, cudaStream_t s, int numSMs);
 
+// ---- schedule 3: decoupled-row fused sweeps (sweep2.cu, sweep2_kernel.cuh) ----
+struct Sweep2Plan {
+    int R;                 // rows per band (warps per CTA = R + 2)
+    int QB;                // import / last-row ring slots
+    int nBands;            // bands per sweep
+    int M;                 // exchange rows per sweep
+    int grid;              // CTAs launched (persistent, ticket-scheduled)
+    int smem;              // dynamic shared memory per CTA
+    size_t ringBytes;      // exchange rows, both sweeps
+    size_t counterWords;   // prod + cons + ticket
+};
+int sweep2_rows_options(int Dp, int* out, int max);
+cudaError_t sweep2_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSMs, Sweep2Plan* plan);
+cudaError_t launch_aggregate_sweep2(const PairView& pv, uint16_t* partB, const SgmConsts& k,
+                                    bool wrap, bool diag, const Sweep2Plan& plan, uint8_t* xring,
+                                    unsigned* counters, int* status, long long spinMax,
+                                    cudaStream_t s, int stallTest = 0);
+
 // aggB (nullable): second partial volume summed with agg (mod 2^16 when wrap).
 cudaError_t launch_select(const uint16_t* agg, const uint16_t* aggB, bool wrap, int W, int H,
                           int D, int Dp, int minD, int UR, int16_t* dispL, int16_t* dispR,

@@ -14,6 +14,7 @@ import numpy as np
 import pytest
 
 from lumenstereo_b200 import (MatchingCostMode, StereoException, StereoParams, StereoSGBM,
+                              TimeoutException,
                               bgr_to_gray, kSgbmMaxDisparityRange, rectify_image_gpu, synth)
 from tests.conftest import params_dict
 
@@ -103,7 +104,7 @@ CASES = {
 }
 
 
-@pytest.mark.parametrize("schedule", [1, 2])
+@pytest.mark.parametrize("schedule", [1, 2, 3])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_parity_small(name, schedule, oracle_mod):
     w, h, over = CASES[name]
@@ -141,6 +142,49 @@ def test_parity_sweep_configs(D, cfg, oracle_mod):
         ref_disp, ref = oracle_mod.sgbm(pd, left, right, intermediates=True)
         assert np.array_equal(agg, ref["agg"]), (mode, nd)
         assert_subpix_close(disp, ref_disp)
+
+
+@pytest.mark.parametrize("rows", [4, 8])
+@pytest.mark.parametrize("D", [40, 128, 150, 290, 512])
+def test_parity_schedule3_rows(D, rows, oracle_mod):
+    """The decoupled-row sweeps (schedule 3) at both band heights reproduce the
+    oracle bit for bit, both cost modes, 4 and 8 paths, odd image sizes."""
+    left, right, _ = synth.make_pair(synth.PairSpec(131, 37, 4, 1, min(D - 1, 40), 2.0, 70 + D))
+    for mode, nd in ((0, 8), (1, 4), (1, 8)):
+        pd = params_dict(maxDisparity=D, numDirections=nd, matchingCostMode=mode,
+                         speckleWindowSize=0)
+        with StereoSGBM(to_params(pd)) as s:
+            s.set_schedule(3)
+            s.set_tuning(32, rows)
+            s.retain_intermediates(True)
+            disp = s.compute(left, right)
+            agg = s.intermediate("agg", (37, 131, D), np.uint16)
+            used = s.get_tuning()
+        if not (D == 512 and rows == 8 and nd == 8):  # too large for shared memory: falls back
+            assert used == (3, 32, rows), used
+        ref_disp, ref = oracle_mod.sgbm(pd, left, right, intermediates=True)
+        assert np.array_equal(agg, ref["agg"]), (mode, nd)
+        assert_subpix_close(disp, ref_disp)
+
+
+def test_schedule3_timeout_reports_error():
+    """A device-side wait that runs out ends the launch with a timeout status,
+    not a hang: one wait of the first band is made unsatisfiable and the wait
+    limit is cut, so the launch gives up quickly; the handle then recovers."""
+    left, right = synth.random_pair(300, 64, seed=3)
+    p = StereoParams(maxDisparity=64, numDirections=8, speckleWindowSize=0)
+    with StereoSGBM(p) as s:
+        s.set_schedule(3)
+        s.set_wait_limit(1 << 14)
+        s.stall_test(True)
+        with pytest.raises(TimeoutException):
+            s.compute(left, right)
+        s.stall_test(False)
+        s.set_wait_limit(0)
+        ref = s.compute(left, right)
+    with StereoSGBM(p) as s:
+        s.set_schedule(1)
+        assert np.array_equal(s.compute(left, right), ref)
 
 
 def test_autotune_and_cache(tmp_path):
@@ -254,15 +298,16 @@ def test_schedules_agree_full_size(wl):
                      matchingCostMode=MatchingCostMode.Census if w.census else MatchingCostMode.SAD,
                      speckleWindowSize=0)
     outs = []
-    for schedule in (1, 2):
+    for schedule in (1, 2, 3):
         with StereoSGBM(p) as s:
             s.set_schedule(schedule)
             s.retain_intermediates(True)
             d = s.compute(left, right)
             agg = s.intermediate("agg", left.shape + (w.max_disparity,), np.uint16)
             outs.append((d, agg))
-    assert np.array_equal(outs[0][1], outs[1][1])
-    assert np.array_equal(outs[0][0], outs[1][0])
+    for k in (1, 2):
+        assert np.array_equal(outs[0][1], outs[k][1]), k
+        assert np.array_equal(outs[0][0], outs[k][0]), k
 
 
 def test_deterministic_and_handle_reuse():
@@ -330,7 +375,7 @@ def test_parity_vs_reference_kernels_full_size(wl, oracle_mod):
     p = params_dict(maxDisparity=w.max_disparity, matchingCostMode=int(w.census),
                     numDirections=w.num_directions, speckleWindowSize=0)
     ref_disp, ref, _ = oracle_mod.ref_sgbm(p, left, right, intermediates=False)
-    for schedule in (1, 2):
+    for schedule in (1, 2, 3):
         ours, inter = run_ours_light(p, left, right, schedule)
         assert np.array_equal(ours, ref_disp), schedule
     # sanity: the scene's disparities are recovered
@@ -356,7 +401,7 @@ def test_parity_vs_reference_kernels_intermediates(oracle_mod):
         p = params_dict(maxDisparity=64, matchingCostMode=mode, numDirections=nd,
                         uniquenessRatio=ur, speckleWindowSize=0)
         ref_disp, ref, _ = oracle_mod.ref_sgbm(p, left, right, intermediates=True)
-        for schedule in (1, 2):
+        for schedule in (1, 2, 3):
             disp, ours = run_ours(p, left, right, schedule=schedule)
             for key in ("cost", "agg", "disp_wta", "disp_right", "disp_lr"):
                 assert np.array_equal(ours[key], ref[key]), (mode, nd, key, schedule)
