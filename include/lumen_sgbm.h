@@ -182,6 +182,27 @@ lumen_status lumen_remap(const uint8_t* src, const float* map_x, const float* ma
 lumen_status lumen_bgr_to_gray(const uint8_t* bgr, size_t stride, uint8_t* gray, int width,
                                int height);
 
+/* ---- Census cost volume without device allocation.  No counterpart in the
+ * reference: it serves callers that cannot call cudaMalloc (a real-time loop
+ * that must not take cudaMalloc's implicit device synchronisation, a plugin host
+ * whose pool owns all device memory, work built inside a stream capture). ----
+ *
+ * Census 5x5 descriptors of both DEVICE images (gray, width*height bytes, pitch
+ * width) and the uint8 cost volume d_cost[(y*width + x)*cost_stride + d], the
+ * values of the Census stage of lumen_sgbm_compute (entries d >= maxDisparity -
+ * minDisparity are 0).  cost_stride: a multiple of 16, >= the disparity range.
+ * Asynchronous on `stream` (NULL = the default stream).  The descriptors live
+ * in a fixed 16 MiB array inside the library (held by every GPU that loads it
+ * until exit): images above lumen_census_cost_noalloc_max_pixels() pixels
+ * (2^21, so 1920x1080 fits) return LUMEN_ERR_OUT_OF_BUDGET.  The first call on
+ * a device looks up that array's device address (make it before any stream
+ * capture).  All calls share the array: calls whose work overlaps on the GPU
+ * race and must be serialised. */
+lumen_status lumen_census_cost_noalloc(const uint8_t* d_left, const uint8_t* d_right, int width,
+                                       int height, int min_disparity, int max_disparity,
+                                       uint8_t* d_cost, int cost_stride, void* stream);
+size_t lumen_census_cost_noalloc_max_pixels(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -67,6 +67,8 @@ def _declare(lib):
         "lumen_rectifier_rectify_device": (i, [vp, vp, vp, i, vp, vp, vp]),
         "lumen_remap": (i, [vp, vp, vp, vp, i, i, i]),
         "lumen_bgr_to_gray": (i, [vp, sz, vp, i, i]),
+        "lumen_census_cost_noalloc": (i, [vp, vp, i, i, i, i, vp, i, vp]),
+        "lumen_census_cost_noalloc_max_pixels": (sz, []),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

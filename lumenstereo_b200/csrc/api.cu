@@ -71,6 +71,10 @@ __global__ void magic_kernel(uint32_t* m, int n) {
 
 }  // namespace
 
+// Records `msg` as this thread's last error (lumen_last_error_string) for
+// entry points defined in other translation units.
+lumen_status lumen::set_error(lumen_status s, const std::string& msg) { return fail(s, msg); }
+
 struct lumen_sgbm {
     lumen_stereo_params params{};
     int device = 0;

@@ -1,8 +1,14 @@
 // kernels.cuh -- launchers of the B200 SGBM kernels (host-callable).
 #pragma once
+#include <string>
+
+#include "../../include/lumen_sgbm.h"
 #include "common.cuh"
 
 namespace lumen {
+
+// Records `msg` as the calling thread's last error and returns `s` (api.cu).
+lumen_status set_error(lumen_status s, const std::string& msg);
 
 // Number of path lines of direction dir (LR, RL, TB, BT, TLBR, BRTL, TRBL, BLTR).
 __host__ __device__ inline int num_lines(int dir, int W, int H) {
