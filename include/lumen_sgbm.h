@@ -115,12 +115,15 @@ lumen_status lumen_sgbm_debug_set_paths(lumen_sgbm* h, uint32_t path_mask);
 /* Aggregation schedule: 0 = automatic (autotuner / heuristic), 1 = one kernel
  * per direction, 2 = two fused wavefront sweeps (rows of a band in lockstep),
  * 3 = two fused wavefront sweeps with decoupled row warps and ticket-ordered
- * bands.  Outputs are identical for every schedule. */
+ * bands, 4 = two fused wavefront sweeps with lockstep row bands and helper
+ * warps for the band hand-offs (the default).  Outputs are identical for
+ * every schedule. */
 lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule);
 /* Pin the fused-sweep configuration: lanes per pixel (8, 16 or 32) and warps
- * per thread block (2, 4 or 8; rows per band = warps * 32 / lanes).  Schedule 3
- * uses 32 lanes and takes `warps` (4 or 8) as its rows per band.  0, 0
- * restores the automatic choice.  Values are identical for every setting. */
+ * per thread block (2, 4, 8 or 16; rows per band = warps * 32 / lanes).
+ * Schedules 3 and 4 use 32 lanes and take `warps` as their rows per band
+ * (schedule 3: 4 or 8; schedule 4: 4, 8 or 16).  0, 0 restores the automatic
+ * choice.  Values are identical for every setting. */
 lumen_status lumen_sgbm_set_tuning(lumen_sgbm* h, int lanes_per_pixel, int warps_per_block);
 /* The schedule and configuration the last compute used: {schedule, lanes, warps}. */
 lumen_status lumen_sgbm_get_tuning(const lumen_sgbm* h, int out[3]);
@@ -143,6 +146,15 @@ lumen_status lumen_sgbm_tuning_load(lumen_sgbm* h, const char* path);
  * pixel.  The debug-retain flag must have been set before the compute. */
 lumen_status lumen_sgbm_debug_retain(lumen_sgbm* h, int enable);
 lumen_status lumen_sgbm_debug_copy(lumen_sgbm* h, int which, void* dst, size_t dst_bytes);
+/* Band timeline of the lockstep row-band sweeps (schedule 4) for the next
+ * computes (enable = 1) or off (0).  lumen_sgbm_debug_trace_copy returns the
+ * last such launch's records, 4 words per band ticket t (t = 2*band + sweep):
+ * globaltimer ns when the band was taken, when its first step began, when it
+ * ended, and SM id << 48 | import polls << 32 | export polls << 16 | cost
+ * chunk polls.  *words receives the record size; dst may be NULL to query it. */
+lumen_status lumen_sgbm_debug_trace(lumen_sgbm* h, int enable);
+lumen_status lumen_sgbm_debug_trace_copy(lumen_sgbm* h, unsigned long long* dst,
+                                         size_t dst_words, size_t* words);
 /* Number of kernels this handle has enqueued so far (all computes). */
 unsigned long long lumen_sgbm_debug_launch_count(const lumen_sgbm* h);
 /* Iteration limit of every device-side wait (0 restores the default, 2^22). */

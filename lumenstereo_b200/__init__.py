@@ -275,6 +275,22 @@ class StereoSGBM:
     def load_tuning(self, path: str) -> None:
         _check(_lib.lib().lumen_sgbm_tuning_load(self._h, path.encode()))
 
+    def enable_trace(self, enable: bool = True) -> None:
+        """Record the band timeline of the lockstep row-band sweeps (schedule 4)."""
+        _check(_lib.lib().lumen_sgbm_debug_trace(self._h, int(enable)))
+
+    def trace(self) -> np.ndarray:
+        """Band timeline of the last schedule-4 launch: one row per band ticket
+        (2*band + sweep): [taken_ns, first_step_ns, end_ns, sm << 48 | import
+        polls << 32 | export polls << 16 | cost-chunk polls]."""
+        lib = _lib.lib()
+        n = C.c_size_t(0)
+        _check(lib.lumen_sgbm_debug_trace_copy(self._h, None, 0, C.byref(n)))
+        out = np.zeros(max(n.value, 4), dtype=np.uint64)
+        if n.value:
+            _check(lib.lumen_sgbm_debug_trace_copy(self._h, out.ctypes.data, n.value, C.byref(n)))
+        return out[: n.value].reshape(-1, 4)
+
     def launch_count(self) -> int:
         """Kernels this handle has enqueued so far."""
         return int(_lib.lib().lumen_sgbm_debug_launch_count(self._h))

@@ -60,6 +60,8 @@ def _declare(lib):
         "lumen_sgbm_debug_retain": (i, [vp, i]),
         "lumen_sgbm_debug_copy": (i, [vp, i, vp, sz]),
         "lumen_sgbm_debug_launch_count": (C.c_ulonglong, [vp]),
+        "lumen_sgbm_debug_trace": (i, [vp, i]),
+        "lumen_sgbm_debug_trace_copy": (i, [vp, vp, sz, C.POINTER(sz)]),
         "lumen_rectifier_create": (i, [i, i, vp, vp, vp, vp, C.POINTER(vp)]),
         "lumen_rectifier_destroy": (i, [vp]),
         "lumen_rectifier_is_pre_rectified": (i, [vp]),

@@ -82,6 +82,9 @@ struct lumen_sgbm {
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     DevBuf inL, inR, gray[2], pref[2], census[2], cost, agg, dispL, dispR, out, dbgLR, magic;
     DevBuf partB, xring, counters, status;  // sweep schedule: backward partial, exchange rings
+    DevBuf trace;                           // lumen_sgbm_debug_trace: band timeline of schedule 4
+    int traceOn = 0;
+    size_t traceWords = 0;
     int numSMs = 148;
     long long spinMax = 1ll << 22;          // bounded device-side waits
     int stallTest = 0;                      // lumen_sgbm_debug_stall_test
@@ -181,7 +184,7 @@ extern "C" lumen_status lumen_sgbm_destroy(lumen_sgbm* h) {
     for (DevBuf* b : {&h->inL, &h->inR, &h->gray[0], &h->gray[1], &h->pref[0], &h->pref[1],
                       &h->census[0], &h->census[1], &h->cost, &h->agg, &h->dispL, &h->dispR,
                       &h->out, &h->dbgLR, &h->magic, &h->partB, &h->xring, &h->counters,
-                      &h->status})
+                      &h->status, &h->trace})
         b->release();
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
@@ -258,6 +261,24 @@ extern "C" lumen_status lumen_sgbm_debug_stall_test(lumen_sgbm* h, int enable) {
     return LUMEN_OK;
 }
 
+extern "C" lumen_status lumen_sgbm_debug_trace(lumen_sgbm* h, int enable) {
+    if (!h) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL handle");
+    h->traceOn = enable ? 1 : 0;
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_sgbm_debug_trace_copy(lumen_sgbm* h, unsigned long long* dst,
+                                                    size_t dst_words, size_t* words) {
+    if (!h || !words) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL argument");
+    *words = h->traceWords;
+    if (!dst || !h->traceWords) return LUMEN_OK;
+    if (dst_words < h->traceWords) return fail(LUMEN_ERR_INVALID_ARGUMENT, "destination too small");
+    LCU(cudaStreamSynchronize(h->stream));
+    LCU(cudaDeviceSynchronize());
+    LCU(cudaMemcpy(dst, h->trace.p, h->traceWords * 8, cudaMemcpyDeviceToHost));
+    return LUMEN_OK;
+}
+
 extern "C" unsigned long long lumen_sgbm_debug_launch_count(const lumen_sgbm* h) {
     return h ? h->launches : 0ull;
 }
@@ -270,8 +291,8 @@ extern "C" lumen_status lumen_sgbm_debug_set_paths(lumen_sgbm* h, uint32_t mask)
 
 extern "C" lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule) {
     if (!h) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL handle");
-    if (schedule < 0 || schedule > 3)
-        return fail(LUMEN_ERR_INVALID_ARGUMENT, "schedule must be 0, 1, 2 or 3");
+    if (schedule < 0 || schedule > 4)
+        return fail(LUMEN_ERR_INVALID_ARGUMENT, "schedule must be 0, 1, 2, 3 or 4");
     h->schedule = schedule;
     return LUMEN_OK;
 }
@@ -282,8 +303,8 @@ extern "C" lumen_status lumen_sgbm_set_tuning(lumen_sgbm* h, int lanes, int warp
         h->forced = SweepConfig{0, 0};
         return LUMEN_OK;
     }
-    if (!(lanes == 8 || lanes == 16 || lanes == 32) || !(warps == 2 || warps == 4 || warps == 8))
-        return fail(LUMEN_ERR_INVALID_ARGUMENT, "lanes must be 8/16/32 and warps 2/4/8");
+    if (!(lanes == 8 || lanes == 16 || lanes == 32) || !(warps == 2 || warps == 4 || warps == 8 || warps == 16))
+        return fail(LUMEN_ERR_INVALID_ARGUMENT, "lanes must be 8/16/32 and warps 2/4/8/16");
     h->forced = SweepConfig{lanes, warps};
     return LUMEN_OK;
 }
@@ -445,8 +466,20 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
             cfg = it->second.second;
         }
     }
-    if (sched == 0) sched = sweepable ? 2 : 1;
+    if (sched == 0) sched = sweepable ? 4 : 1;
     if (sched >= 2 && !sweepable) sched = 1;          // single-path debug masks: per-direction kernels
+    WavePlan plan4{};
+    if (sched == 4) {
+        const int R = (cfg.T == 32 && (cfg.NW == 4 || cfg.NW == 8 || cfg.NW == 16)) ? cfg.NW : 8;
+        if (wave_plan(k, R, wrap, mask == 0xFFu, h->numSMs, &plan4) == cudaSuccess ||
+            wave_plan(k, 8, wrap, mask == 0xFFu, h->numSMs, &plan4) == cudaSuccess ||
+            wave_plan(k, 4, wrap, mask == 0xFFu, h->numSMs, &plan4) == cudaSuccess) {
+            cfg = SweepConfig{32, plan4.R};  // lanes per pixel, rows per band
+        } else {
+            sched = 3;
+            cfg = sweep_default_config(Dp, wrap);
+        }
+    }
     Sweep2Plan plan2{};
     if (sched == 3) {
         const int R = (cfg.T == 32 && (cfg.NW == 4 || cfg.NW == 8)) ? cfg.NW : 8;
@@ -459,7 +492,30 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
     }
     if (sched == 2 && !sweep_fits(W, Dp, cfg)) sched = 1;  // very wide images: per-direction kernels
     const uint16_t* aggB = nullptr;
-    if (sched == 3) {
+    if (sched == 4) {
+        LCU(h->partB.ensure(ND * 2));
+        LCU(h->xring.ensure(plan4.ringBytes));
+        LCU(h->counters.ensure(sizeof(unsigned) * plan4.counterWords));
+        unsigned long long* trace = nullptr;
+        if (h->traceOn) {
+            h->traceWords = 4 * 2 * (size_t)plan4.nBands;
+            LCU(h->trace.ensure(h->traceWords * 8));
+            LCU(cudaMemsetAsync(h->trace.p, 0, h->traceWords * 8, s));
+            trace = h->trace.as<unsigned long long>();
+        }
+        LCU(launch_aggregate_wave(pv, h->partB.as<uint16_t>(), k, wrap, mask == 0xFFu, plan4,
+                                  h->xring.as<uint8_t>(), h->counters.as<unsigned>(),
+                                  h->status.as<int>(), h->spinMax, s, h->stallTest, trace));
+        h->statusPending = true;
+        nl += 1;
+        aggB = h->partB.as<uint16_t>();
+        if (h->retain || select_needs_summed_volume(D, Dp)) {
+            launch_sum_volumes(h->agg.as<uint16_t>(), aggB, h->agg.as<uint16_t>(), ND, s);
+            LCU(cudaGetLastError());
+            nl += 1;
+            aggB = nullptr;
+        }
+    } else if (sched == 3) {
         LCU(h->partB.ensure(ND * 2));
         LCU(h->xring.ensure(plan2.ringBytes));
         LCU(h->counters.ensure(sizeof(unsigned) * plan2.counterWords));
@@ -603,6 +659,8 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
         int rs[4];
         const int nr = sweep2_rows_options(Dp, rs, 4);
         for (int i = 0; i < nr; ++i) cands.push_back({3, SweepConfig{32, rs[i]}});
+        const int nw = wave_rows_options(Dp, rs, 4);
+        for (int i = 0; i < nw; ++i) cands.push_back({4, SweepConfig{32, rs[i]}});
     }
     const SweepConfig savedForced = h->forced;
     const int savedSched = h->schedule;

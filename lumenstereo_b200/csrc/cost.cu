@@ -213,11 +213,12 @@ __device__ __forceinline__ void sad_row_quad(const uint8_t* sLrow, const uint8_t
     od = (v >> 8) & 0x00FF00FFu;
 }
 
-template <bool WIDE>
+template <bool WIDE, int KP>
 __global__ void __launch_bounds__(256)
 sad_cost_kernel(const uint8_t* __restrict__ pl, const uint8_t* __restrict__ pr, int W, int H,
-                int D, int Dp, int minD, int r, const uint32_t* __restrict__ magic,
+                int D, int minD, int r, const uint32_t* __restrict__ magic,
                 uint8_t* __restrict__ cost) {
+    constexpr int Dp = 64 * KP;  // padded disparities: divisions below are by constants
     extern __shared__ __align__(16) uint8_t sm[];
     const SadGeom g = sad_geom(Dp, r);
     const int x0 = blockIdx.x * kSadTile;
@@ -225,7 +226,7 @@ sad_cost_kernel(const uint8_t* __restrict__ pl, const uint8_t* __restrict__ pr, 
     const int yEnd = min(H, yb + kSadBand);
     const int lx0 = x0 - r;                        // column of cs index 0
     const int rtop = lx0 + g.ncol - 1 - minD;      // right column at reversed index 0
-    const int quads = Dp / 4;
+    constexpr int quads = Dp / 4;
     uint8_t* sL = sm;                              // [ring][ncolp]
     uint8_t* sR = sL + g.ring * g.ncolp;           // [ring][rw]
     uint2* cs = reinterpret_cast<uint2*>(sm + ((g.ring * (g.ncolp + g.rw) + 15) & ~15));  // [ncol][quads]
@@ -281,22 +282,26 @@ sad_cost_kernel(const uint8_t* __restrict__ pl, const uint8_t* __restrict__ pr, 
             const int yin = y + r, yout = y - r - 1;
             if (yin < H) load_row(yin);
             __syncthreads();
+            const bool hasIn = yin < H, hasOut = yout >= 0;
+            const uint8_t* sLin = sL + (hasIn ? yin % g.ring : 0) * g.ncolp;
+            const uint8_t* sRin = sR + (hasIn ? yin % g.ring : 0) * g.rw;
+            const uint8_t* sLout = sL + (hasOut ? yout % g.ring : 0) * g.ncolp;
+            const uint8_t* sRout = sR + (hasOut ? yout % g.ring : 0) * g.rw;
             for (int c = warp; c < g.ncol; c += nw) {
+#pragma unroll
                 for (int q = lane; q < quads; q += 32) {
                     const uint32_t mask = quad_mask(c, q);
                     if (!mask) continue;
                     const int j0 = rtop - (lx0 + c - minD - 4 * q);
                     uint2 v = cs[c * quads + q];
                     uint32_t e, o;
-                    if (yin < H) {
-                        const int slot = yin % g.ring;
-                        sad_row_quad(sL + slot * g.ncolp, sR + slot * g.rw, c, j0, mask, e, o);
+                    if (hasIn) {
+                        sad_row_quad(sLin, sRin, c, j0, mask, e, o);
                         v.x += e;
                         v.y += o;
                     }
-                    if (yout >= 0) {
-                        const int slot = yout % g.ring;
-                        sad_row_quad(sL + slot * g.ncolp, sR + slot * g.rw, c, j0, mask, e, o);
+                    if (hasOut) {
+                        sad_row_quad(sLout, sRout, c, j0, mask, e, o);
                         v.x -= e;
                         v.y -= o;
                     }
@@ -311,7 +316,7 @@ sad_cost_kernel(const uint8_t* __restrict__ pl, const uint8_t* __restrict__ pr, 
         const uint32_t mfull = magic[full];
         const int runs = kSadTile / kSadRun;
         for (int item = threadIdx.x; item < quads * runs; item += blockDim.x) {
-            const int q = item % quads, run = item / quads;  // quads is 16..128: shifts when a power of 2
+            const int q = item % quads, run = item / quads;  // quads is a compile-time constant
             const int px0 = run * kSadRun;
             const int d0 = 4 * q;
             uint32_t s0, s1, s2, s3;  // window sums of d0..d0+3 (WIDE) or packed pairs
@@ -415,6 +420,34 @@ cudaError_t launch_census_cost(const uint32_t* cl, const uint32_t* cr, int W, in
     return cudaGetLastError();
 }
 
+template <bool WIDE>
+static cudaError_t launch_sad_kp(const uint8_t* pl, const uint8_t* pr, int W, int H, int D, int Dp,
+                                 int minD, int r, const uint32_t* magic, uint8_t* cost, size_t smem,
+                                 cudaStream_t s) {
+    dim3 g((W + kSadTile - 1) / kSadTile, (H + kSadBand - 1) / kSadBand);
+#define LUMEN_SAD_CASE(KP)                                                                     \
+    case KP: {                                                                                 \
+        auto kern = sad_cost_kernel<WIDE, KP>;                                                 \
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                             (int)smem);                                       \
+        if (e != cudaSuccess) return e;                                                        \
+        kern<<<g, 256, smem, s>>>(pl, pr, W, H, D, minD, r, magic, cost);                       \
+        return cudaGetLastError();                                                             \
+    }
+    switch (Dp / 64) {
+        LUMEN_SAD_CASE(1)
+        LUMEN_SAD_CASE(2)
+        LUMEN_SAD_CASE(3)
+        LUMEN_SAD_CASE(4)
+        LUMEN_SAD_CASE(5)
+        LUMEN_SAD_CASE(6)
+        LUMEN_SAD_CASE(7)
+        LUMEN_SAD_CASE(8)
+    default: return cudaErrorInvalidValue;
+    }
+#undef LUMEN_SAD_CASE
+}
+
 size_t sad_cost_smem(int Dp, int r) {
     const SadGeom g = sad_geom(Dp, r);
     return (size_t)((g.ring * (g.ncolp + g.rw) + 15) & ~15) + (size_t)g.ncol * (Dp / 4) * 8;
@@ -424,12 +457,8 @@ cudaError_t launch_sad_cost(const uint8_t* pl, const uint8_t* pr, int W, int H, 
                             int minD, int r, const uint32_t* magic, int wide, uint8_t* cost,
                             cudaStream_t s) {
     const size_t smem = sad_cost_smem(Dp, r);
-    auto kern = wide ? sad_cost_kernel<true> : sad_cost_kernel<false>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    dim3 g((W + kSadTile - 1) / kSadTile, (H + kSadBand - 1) / kSadBand);
-    kern<<<g, 256, smem, s>>>(pl, pr, W, H, D, Dp, minD, r, magic, cost);
-    return cudaGetLastError();
+    return wide ? launch_sad_kp<true>(pl, pr, W, H, D, Dp, minD, r, magic, cost, smem, s)
+                : launch_sad_kp<false>(pl, pr, W, H, D, Dp, minD, r, magic, cost, smem, s);
 }
 
 }  // namespace lumen

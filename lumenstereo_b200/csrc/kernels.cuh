@@ -73,6 +73,24 @@ cudaError_t launch_aggregate_sweep2(const PairView& pv, uint16_t* partB, const S
                                     unsigned* counters, int* status, long long spinMax,
                                     cudaStream_t s, int stallTest = 0);
 
+// ---- schedule 4: lockstep row-band fused sweeps (wave.cu, wave_kernel.cuh) ----
+struct WavePlan {
+    int R;                 // rows per band
+    int Q;                 // import / export ring slots
+    int nBands;            // bands per sweep
+    int grid;              // CTAs launched (persistent, ticket-scheduled)
+    int smem;              // dynamic shared memory per CTA
+    size_t ringBytes;      // exchange rings, both sweeps
+    size_t counterWords;   // prod + cons + ticket
+};
+int wave_rows_options(int Dp, int* out, int max);
+cudaError_t wave_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSMs, WavePlan* plan);
+cudaError_t launch_aggregate_wave(const PairView& pv, uint16_t* partB, const SgmConsts& k,
+                                  bool wrap, bool diag, const WavePlan& plan, uint8_t* xring,
+                                  unsigned* counters, int* status, long long spinMax,
+                                  cudaStream_t s, int stallTest = 0,
+                                  unsigned long long* trace = nullptr);
+
 // aggB (nullable): second partial volume summed with agg (mod 2^16 when wrap).
 cudaError_t launch_select(const uint16_t* agg, const uint16_t* aggB, bool wrap, int W, int H,
                           int D, int Dp, int minD, int UR, int16_t* dispL, int16_t* dispR,

@@ -1,10 +1,10 @@
 // select.cu -- disparity selection and post-processing.
 //
-// select_kernel  replaces selectDisparityWTA + selectDisparityRight
-//                (src/sgbm_kernels.cu:748-856): one CTA per (row, tile of T
-//                left pixels) stages the aggregated rows it needs in shared
-//                memory once and serves both views from there (the right view
-//                reads the diagonal agg[y][xr+minD+d][d]).
+// select_team_kernel / select_row_kernel replace selectDisparityWTA +
+//                selectDisparityRight (src/sgbm_kernels.cu:748-856): the team
+//                kernel stages a row tile in shared memory and serves both
+//                views from it; the row kernel handles tiles too large for
+//                shared memory.
 // post_kernel    replaces consistencyCheck + speckleFilter + medianFilter3x3
 //                and the device-to-device copy back (src/sgbm_kernels.cu:
 //                862-1013, src/sgbm_gpu.cu:460-515) with one tiled pass.
@@ -32,111 +32,6 @@ __device__ __forceinline__ int16_t subpixel_disp(float c0, float c1, float c2, i
         }
     }
     return static_cast<int16_t>((subpixelD + minD) * 16.0f);
-}
-
-// KW: words per lane as in aggregation (lane holds d in [2KW*lane, 2KW*lane+2KW)).
-// SMEM: serve the right view from the staged tile (else gather from global).
-template <int KW, bool SMEM>
-__global__ void __launch_bounds__(256)
-select_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict__ aggB, int wrap, int W,
-              int H, int D, int Dp, int minD, int UR, int T, int16_t* __restrict__ dispL,
-              int16_t* __restrict__ dispR) {
-    extern __shared__ __align__(16) uint16_t sa[];
-    const int y = blockIdx.y;
-    const int x0 = blockIdx.x * T;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const uint16_t* row = agg + (size_t)y * W * Dp;
-    const int loadHi = min(W, x0 + T + D - 1);
-    const int nload = SMEM ? max(0, loadHi - x0) : 0;
-    if (SMEM) {
-        const uint4* src = reinterpret_cast<const uint4*>(row + (size_t)x0 * Dp);
-        uint4* dst = reinterpret_cast<uint4*>(sa);
-        const int n16 = nload * Dp / 8;
-        if (aggB) {  // two partial volumes (sweep schedule): sum while staging
-            const uint4* srcB = reinterpret_cast<const uint4*>(aggB + (size_t)y * W * Dp + (size_t)x0 * Dp);
-            for (int i = threadIdx.x; i < n16; i += blockDim.x) {
-                const uint4 p = src[i], q = srcB[i];
-                dst[i] = wrap ? make_uint4(__vadd2(p.x, q.x), __vadd2(p.y, q.y), __vadd2(p.z, q.z), __vadd2(p.w, q.w))
-                              : make_uint4(p.x + q.x, p.y + q.y, p.z + q.z, p.w + q.w);
-            }
-        } else {
-            for (int i = threadIdx.x; i < n16; i += blockDim.x) dst[i] = src[i];
-        }
-        __syncthreads();
-    }
-    const int dBase = 2 * KW * lane;
-    // ---- left view: x in [x0, x0+T) ----
-    for (int px = warp; px < T; px += nw) {
-        const int x = x0 + px;
-        if (x >= W) break;
-        const uint16_t* v = SMEM ? sa + (size_t)px * Dp : row + (size_t)x * Dp;
-        uint32_t m1 = 0x10000u, m2 = 0x10000u, i1 = 0xFFFFu;
-#pragma unroll
-        for (int j = 0; j < 2 * KW; ++j) {
-            const int d = dBase + j;
-            if (d < D) {
-                const uint32_t c = v[d];
-                if (c < m1) { m2 = m1; m1 = c; i1 = d; }
-                else if (c < m2) m2 = c;
-            }
-        }
-        const uint32_t key = (m1 <= 0xFFFFu) ? ((m1 << 16) | i1) : 0xFFFFFFFFu;
-        const uint32_t kmin = __reduce_min_sync(kFullMask, key);
-        const uint32_t best = kmin >> 16;
-        const int bestD = (int)(kmin & 0xFFFFu);
-        // second order statistic of the multiset = min(all lane seconds,
-        // second smallest of the lane minima)
-        const uint32_t sA = __reduce_min_sync(kFullMask, m2);
-        const unsigned ties = __ballot_sync(kFullMask, m1 == best);
-        uint32_t sB;
-        if (__popc(ties) >= 2) sB = best;
-        else sB = __reduce_min_sync(kFullMask, key == kmin ? 0x10000u : m1);
-        uint32_t second = min(min(sA, sB), 0xFFFFu);
-        if (lane == 0) {
-            int16_t out;
-            if (UR > 0 && second != 0xFFFFu &&
-                second <= best + (best * (uint32_t)UR) / 100u) {
-                out = -1;
-            } else if (bestD > 0 && bestD < D - 1) {
-                out = subpixel_disp((float)v[bestD - 1], (float)v[bestD], (float)v[bestD + 1],
-                                    bestD, D, minD);
-            } else {
-                out = subpixel_disp(0.f, 0.f, 0.f, bestD, D, minD);
-            }
-            dispL[(size_t)y * W + x] = out;
-        }
-    }
-    // ---- right view: xr in [x0-minD, x0-minD+T) ----
-    for (int px = warp; px < T; px += nw) {
-        const int xr = x0 - minD + px;
-        if (xr < 0) continue;
-        if (xr >= W) break;
-        uint32_t key = 0xFFFFFFFFu;
-#pragma unroll
-        for (int j = 0; j < 2 * KW; ++j) {
-            const int d = dBase + j;
-            const int lx = xr + minD + d;  // = x0 + px + d
-            if (d < D && lx < W) {
-                const uint32_t c = SMEM ? sa[(size_t)(px + d) * Dp + d] : row[(size_t)lx * Dp + d];
-                const uint32_t k = (c << 16) | (uint32_t)d;
-                key = min(key, k);
-            }
-        }
-        const uint32_t kmin = __reduce_min_sync(kFullMask, key);
-        if (lane == 0) {
-            const int bestD = kmin == 0xFFFFFFFFu ? 0 : (int)(kmin & 0xFFFFu);
-            int16_t out;
-            if (bestD > 0 && bestD < D - 1) {
-                const uint16_t* v = SMEM ? sa + (size_t)(px + bestD) * Dp
-                                         : row + (size_t)(xr + minD + bestD) * Dp;
-                out = subpixel_disp((float)v[bestD - 1], (float)v[bestD], (float)v[bestD + 1],
-                                    bestD, D, minD);
-            } else {
-                out = subpixel_disp(0.f, 0.f, 0.f, bestD, D, minD);
-            }
-            dispR[(size_t)y * W + xr] = out;
-        }
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -276,6 +171,8 @@ select_team_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict_
     }
 }
 
+constexpr size_t kSelectSmemMax = 227 * 1024;  // opt-in shared memory per block on sm_100
+
 template <int KS>
 static cudaError_t launch_select_team(const uint16_t* agg, const uint16_t* aggB, bool wrap, int W,
                                       int H, int D, int Dp, int minD, int UR, int16_t* dispL,
@@ -284,10 +181,12 @@ static cudaError_t launch_select_team(const uint16_t* agg, const uint16_t* aggB,
     size_t smem = 0;
     for (int t : {128, 64, 32}) {
         const size_t b = (size_t)(t + D - 1) * (Dp + 2) * 2;
-        if (b <= 200 * 1024) { T = t; smem = b; break; }
+        if (b <= kSelectSmemMax) { T = t; smem = b; break; }
     }
     *launched = false;
-    if (T == 0) return cudaSuccess;
+    // a tile stages T + D - 1 pixels for T outputs: past ~2.5x re-reads the row
+    // kernel, which reads every vector once, is faster
+    if (T == 0 || 2 * (T + D - 1) > 5 * T) return cudaSuccess;
     cudaError_t e = cudaFuncSetAttribute(select_team_kernel<KS>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -297,41 +196,104 @@ static cudaError_t launch_select_team(const uint16_t* agg, const uint16_t* aggB,
     return cudaGetLastError();
 }
 
-template <int KW>
-static cudaError_t launch_select_kw(const uint16_t* agg, const uint16_t* aggB, bool wrap, int W,
-                                    int H, int D, int Dp, int minD, int UR, int16_t* dispL,
-                                    int16_t* dispR, cudaStream_t s) {
-    // Largest tile whose staged rows fit in shared memory.
-    int T = 0;
-    size_t smem = 0;
-    for (int t : {128, 64, 32, 16}) {
-        const size_t b = (size_t)(t + D - 1) * Dp * 2;
-        if (b <= 200 * 1024) { T = t; smem = b; break; }
+// ---------------------------------------------------------------------------
+// select_row_kernel: both selections for one image row per CTA (the
+// fallback when a tile of the team kernel does not fit in shared memory):
+// each aggregated vector is read once; the left view is a warp per pixel
+// with lane l holding d = l + 32 j, the right view a shared-memory
+// atomicMin over (cost << 16 | d) keys of right pixel xr = x - minD - d
+// (ties to the smaller d), whose subpixel neighbours are then read at the left
+// pixel xr + minD + bestD (src/sgbm_kernels.cu:839-845).
+// ---------------------------------------------------------------------------
+template <int NJ>
+__global__ void __launch_bounds__(256)
+select_row_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict__ aggB, int W,
+                  int D, int Dp, int minD, int UR, int16_t* __restrict__ dispL,
+                  int16_t* __restrict__ dispR) {
+    extern __shared__ uint32_t rec[];  // [W] right-view keys
+    const int y = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int i = threadIdx.x; i < W; i += blockDim.x) rec[i] = 0xFFFFFFFFu;
+    __syncthreads();
+    const uint16_t* rowA = agg + (size_t)y * W * Dp;
+    const uint16_t* rowB = aggB ? aggB + (size_t)y * W * Dp : nullptr;
+    auto cost_at = [&](int x, int d) -> uint32_t {
+        const size_t i = (size_t)x * Dp + d;
+        uint32_t c = rowA[i];
+        if (rowB) c = (c + rowB[i]) & 0xFFFFu;
+        return c;
+    };
+    for (int x = warp; x < W; x += nw) {
+        uint32_t key[NJ];
+        uint32_t kl = 0xFFFFFFFFu;
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+            const int d = lane + 32 * j;
+            uint32_t k = 0xFFFFFFFFu;
+            if (d < D) k = (cost_at(x, d) << 16) | (uint32_t)d;
+            key[j] = k;
+            kl = min(kl, k);
+        }
+        const uint32_t kmin = __reduce_min_sync(kFullMask, kl);
+        const uint32_t best = kmin >> 16;
+        const int bestD = (int)(kmin & 0xFFFFu);
+        uint32_t m2 = 0xFFFFu;
+#pragma unroll
+        for (int j = 0; j < NJ; ++j)
+            if (key[j] != 0xFFFFFFFFu && (int)(key[j] & 0xFFFFu) != bestD) m2 = min(m2, key[j] >> 16);
+        const uint32_t second = __reduce_min_sync(kFullMask, m2);
+        if (lane == 0) {
+            int16_t out;
+            if (UR > 0 && second != 0xFFFFu && second <= best + (best * (uint32_t)UR) / 100u) {
+                out = -1;
+            } else if (bestD > 0 && bestD < D - 1) {
+                out = subpixel_disp((float)cost_at(x, bestD - 1), (float)best, (float)cost_at(x, bestD + 1),
+                                    bestD, D, minD);
+            } else {
+                out = subpixel_disp(0.f, 0.f, 0.f, bestD, D, minD);
+            }
+            dispL[(size_t)y * W + x] = out;
+        }
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+            const int xr = x - minD - (lane + 32 * j);
+            if (key[j] != 0xFFFFFFFFu && xr >= 0) atomicMin(&rec[xr], key[j]);
+        }
     }
-    if (T > 0) {
-        cudaError_t e = cudaFuncSetAttribute(select_kernel<KW, true>,
+    __syncthreads();
+    for (int xr = threadIdx.x; xr < W; xr += blockDim.x) {
+        const uint32_t k = rec[xr];
+        const int bestD = k == 0xFFFFFFFFu ? 0 : (int)(k & 0xFFFFu);
+        int16_t out;
+        if (bestD > 0 && bestD < D - 1) {
+            const int lx = xr + minD + bestD;
+            out = subpixel_disp((float)cost_at(lx, bestD - 1), (float)(k >> 16), (float)cost_at(lx, bestD + 1),
+                                bestD, D, minD);
+        } else {
+            out = subpixel_disp(0.f, 0.f, 0.f, bestD, D, minD);
+        }
+        dispR[(size_t)y * W + xr] = out;
+    }
+}
+
+template <int NJ>
+static cudaError_t launch_select_row(const uint16_t* agg, const uint16_t* aggB, int W, int H, int D,
+                                     int Dp, int minD, int UR, int16_t* dispL, int16_t* dispR,
+                                     cudaStream_t s) {
+    const size_t smem = (size_t)W * 4;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(select_row_kernel<NJ>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        dim3 g((W + minD + T - 1) / T, H);
-        select_kernel<KW, true><<<g, 256, smem, s>>>(agg, aggB, wrap, W, H, D, Dp, minD, UR, T,
-                                                     dispL, dispR);
-    } else {
-        if (aggB) return cudaErrorInvalidValue;  // the caller sums the partials first
-        T = 32;
-        dim3 g((W + minD + T - 1) / T, H);
-        select_kernel<KW, false><<<g, 256, 0, s>>>(agg, nullptr, 0, W, H, D, Dp, minD, UR, T,
-                                                   dispL, dispR);
     }
+    select_row_kernel<NJ><<<H, 256, smem, s>>>(agg, aggB, W, D, Dp, minD, UR, dispL, dispR);
     return cudaGetLastError();
 }
 
 bool select_needs_summed_volume(int D, int Dp) {
-    if (Dp <= 320)
-        for (int t : {128, 64, 32})
-            if ((size_t)(t + D - 1) * (Dp + 2) * 2 <= 200 * 1024) return false;
-    for (int t : {128, 64, 32, 16})
-        if ((size_t)(t + D - 1) * Dp * 2 <= 200 * 1024) return false;
-    return true;
+    (void)D;
+    (void)Dp;
+    return false;  // both select kernels sum the two partial volumes themselves
 }
 
 __global__ void sum_volumes_kernel(const uint32_t* __restrict__ a, const uint32_t* __restrict__ b,
@@ -364,15 +326,17 @@ cudaError_t launch_select(const uint16_t* agg, const uint16_t* aggB, bool wrap, 
     default: break;
     }
     if (e != cudaSuccess || launched) return e;
-    switch (Dp / 64) {
-    case 1: return launch_select_kw<1>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 2: return launch_select_kw<2>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 3: return launch_select_kw<3>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 4: return launch_select_kw<4>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 5: return launch_select_kw<5>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 6: return launch_select_kw<6>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 7: return launch_select_kw<7>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 8: return launch_select_kw<8>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    // the row kernel sums uint16 values mod 2^16 whether or not they can wrap
+    if ((size_t)W * 4 > kSelectSmemMax) return cudaErrorInvalidValue;
+    switch (Dp / 32) {
+    case 2: return launch_select_row<2>(agg, aggB, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 4: return launch_select_row<4>(agg, aggB, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 6: return launch_select_row<6>(agg, aggB, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 8: return launch_select_row<8>(agg, aggB, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 10: return launch_select_row<10>(agg, aggB, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 12: return launch_select_row<12>(agg, aggB, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 14: return launch_select_row<14>(agg, aggB, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 16: return launch_select_row<16>(agg, aggB, W, H, D, Dp, minD, UR, dispL, dispR, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -440,20 +404,39 @@ post_kernel(const int16_t* __restrict__ dispL, const int16_t* __restrict__ dispR
     if (x >= W || y >= H) return;
     const int cy = threadIdx.y + kApron, cx = threadIdx.x + kApron;
     if (dbgLR) dbgLR[(size_t)y * W + x] = M[cy][cx];
-    int16_t v[9];
+    // positive-only upper median (src/sgbm_kernels.cu:892-935): non-positive
+    // neighbours become +32767 (above every valid 1/16-px disparity), a
+    // min/max network sorts the nine values in registers, and the
+    // count/2-th positive value is picked
+    int v[9];
     int count = 0;
 #pragma unroll
     for (int dy = -1; dy <= 1; ++dy)
 #pragma unroll
         for (int dx = -1; dx <= 1; ++dx) {
-            const int16_t val = M[cy + dy][cx + dx];
-            if (val > 0) {
-                int j = count++;
-                while (j > 0 && v[j - 1] > val) { v[j] = v[j - 1]; --j; }
-                v[j] = val;
-            }
+            const int val = M[cy + dy][cx + dx];
+            const bool pos = val > 0;
+            count += pos;
+            v[(dy + 1) * 3 + dx + 1] = pos ? val : 32767;
         }
-    out[(size_t)y * outPitch + x] = count == 0 ? M[cy][cx] : v[count / 2];
+    auto cx2 = [](int& a, int& b) { const int lo = min(a, b); b = max(a, b); a = lo; };
+    // 9-input sorting network (25 compare-exchanges)
+    cx2(v[0], v[1]); cx2(v[3], v[4]); cx2(v[6], v[7]);
+    cx2(v[1], v[2]); cx2(v[4], v[5]); cx2(v[7], v[8]);
+    cx2(v[0], v[1]); cx2(v[3], v[4]); cx2(v[6], v[7]);
+    cx2(v[0], v[3]); cx2(v[3], v[6]); cx2(v[0], v[3]);
+    cx2(v[1], v[4]); cx2(v[4], v[7]); cx2(v[1], v[4]);
+    cx2(v[2], v[5]); cx2(v[5], v[8]); cx2(v[2], v[5]);
+    cx2(v[1], v[3]); cx2(v[5], v[7]); cx2(v[2], v[6]);
+    cx2(v[4], v[6]); cx2(v[2], v[4]); cx2(v[2], v[3]);
+    cx2(v[5], v[6]);
+    const int k = count >> 1;
+    int med = v[0];
+    med = k == 1 ? v[1] : med;
+    med = k == 2 ? v[2] : med;
+    med = k == 3 ? v[3] : med;
+    med = k == 4 ? v[4] : med;
+    out[(size_t)y * outPitch + x] = count == 0 ? M[cy][cx] : (int16_t)med;
 }
 
 cudaError_t launch_post(const int16_t* dispL, const int16_t* dispR, int W, int H, int lrMaxDiff,

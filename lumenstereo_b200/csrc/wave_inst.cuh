@@ -1,0 +1,51 @@
+// wave_inst.cuh -- launch helper of the schedule-4 wave kernel, instantiated
+// once per padded disparity count (64 * KP) in wave_k<KP>.cu.
+#pragma once
+#include "wave_kernel.cuh"
+
+namespace lumen {
+
+// grid == 0: report the CTAs per SM that fit (occupancy) in *perSM, launch nothing.
+template <int KW, bool WRAP, bool FULL, int NP, int R>
+cudaError_t wave_launch_t(const WaveArgs& a, int smem, int grid, cudaStream_t s, int* perSM) {
+    auto kern = wave_kernel<KW, WRAP, FULL, NP, R>;
+    constexpr int threads = (R + 2) * 32;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    if (grid == 0) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, kern, threads, smem);
+    kern<<<grid, threads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int KW, int NP, int R>
+cudaError_t wave_launch_np(const WaveArgs& a, bool wrap, bool full, int smem, int grid,
+                           cudaStream_t s, int* perSM) {
+    if (wrap) return full ? wave_launch_t<KW, true, true, NP, R>(a, smem, grid, s, perSM)
+                          : wave_launch_t<KW, true, false, NP, R>(a, smem, grid, s, perSM);
+    return full ? wave_launch_t<KW, false, true, NP, R>(a, smem, grid, s, perSM)
+                : wave_launch_t<KW, false, false, NP, R>(a, smem, grid, s, perSM);
+}
+
+template <int KP>
+cudaError_t wave_dispatch_kp(const WaveArgs& a, int R, int NP, bool wrap, int smem, int grid,
+                             cudaStream_t s, int* perSM) {
+    constexpr int KW = KP;
+    const bool full = (a.D == a.Dp);
+    if (R == 4) return NP == 3 ? wave_launch_np<KW, 3, 4>(a, wrap, full, smem, grid, s, perSM)
+                               : wave_launch_np<KW, 1, 4>(a, wrap, full, smem, grid, s, perSM);
+    if (R == 8) return NP == 3 ? wave_launch_np<KW, 3, 8>(a, wrap, full, smem, grid, s, perSM)
+                               : wave_launch_np<KW, 1, 8>(a, wrap, full, smem, grid, s, perSM);
+    if (R == 16) return NP == 3 ? wave_launch_np<KW, 3, 16>(a, wrap, full, smem, grid, s, perSM)
+                                : wave_launch_np<KW, 1, 16>(a, wrap, full, smem, grid, s, perSM);
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace lumen
+
+#define LUMEN_WAVE_INSTANCE(KP)                                                                \
+    namespace lumen {                                                                          \
+    cudaError_t wave_dispatch_##KP(const WaveArgs& a, int R, int NP, bool wrap, int smem,      \
+                                   int grid, cudaStream_t s, int* perSM) {                     \
+        return wave_dispatch_kp<KP>(a, R, NP, wrap, smem, grid, s, perSM);                     \
+    }                                                                                          \
+    }

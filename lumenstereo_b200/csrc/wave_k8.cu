@@ -1,0 +1,5 @@
+// wave_k8.cu -- schedule-4 wave kernel instances for padded disparity count 512;
+// one translation unit per width keeps the build parallel.
+#include "wave_inst.cuh"
+
+LUMEN_WAVE_INSTANCE(8)

@@ -104,7 +104,7 @@ CASES = {
 }
 
 
-@pytest.mark.parametrize("schedule", [1, 2, 3])
+@pytest.mark.parametrize("schedule", [1, 2, 3, 4])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_parity_small(name, schedule, oracle_mod):
     w, h, over = CASES[name]
@@ -167,14 +167,54 @@ def test_parity_schedule3_rows(D, rows, oracle_mod):
         assert_subpix_close(disp, ref_disp)
 
 
-def test_schedule3_timeout_reports_error():
+@pytest.mark.parametrize("rows", [8, 16])
+@pytest.mark.parametrize("D", [40, 128, 150, 290, 512])
+def test_parity_schedule4_rows(D, rows, oracle_mod):
+    """The lockstep row-band sweeps (schedule 4) at both band heights reproduce
+    the oracle bit for bit, both cost modes, 4 and 8 paths, odd image sizes
+    (several bands per sweep, a partial last band)."""
+    left, right, _ = synth.make_pair(synth.PairSpec(131, 53, 4, 1, min(D - 1, 40), 2.0, 80 + D))
+    for mode, nd in ((0, 8), (1, 4), (1, 8)):
+        pd = params_dict(maxDisparity=D, numDirections=nd, matchingCostMode=mode,
+                         speckleWindowSize=0)
+        with StereoSGBM(to_params(pd)) as s:
+            s.set_schedule(4)
+            s.set_tuning(32, rows)
+            s.retain_intermediates(True)
+            disp = s.compute(left, right)
+            agg = s.intermediate("agg", (53, 131, D), np.uint16)
+            used = s.get_tuning()
+        assert used[0] == 4, used
+        ref_disp, ref = oracle_mod.sgbm(pd, left, right, intermediates=True)
+        assert np.array_equal(agg, ref["agg"]), (mode, nd)
+        assert_subpix_close(disp, ref_disp)
+
+
+def test_parity_schedule4_wide_image(oracle_mod):
+    """A row longer than the exchange ring (kWK = 64 pixels) exercises the
+    exporter's back-pressure waits between bands."""
+    left, right, _ = synth.make_pair(synth.PairSpec(700, 40, 4, 1, 30, 2.0, 99))
+    for nd in (4, 8):
+        pd = params_dict(maxDisparity=48, numDirections=nd, speckleWindowSize=0)
+        with StereoSGBM(to_params(pd)) as s:
+            s.set_schedule(4)
+            s.retain_intermediates(True)
+            disp = s.compute(left, right)
+            agg = s.intermediate("agg", (40, 700, 48), np.uint16)
+        ref_disp, ref = oracle_mod.sgbm(pd, left, right, intermediates=True)
+        assert np.array_equal(agg, ref["agg"]), nd
+        assert_subpix_close(disp, ref_disp)
+
+
+@pytest.mark.parametrize("schedule", [3, 4])
+def test_fused_sweep_timeout_reports_error(schedule):
     """A device-side wait that runs out ends the launch with a timeout status,
-    not a hang: one wait of the first band is made unsatisfiable and the wait
+    not a hang: one wait of the second band is made unsatisfiable and the wait
     limit is cut, so the launch gives up quickly; the handle then recovers."""
     left, right = synth.random_pair(300, 64, seed=3)
     p = StereoParams(maxDisparity=64, numDirections=8, speckleWindowSize=0)
     with StereoSGBM(p) as s:
-        s.set_schedule(3)
+        s.set_schedule(schedule)
         s.set_wait_limit(1 << 14)
         s.stall_test(True)
         with pytest.raises(TimeoutException):
@@ -298,14 +338,14 @@ def test_schedules_agree_full_size(wl):
                      matchingCostMode=MatchingCostMode.Census if w.census else MatchingCostMode.SAD,
                      speckleWindowSize=0)
     outs = []
-    for schedule in (1, 2, 3):
+    for schedule in (1, 2, 3, 4):
         with StereoSGBM(p) as s:
             s.set_schedule(schedule)
             s.retain_intermediates(True)
             d = s.compute(left, right)
             agg = s.intermediate("agg", left.shape + (w.max_disparity,), np.uint16)
             outs.append((d, agg))
-    for k in (1, 2):
+    for k in (1, 2, 3):
         assert np.array_equal(outs[0][1], outs[k][1]), k
         assert np.array_equal(outs[0][0], outs[k][0]), k
 
