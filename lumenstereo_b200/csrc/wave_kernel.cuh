@@ -215,6 +215,8 @@ __device__ __forceinline__ bool w_wait_cta(const unsigned* p, unsigned need, uns
             *abortFlag = 1;
             return false;
         }
+        // back off: a spinning helper warp would take issue slots from the rows
+        __nanosleep(40);
     }
 }
 
