@@ -194,6 +194,36 @@ lumen_status lumen_remap(const uint8_t* src, const float* map_x, const float* ma
 lumen_status lumen_bgr_to_gray(const uint8_t* bgr, size_t stride, uint8_t* gray, int width,
                                int height);
 
+/* ---- batched form (no counterpart in the reference's API; LumenStereo's
+ * callers loop over StereoSGBM::compute, e.g. tools/evaluate.cpp:158-160) ----
+ *
+ * A batch holds stereo pairs of any sizes and parameters (gray DEVICE images
+ * of width*height bytes with row pitch width; int16 DEVICE outputs with row
+ * pitch width, 1/16 px, -1 invalid).  lumen_sgbm_batch_run enqueues every pair
+ * on `stream`: cost volumes per pair, one persistent aggregation launch per
+ * group of pairs of one kernel class (the wavefronts of all its pairs share
+ * the GPU), then selection per pair.  The first run after an add, a clear or
+ * an option change plans and allocates one pooled buffer (groups are cut so
+ * each fits device_budget_bytes, default 48 GiB) and, with graphs enabled,
+ * captures the run into a CUDA graph that later runs replay.  Outputs equal
+ * lumen_sgbm_compute_device's bit for bit.  lumen_sgbm_batch_sync waits for
+ * `stream` and reports a device-side timeout. */
+typedef struct lumen_sgbm_batch lumen_sgbm_batch;
+lumen_status lumen_sgbm_batch_create(lumen_sgbm_batch** out);
+lumen_status lumen_sgbm_batch_destroy(lumen_sgbm_batch* b);
+lumen_status lumen_sgbm_batch_add(lumen_sgbm_batch* b, const lumen_stereo_params* params,
+                                  const uint8_t* d_left, const uint8_t* d_right, int width,
+                                  int height, int16_t* d_out);
+lumen_status lumen_sgbm_batch_clear(lumen_sgbm_batch* b);
+/* rows_per_band: 4, 8 or 16 (0 = 8); use_graph: capture and replay; budget 0 = keep. */
+lumen_status lumen_sgbm_batch_set_options(lumen_sgbm_batch* b, int rows_per_band, int use_graph,
+                                          size_t device_budget_bytes);
+lumen_status lumen_sgbm_batch_run(lumen_sgbm_batch* b, void* stream);
+lumen_status lumen_sgbm_batch_sync(lumen_sgbm_batch* b, void* stream);
+/* Pooled device bytes, number of launch groups, kernels per run. */
+lumen_status lumen_sgbm_batch_info(const lumen_sgbm_batch* b, size_t* device_bytes, int* groups,
+                                   unsigned long long* launches);
+
 /* ---- Census cost volume without device allocation.  No counterpart in the
  * reference: it serves callers that cannot call cudaMalloc (a real-time loop
  * that must not take cudaMalloc's implicit device synchronisation, a plugin host

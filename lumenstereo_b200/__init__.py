@@ -23,7 +23,7 @@ import numpy as np
 
 from . import _lib
 
-__all__ = ["MatchingCostMode", "StereoParams", "StereoSGBM", "StereoRectifier",
+__all__ = ["MatchingCostMode", "StereoParams", "StereoSGBM", "StereoBatch", "StereoRectifier",
            "StereoException", "CudaException", "kSgbmMaxDisparityRange",
            "middleburyMatcherMaxDisparity", "rectify_image_gpu", "bgr_to_gray"]
 
@@ -309,6 +309,58 @@ class StereoSGBM:
         out = np.empty(shape, dtype)
         _check(_lib.lib().lumen_sgbm_debug_copy(self._h, ids[which], out.ctypes.data, out.nbytes))
         return out
+
+
+class StereoBatch:
+    """Batched form of StereoSGBM.compute_device: many pairs (device buffers,
+    their own sizes and parameters) per run, one persistent aggregation launch
+    per kernel class, optionally replayed from a CUDA graph
+    (lumen_sgbm_batch_* in include/lumen_sgbm.h)."""
+
+    def __init__(self, rows_per_band: int = 0, use_graph: bool = False, budget_bytes: int = 0):
+        self._h = C.c_void_p()
+        _check(_lib.lib().lumen_sgbm_batch_create(C.byref(self._h)))
+        self.set_options(rows_per_band, use_graph, budget_bytes)
+
+    def set_options(self, rows_per_band: int = 0, use_graph: bool = False, budget_bytes: int = 0) -> None:
+        _check(_lib.lib().lumen_sgbm_batch_set_options(self._h, rows_per_band, int(use_graph), budget_bytes))
+
+    def add(self, params: StereoParams, left_ptr: int, right_ptr: int, width: int, height: int,
+            out_ptr: int) -> None:
+        c = params.to_c()
+        _check(_lib.lib().lumen_sgbm_batch_add(self._h, C.byref(c), left_ptr, right_ptr, width, height,
+                                               out_ptr))
+
+    def clear(self) -> None:
+        _check(_lib.lib().lumen_sgbm_batch_clear(self._h))
+
+    def run(self, stream: int = 0) -> None:
+        _check(_lib.lib().lumen_sgbm_batch_run(self._h, stream))
+
+    def sync(self, stream: int = 0) -> None:
+        _check(_lib.lib().lumen_sgbm_batch_sync(self._h, stream))
+
+    def info(self):
+        nb, ng, nl = C.c_size_t(0), C.c_int(0), C.c_ulonglong(0)
+        _check(_lib.lib().lumen_sgbm_batch_info(self._h, C.byref(nb), C.byref(ng), C.byref(nl)))
+        return {"device_bytes": nb.value, "groups": ng.value, "launches": nl.value}
+
+    def close(self) -> None:
+        if self._h:
+            _lib.lib().lumen_sgbm_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 class StereoRectifier:

@@ -69,6 +69,14 @@ def _declare(lib):
         "lumen_rectifier_rectify_device": (i, [vp, vp, vp, i, vp, vp, vp]),
         "lumen_remap": (i, [vp, vp, vp, vp, i, i, i]),
         "lumen_bgr_to_gray": (i, [vp, sz, vp, i, i]),
+        "lumen_sgbm_batch_create": (i, [C.POINTER(vp)]),
+        "lumen_sgbm_batch_destroy": (i, [vp]),
+        "lumen_sgbm_batch_add": (i, [vp, C.POINTER(CParams), vp, vp, i, i, vp]),
+        "lumen_sgbm_batch_clear": (i, [vp]),
+        "lumen_sgbm_batch_set_options": (i, [vp, i, i, sz]),
+        "lumen_sgbm_batch_run": (i, [vp, vp]),
+        "lumen_sgbm_batch_sync": (i, [vp, vp]),
+        "lumen_sgbm_batch_info": (i, [vp, C.POINTER(sz), C.POINTER(C.c_int), C.POINTER(C.c_ulonglong)]),
         "lumen_census_cost_noalloc": (i, [vp, vp, i, i, i, i, vp, i, vp]),
         "lumen_census_cost_noalloc_max_pixels": (sz, []),
     }

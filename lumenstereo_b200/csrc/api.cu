@@ -59,16 +59,6 @@ struct DevBuf {
     template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
-// ceil(2^32 / c) for c >= 2 (c = 0, 1 unused): sum / c == umulhi(sum, m[c])
-// whenever sum * (m[c]*c - 2^32) < 2^32, which holds for every SAD window sum.
-__global__ void magic_kernel(uint32_t* m, int n) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
-    m[c] = c >= 2 ? (uint32_t)((0x100000000ull + (unsigned long long)c - 1ull) /
-                               (unsigned long long)c)
-                  : 0u;
-}
-
 }  // namespace
 
 // Records `msg` as this thread's last error (lumen_last_error_string) for
@@ -432,8 +422,7 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
         LCU(h->pref[1].ensure(N));
         if (h->magicR != r) {
             LCU(h->magic.ensure((size_t)nmagic * 4));
-            magic_kernel<<<(nmagic + 255) / 256, 256, 0, s>>>(h->magic.as<uint32_t>(), nmagic);
-            LCU(cudaGetLastError());
+            LCU(launch_magic(h->magic.as<uint32_t>(), nmagic, s));
             h->magicR = r;
             nl += 1;
         }

@@ -1,0 +1,430 @@
+// batch.cu -- batched SGBM (lumen_sgbm_batch_*): many stereo pairs per run.
+//
+// The plain call (lumen_sgbm_compute_device) runs one pair's aggregation
+// wavefront, whose span (about W + 2H steps) leaves most of the GPU idle.  A
+// batch groups its pairs by kernel class (padded disparity count, path set,
+// arithmetic mode, full padding) and runs each group's aggregation as ONE
+// persistent launch of the lockstep row-band sweeps over the bands of all its
+// pairs (wave_kernel.cuh, tickets in band-major order), so the wavefronts of
+// different pairs fill the GPU together.  Cost volumes and the selection run
+// per pair around it.  Buffers come from one pooled device allocation reused
+// group after group, sized by a device-memory budget; with graphs enabled the
+// whole run is captured once into a CUDA graph and replayed.  Every pair's
+// output equals lumen_sgbm_compute_device's for the same pair bit for bit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <sstream>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/lumen_sgbm.h"
+#include "common.cuh"
+#include "kernels.cuh"
+#include "wave_kernel.cuh"
+
+using namespace lumen;
+
+namespace {
+
+struct BatchPair {
+    lumen_stereo_params p;
+    const uint8_t* left;
+    const uint8_t* right;
+    int W, H;
+    int16_t* out;
+    // derived
+    int D, Dp, r, cap;
+    bool census, diag, wrap, full;
+    SgmConsts k;
+    int nBands;
+    // pool offsets (bytes)
+    size_t oCost, oAgg, oPartB, oDispL, oDispR, oAux0, oAux1, oRing, oCtr;
+};
+
+struct BatchGroup {
+    int Dp;
+    bool diag, wrap, full;
+    std::vector<int> pairs;
+    int Wmax = 0;
+    WavePlan plan{};
+    int nTickets = 0;
+    size_t ctrOff = 0, ctrWords = 0;  // pool offset / size of the group's counters (prod, cons, ticket)
+    size_t jobsOff = 0, tableOff = 0;  // offsets in the descriptor buffer
+};
+
+lumen_status bfail(lumen_status s, const std::string& m) { return set_error(s, m); }
+
+#define BCU(call)                                                                              \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return bfail(LUMEN_ERR_CUDA, std::string("CUDA error in ") + #call + ": " +       \
+                                             cudaGetErrorString(e_));                          \
+    } while (0)
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Same rule as the plain call: every uint16 quantity provably stays in range.
+bool batch_no_wrap(const lumen_stereo_params& p, int cs, int nPaths) {
+    if (p.P1 < 0 || cs < 0) return false;
+    if (std::abs((long long)p.P2) >= (1ll << 27)) return false;
+    const long long cmax = 255ll * cs;
+    const long long p2max = std::max<long long>((long long)p.P1 + 1, (long long)p.P2);
+    const long long lmax = cmax + p2max;
+    return cmax <= 65535 && lmax + p.P1 <= 65535 && lmax + p2max <= 65535 && lmax * nPaths <= 65535;
+}
+
+}  // namespace
+
+struct lumen_sgbm_batch {
+    std::vector<BatchPair> pairs;
+    std::vector<BatchGroup> groups;
+    bool planned = false;
+    int rows = 0;       // rows per band (0: 8)
+    int useGraph = 0;
+    size_t budget = 48ull << 30;
+    int numSMs = 148;
+    long long spinMax = 1ll << 22;
+    void* pool = nullptr;
+    size_t poolBytes = 0;
+    void* desc = nullptr;  // WaveJob arrays and ticket tables of all groups
+    size_t descBytes = 0;
+    uint32_t* magic = nullptr;
+    int* status = nullptr;
+    cudaStream_t capStream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long launches = 0;  // kernels per run
+};
+
+static void batch_release(lumen_sgbm_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    if (b->pool) cudaFree(b->pool);
+    if (b->desc) cudaFree(b->desc);
+    b->pool = b->desc = nullptr;
+    b->poolBytes = b->descBytes = 0;
+    b->planned = false;
+}
+
+// Buffers, groups, job descriptors and ticket tables for the current pairs.
+static lumen_status batch_plan(lumen_sgbm_batch* b) {
+    batch_release(b);
+    const int R = b->rows ? b->rows : 8;
+    // classes
+    std::map<std::tuple<int, bool, bool, bool>, std::vector<int>> cls;
+    for (int i = 0; i < (int)b->pairs.size(); ++i) {
+        const BatchPair& q = b->pairs[i];
+        cls[std::make_tuple(q.Dp, q.diag, q.wrap, q.full)].push_back(i);
+    }
+    // groups: one class each, cut by the budget and by the hand-off bound
+    // (2 * pairs + 1 <= resident CTAs)
+    b->groups.clear();
+    size_t poolNeed = 0;
+    for (auto& kv : cls) {
+        const int Dp = std::get<0>(kv.first);
+        const bool diag = std::get<1>(kv.first), wrap = std::get<2>(kv.first), full = std::get<3>(kv.first);
+        BatchGroup g;
+        g.Dp = Dp;
+        g.diag = diag;
+        g.wrap = wrap;
+        g.full = full;
+        size_t bytes = 0;
+        int cap = 0;
+        auto flush = [&]() {
+            if (!g.pairs.empty()) {
+                poolNeed = std::max(poolNeed, bytes);
+                b->groups.push_back(g);
+            }
+            g.pairs.clear();
+            g.Wmax = 0;
+            bytes = 0;
+        };
+        for (int i : kv.second) {
+            BatchPair& q = b->pairs[i];
+            const size_t N = (size_t)q.W * q.H, ND = N * Dp;
+            q.nBands = (q.H + R - 1) / R;
+            const size_t need = align256(ND) + 2 * align256(ND * 2) + 2 * align256(N * 2) +
+                                2 * align256(q.census ? N * 4 : N) +
+                                align256(wave_ring_bytes(q.nBands, Dp, diag)) +
+                                align256((4 * (size_t)q.nBands + 32) * 4);
+            WavePlan pl{};
+            cudaError_t e = wave_batch_plan(std::max(g.Wmax, q.W), Dp, R, wrap, full, diag, b->numSMs, &pl);
+            if (e != cudaSuccess)
+                return bfail(LUMEN_ERR_INVALID_ARGUMENT,
+                             std::string("batch: no sweep configuration for a pair: ") + cudaGetErrorString(e));
+            cap = pl.grid;
+            if (!g.pairs.empty() && (bytes + need > b->budget || 2 * (int)(g.pairs.size() + 1) + 1 > cap)) flush();
+            if (need > b->budget)
+                return bfail(LUMEN_ERR_OUT_OF_BUDGET, "batch: one pair needs more device memory than the budget");
+            // offsets within the group's slice of the pool
+            size_t o = bytes;
+            auto take = [&](size_t n) { const size_t r0 = o; o += align256(n); return r0; };
+            q.oCost = take(ND);
+            q.oAgg = take(ND * 2);
+            q.oPartB = take(ND * 2);
+            q.oDispL = take(N * 2);
+            q.oDispR = take(N * 2);
+            q.oAux0 = take(q.census ? N * 4 : N);
+            q.oAux1 = take(q.census ? N * 4 : N);
+            q.oRing = take(wave_ring_bytes(q.nBands, Dp, diag));
+            q.oCtr = take((4 * (size_t)q.nBands + 32) * 4);
+            bytes = o;
+            g.pairs.push_back(i);
+            g.Wmax = std::max(g.Wmax, q.W);
+        }
+        flush();
+    }
+    // plans and descriptor layout
+    size_t dOff = 0;
+    for (BatchGroup& g : b->groups) {
+        cudaError_t e = wave_batch_plan(g.Wmax, g.Dp, R, g.wrap, g.full, g.diag, b->numSMs, &g.plan);
+        if (e != cudaSuccess) return bfail(LUMEN_ERR_CUDA, std::string("batch plan: ") + cudaGetErrorString(e));
+        g.nTickets = 0;
+        for (int i : g.pairs) g.nTickets += 2 * b->pairs[i].nBands;
+        g.jobsOff = dOff;
+        dOff = align256(dOff + sizeof(WaveJob) * g.pairs.size());
+        g.tableOff = dOff;
+        dOff = align256(dOff + sizeof(uint32_t) * (size_t)g.nTickets + 4);  // + the ticket counter
+    }
+    BCU(cudaMalloc(&b->pool, std::max<size_t>(poolNeed, 256)));
+    b->poolBytes = poolNeed;
+    BCU(cudaMalloc(&b->desc, std::max<size_t>(dOff, 256)));
+    b->descBytes = dOff;
+    // job descriptors and band-major ticket tables
+    uint8_t* base = static_cast<uint8_t*>(b->pool);
+    std::vector<uint8_t> host(dOff, 0);
+    for (BatchGroup& g : b->groups) {
+        WaveJob* jobs = reinterpret_cast<WaveJob*>(host.data() + g.jobsOff);
+        uint32_t* table = reinterpret_cast<uint32_t*>(host.data() + g.tableOff);
+        int maxB = 0;
+        for (int j = 0; j < (int)g.pairs.size(); ++j) {
+            const BatchPair& q = b->pairs[g.pairs[j]];
+            PairView pv{reinterpret_cast<const uint8_t*>(base + q.oCost), q.left,
+                        reinterpret_cast<uint16_t*>(base + q.oAgg)};
+            jobs[j] = wave_job(pv, reinterpret_cast<uint16_t*>(base + q.oPartB), q.k, R, base + q.oRing,
+                               reinterpret_cast<unsigned*>(base + q.oCtr));
+            maxB = std::max(maxB, q.nBands);
+        }
+        int t = 0;
+        for (int band = 0; band < maxB; ++band)
+            for (int j = 0; j < (int)g.pairs.size(); ++j)
+                if (band < b->pairs[g.pairs[j]].nBands)
+                    for (int sw = 0; sw < 2; ++sw)
+                        table[t++] = ((uint32_t)j << 20) | ((uint32_t)sw << 19) | (uint32_t)band;
+    }
+    BCU(cudaMemcpy(b->desc, host.data(), dOff, cudaMemcpyHostToDevice));
+    b->planned = true;
+    return LUMEN_OK;
+}
+
+// Every launch of one run, enqueued on `s`.
+static lumen_status batch_enqueue(lumen_sgbm_batch* b, cudaStream_t s) {
+    uint8_t* base = static_cast<uint8_t*>(b->pool);
+    uint8_t* desc = static_cast<uint8_t*>(b->desc);
+    unsigned long long nl = 0;
+    for (const BatchGroup& g : b->groups) {
+        // counters of the group's pairs and the group's ticket
+        for (int i : g.pairs) {
+            const BatchPair& q = b->pairs[i];
+            BCU(cudaMemsetAsync(base + q.oCtr, 0, (4 * (size_t)q.nBands + 32) * 4, s));
+        }
+        unsigned* ticket = reinterpret_cast<unsigned*>(desc + g.tableOff + sizeof(uint32_t) * (size_t)g.nTickets);
+        BCU(cudaMemsetAsync(ticket, 0, 4, s));
+        // cost volumes
+        for (int i : g.pairs) {
+            const BatchPair& q = b->pairs[i];
+            uint8_t* cost = base + q.oCost;
+            if (q.census) {
+                uint32_t* c0 = reinterpret_cast<uint32_t*>(base + q.oAux0);
+                uint32_t* c1 = reinterpret_cast<uint32_t*>(base + q.oAux1);
+                launch_census(q.left, q.right, q.W, q.H, c0, c1, s);
+                BCU(launch_census_cost(c0, c1, q.W, q.H, q.D, q.Dp, q.p.minDisparity, cost, s));
+            } else {
+                uint8_t* p0 = base + q.oAux0;
+                uint8_t* p1 = base + q.oAux1;
+                launch_prefilter(q.left, q.right, q.W, q.H, q.cap, p0, p1, s);
+                const int wide = (long long)(2 * q.r + 1) * (2 * q.r + 1) * 2 * q.cap > 65535;
+                BCU(launch_sad_cost(p0, p1, q.W, q.H, q.D, q.Dp, q.p.minDisparity, q.r, b->magic, wide, cost, s));
+            }
+            nl += 2;
+        }
+        // one aggregation launch over all bands of the group
+        BCU(launch_aggregate_wave_batch(reinterpret_cast<const WaveJob*>(desc + g.jobsOff),
+                                        reinterpret_cast<const uint32_t*>(desc + g.tableOff), g.nTickets,
+                                        2 * (int)g.pairs.size(), g.Wmax, g.Dp, g.wrap, g.full, g.diag, g.plan,
+                                        ticket, b->status, b->spinMax, s));
+        nl += 1;
+        // selection and post-processing
+        for (int i : g.pairs) {
+            const BatchPair& q = b->pairs[i];
+            int16_t* dl = reinterpret_cast<int16_t*>(base + q.oDispL);
+            int16_t* dr = reinterpret_cast<int16_t*>(base + q.oDispR);
+            BCU(launch_select(reinterpret_cast<uint16_t*>(base + q.oAgg), reinterpret_cast<uint16_t*>(base + q.oPartB),
+                              q.wrap, q.W, q.H, q.D, q.Dp, q.p.minDisparity, q.p.uniquenessRatio, dl, dr, s));
+            const int lr = q.p.disp12MaxDiff >= 0 ? q.p.disp12MaxDiff * 16 : -1;
+            const int spk = q.p.speckleWindowSize > 0 ? std::min(q.p.speckleWindowSize, 25) : 0;
+            BCU(launch_post(dl, dr, q.W, q.H, lr, spk, q.p.speckleRange * 16, q.out, (size_t)q.W, nullptr, s));
+            nl += 2;
+        }
+    }
+    b->launches = nl;
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_sgbm_batch_create(lumen_sgbm_batch** out) {
+    if (!out) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "lumen_sgbm_batch_create: out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return bfail(LUMEN_ERR_NO_DEVICE, "no CUDA device available");
+    lumen_sgbm_batch* b = new lumen_sgbm_batch();
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&b->numSMs, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaMalloc(&b->status, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(b->status, 0, sizeof(int));
+    // reciprocal table for every SAD window up to 21x21 (blockSize <= 21)
+    if (e == cudaSuccess) e = cudaMalloc(&b->magic, 443 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = launch_magic(b->magic, 443, 0);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->capStream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        lumen_sgbm_batch_destroy(b);
+        return bfail(LUMEN_ERR_CUDA, std::string("lumen_sgbm_batch_create: ") + cudaGetErrorString(e));
+    }
+    *out = b;
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_sgbm_batch_destroy(lumen_sgbm_batch* b) {
+    if (!b) return LUMEN_OK;
+    cudaDeviceSynchronize();
+    batch_release(b);
+    if (b->status) cudaFree(b->status);
+    if (b->magic) cudaFree(b->magic);
+    if (b->capStream) cudaStreamDestroy(b->capStream);
+    delete b;
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_sgbm_batch_add(lumen_sgbm_batch* b, const lumen_stereo_params* p,
+                                             const uint8_t* d_left, const uint8_t* d_right, int width,
+                                             int height, int16_t* d_out) {
+    if (!b || !p) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "lumen_sgbm_batch_add: NULL argument");
+    if (!d_left || !d_right || width <= 0 || height <= 0)
+        return bfail(LUMEN_ERR_INVALID_ARGUMENT, "Input images are empty");
+    if (!d_out) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "output buffer is NULL");
+    const int D = p->maxDisparity - p->minDisparity;
+    if (D < 1)
+        return bfail(LUMEN_ERR_INVALID_ARGUMENT,
+                     "Invalid disparity range: maxDisparity must be greater than minDisparity");
+    if (D > LUMEN_MAX_DISPARITY_RANGE)
+        return bfail(LUMEN_ERR_RANGE_EXCEEDS_LIMIT,
+                     "Disparity range (maxDisparity - minDisparity) exceeds GPU limit (512). Reduce the search range.");
+    if (p->minDisparity < 0) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "minDisparity must be >= 0");
+    if (p->blockSize < 0 || p->blockSize > 21) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "blockSize must be in [0, 21]");
+    if (width < 2) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "image width must be at least 2");
+    if ((long long)p->maxDisparity * 16 > 32767)
+        return bfail(LUMEN_ERR_INVALID_ARGUMENT, "maxDisparity*16 must fit int16 disparities");
+    if (b->pairs.size() >= 4095) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "a batch holds at most 4095 pairs");
+    BatchPair q{};
+    q.p = *p;
+    q.left = d_left;
+    q.right = d_right;
+    q.W = width;
+    q.H = height;
+    q.out = d_out;
+    q.D = D;
+    q.Dp = padded_d(D);
+    q.census = p->matchingCostMode == 1;
+    q.diag = p->numDirections >= 8;
+    q.r = p->blockSize / 2;
+    q.cap = std::max(1, p->preFilterCap);
+    const int cs = q.census ? std::max(1, (p->blockSize * p->blockSize * 2 * p->preFilterCap) / 255)
+                            : p->blockSize * p->blockSize;
+    q.wrap = !batch_no_wrap(*p, cs, q.diag ? 8 : 4);
+    q.full = q.D == q.Dp;
+    q.k.W = width; q.k.H = height; q.k.D = D; q.k.Dp = q.Dp;
+    q.k.P1 = p->P1; q.k.P2 = p->P2; q.k.costScale = cs;
+    q.k.p1x2 = ((uint32_t)p->P1 & 0xFFFFu) * 0x10001u;
+    q.k.bsub = ((uint32_t)(0xFFFF - p->P1) & 0xFFFFu) * 0x10001u;
+    b->pairs.push_back(q);
+    b->planned = false;
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_sgbm_batch_clear(lumen_sgbm_batch* b) {
+    if (!b) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "NULL batch");
+    cudaDeviceSynchronize();
+    b->pairs.clear();
+    batch_release(b);
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_sgbm_batch_set_options(lumen_sgbm_batch* b, int rows_per_band, int use_graph,
+                                                     size_t device_budget_bytes) {
+    if (!b) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "NULL batch");
+    if (rows_per_band != 0 && rows_per_band != 4 && rows_per_band != 8 && rows_per_band != 16)
+        return bfail(LUMEN_ERR_INVALID_ARGUMENT, "rows_per_band must be 0, 4, 8 or 16");
+    cudaDeviceSynchronize();
+    b->rows = rows_per_band;
+    b->useGraph = use_graph ? 1 : 0;
+    if (device_budget_bytes) b->budget = device_budget_bytes;
+    batch_release(b);
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_sgbm_batch_run(lumen_sgbm_batch* b, void* stream) {
+    if (!b) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "NULL batch");
+    if (b->pairs.empty()) return LUMEN_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!b->planned) {
+        lumen_status st = batch_plan(b);
+        if (st != LUMEN_OK) return st;
+    }
+    if (!b->useGraph) return batch_enqueue(b, s);
+    if (!b->exec) {
+        BCU(cudaStreamBeginCapture(b->capStream, cudaStreamCaptureModeThreadLocal));
+        lumen_status st = batch_enqueue(b, b->capStream);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(b->capStream, &g);
+        if (st != LUMEN_OK) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        BCU(e);
+        b->graph = g;
+        BCU(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    }
+    BCU(cudaGraphLaunch(b->exec, s));
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_sgbm_batch_sync(lumen_sgbm_batch* b, void* stream) {
+    if (!b) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "NULL batch");
+    BCU(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    int st = 0;
+    BCU(cudaMemcpy(&st, b->status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st != 0) {
+        cudaMemset(b->status, 0, sizeof(int));
+        return bfail(static_cast<lumen_status>(st), "a bounded device-side wait timed out in a batched sweep");
+    }
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_sgbm_batch_info(const lumen_sgbm_batch* b, size_t* device_bytes,
+                                              int* groups, unsigned long long* launches) {
+    if (!b) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "NULL batch");
+    if (device_bytes) *device_bytes = b->poolBytes + b->descBytes;
+    if (groups) *groups = (int)b->groups.size();
+    if (launches) *launches = b->launches;
+    return LUMEN_OK;
+}

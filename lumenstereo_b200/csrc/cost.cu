@@ -386,9 +386,24 @@ sad_cost_kernel(const uint8_t* __restrict__ pl, const uint8_t* __restrict__ pr, 
     }
 }
 
+// ceil(2^32 / c) for c >= 2 (c = 0, 1 unused): sum / c == umulhi(sum, m[c])
+// whenever sum * (m[c]*c - 2^32) < 2^32, which holds for every SAD window sum.
+__global__ void magic_kernel(uint32_t* m, int n) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    m[c] = c >= 2 ? (uint32_t)((0x100000000ull + (unsigned long long)c - 1ull) /
+                               (unsigned long long)c)
+                  : 0u;
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+cudaError_t launch_magic(uint32_t* m, int n, cudaStream_t s) {
+    magic_kernel<<<(n + 255) / 256, 256, 0, s>>>(m, n);
+    return cudaGetLastError();
+}
+
 void launch_stage_gray(const uint8_t* l, const uint8_t* r, size_t pitch, int channels, int W,
                        int H, uint8_t* gl, uint8_t* gr, cudaStream_t s, int nImages) {
     dim3 g((W + 255) / 256, H, nImages);

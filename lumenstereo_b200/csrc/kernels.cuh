@@ -24,6 +24,8 @@ void launch_census(const uint8_t* gl, const uint8_t* gr, int W, int H, uint32_t*
 cudaError_t launch_census_cost(const uint32_t* cl, const uint32_t* cr, int W, int H, int D, int Dp,
                                int minD, uint8_t* cost, cudaStream_t s);
 size_t sad_cost_smem(int Dp, int r);
+// Reciprocal table of the SAD window sizes: m[c] = ceil(2^32 / c), n entries.
+cudaError_t launch_magic(uint32_t* m, int n, cudaStream_t s);
 cudaError_t launch_sad_cost(const uint8_t* pl, const uint8_t* pr, int W, int H, int D, int Dp,
                             int minD, int r, const uint32_t* magic, int wide, uint8_t* cost,
                             cudaStream_t s);
@@ -85,6 +87,19 @@ struct WavePlan {
 };
 int wave_rows_options(int Dp, int* out, int max);
 cudaError_t wave_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSMs, WavePlan* plan);
+// Batched form: one launch over the bands of several pairs of one kernel
+// class (padded disparity count, path set, arithmetic mode).  d_jobs / d_table
+// live in device memory (see wave_kernel.cuh for their layout).
+struct WaveJob;
+size_t wave_ring_bytes(int nBands, int Dp, bool diag);
+WaveJob wave_job(const PairView& pv, uint16_t* partB, const SgmConsts& k, int R, uint8_t* xring,
+                 unsigned* counters);
+cudaError_t wave_batch_plan(int Wmax, int Dp, int R, bool wrap, bool full, bool diag, int numSMs,
+                            WavePlan* plan);
+cudaError_t launch_aggregate_wave_batch(const WaveJob* d_jobs, const uint32_t* d_table, int nTickets,
+                                        int nStreams, int Wmax, int Dp, bool wrap, bool full,
+                                        bool diag, const WavePlan& plan, unsigned* ticket,
+                                        int* status, long long spinMax, cudaStream_t s);
 cudaError_t launch_aggregate_wave(const PairView& pv, uint16_t* partB, const SgmConsts& k,
                                   bool wrap, bool diag, const WavePlan& plan, uint8_t* xring,
                                   unsigned* counters, int* status, long long spinMax,

@@ -9,8 +9,8 @@
 namespace lumen {
 
 #define LUMEN_WAVE_DECL(KW)                                                                    \
-    cudaError_t wave_dispatch_##KW(const WaveArgs& a, int R, int NP, bool wrap, int smem,      \
-                                   int grid, cudaStream_t s, int* perSM);
+    cudaError_t wave_dispatch_##KW(const WaveArgs& a, int R, int NP, bool wrap, bool full,     \
+                                   int smem, int grid, cudaStream_t s, int* perSM);
 LUMEN_WAVE_DECL(1)
 LUMEN_WAVE_DECL(2)
 LUMEN_WAVE_DECL(3)
@@ -20,17 +20,17 @@ LUMEN_WAVE_DECL(6)
 LUMEN_WAVE_DECL(7)
 LUMEN_WAVE_DECL(8)
 
-static cudaError_t dispatch_wave(const WaveArgs& a, int R, int NP, bool wrap, int smem, int grid,
-                                 cudaStream_t s, int* perSM) {
+static cudaError_t dispatch_wave(const WaveArgs& a, int R, int NP, bool wrap, bool full, int smem,
+                                 int grid, cudaStream_t s, int* perSM) {
     switch (a.Dp / 64) {
-    case 1: return wave_dispatch_1(a, R, NP, wrap, smem, grid, s, perSM);
-    case 2: return wave_dispatch_2(a, R, NP, wrap, smem, grid, s, perSM);
-    case 3: return wave_dispatch_3(a, R, NP, wrap, smem, grid, s, perSM);
-    case 4: return wave_dispatch_4(a, R, NP, wrap, smem, grid, s, perSM);
-    case 5: return wave_dispatch_5(a, R, NP, wrap, smem, grid, s, perSM);
-    case 6: return wave_dispatch_6(a, R, NP, wrap, smem, grid, s, perSM);
-    case 7: return wave_dispatch_7(a, R, NP, wrap, smem, grid, s, perSM);
-    case 8: return wave_dispatch_8(a, R, NP, wrap, smem, grid, s, perSM);
+    case 1: return wave_dispatch_1(a, R, NP, wrap, full, smem, grid, s, perSM);
+    case 2: return wave_dispatch_2(a, R, NP, wrap, full, smem, grid, s, perSM);
+    case 3: return wave_dispatch_3(a, R, NP, wrap, full, smem, grid, s, perSM);
+    case 4: return wave_dispatch_4(a, R, NP, wrap, full, smem, grid, s, perSM);
+    case 5: return wave_dispatch_5(a, R, NP, wrap, full, smem, grid, s, perSM);
+    case 6: return wave_dispatch_6(a, R, NP, wrap, full, smem, grid, s, perSM);
+    case 7: return wave_dispatch_7(a, R, NP, wrap, full, smem, grid, s, perSM);
+    case 8: return wave_dispatch_8(a, R, NP, wrap, full, smem, grid, s, perSM);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -44,71 +44,122 @@ int wave_rows_options(int Dp, int* out, int max) {
     return n;
 }
 
-static WaveArgs wave_base_args(const SgmConsts& k, int nBands, int Q) {
-    WaveArgs a{};
-    a.W = k.W; a.H = k.H; a.D = k.D; a.Dp = k.Dp;
-    a.P1 = k.P1; a.P2 = k.P2; a.costScale = k.costScale;
-    a.p1x2 = k.p1x2; a.bsub = k.bsub;
-    a.nBands = nBands;
-    a.QI = Q;
-    a.QX = Q;
-    return a;
-}
-
-cudaError_t wave_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSMs, WavePlan* plan) {
+// Shared-memory fit (largest helper rings) and occupancy of one kernel class
+// at a widest image Wmax.
+static cudaError_t plan_class(int Wmax, int Dp, int R, bool wrap, bool full, bool diag, int numSMs,
+                              WavePlan* plan) {
     if (R != 4 && R != 8 && R != 16) return cudaErrorInvalidValue;
     const int NP = diag ? 3 : 1;
     int dev = 0, maxSmem = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&maxSmem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    // largest helper rings that fit
     int Q = 0;
     WaveSmem L{};
     for (int q : {16, 8}) {
-        L = wave_smem(k.W, k.Dp, R, NP, q, q);
+        L = wave_smem(Wmax, Dp, R, NP, q, q);
         if (L.total <= maxSmem) {
             Q = q;
             break;
         }
     }
     if (!Q) return cudaErrorInvalidConfiguration;
-    const int nBands = (k.H + R - 1) / R;
-    WaveArgs a = wave_base_args(k, nBands, Q);
+    WaveArgs a{};
+    a.Dp = Dp;
+    a.Wmax = Wmax;
+    a.QI = a.QX = Q;
     int perSM = 0;
-    cudaError_t e = dispatch_wave(a, R, NP, wrap, L.total, 0, nullptr, &perSM);
+    cudaError_t e = dispatch_wave(a, R, NP, wrap, full, L.total, 0, nullptr, &perSM);
     if (e != cudaSuccess) return e;
     if (perSM < 1) return cudaErrorInvalidConfiguration;
     plan->R = R;
     plan->Q = Q;
-    plan->nBands = nBands;
-    plan->grid = std::min(2 * nBands, perSM * numSMs);
     plan->smem = L.total;
-    plan->ringBytes = 2 * (size_t)nBands * kWK * (size_t)wave_slot_bytes(k.Dp, NP);
-    plan->counterWords = 4 * (size_t)nBands + 32;
+    plan->grid = perSM * numSMs;  // capacity; callers clamp to their ticket count
     return cudaSuccess;
+}
+
+size_t wave_ring_bytes(int nBands, int Dp, bool diag) {
+    return 2 * (size_t)nBands * kWK * (size_t)wave_slot_bytes(Dp, diag ? 3 : 1);
+}
+
+cudaError_t wave_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSMs, WavePlan* plan) {
+    cudaError_t e = plan_class(k.W, k.Dp, R, wrap, k.D == k.Dp, diag, numSMs, plan);
+    if (e != cudaSuccess) return e;
+    plan->nBands = (k.H + R - 1) / R;
+    plan->grid = std::min(2 * plan->nBands, plan->grid);
+    plan->ringBytes = wave_ring_bytes(plan->nBands, k.Dp, diag);
+    plan->counterWords = 4 * (size_t)plan->nBands + 32;
+    return cudaSuccess;
+}
+
+WaveJob wave_job(const PairView& pv, uint16_t* partB, const SgmConsts& k, int R, uint8_t* xring,
+                 unsigned* counters) {
+    WaveJob j{};
+    j.cost = pv.cost;
+    j.img = pv.img;
+    j.part[0] = pv.agg;
+    j.part[1] = partB;
+    j.xring = xring;
+    j.nBands = (k.H + R - 1) / R;
+    j.prod = counters;
+    j.cons = counters + 2 * j.nBands;
+    j.W = k.W; j.H = k.H; j.D = k.D;
+    j.P1 = k.P1; j.P2 = k.P2; j.costScale = k.costScale;
+    j.p1x2 = k.p1x2; j.bsub = k.bsub;
+    return j;
 }
 
 cudaError_t launch_aggregate_wave(const PairView& pv, uint16_t* partB, const SgmConsts& k,
                                   bool wrap, bool diag, const WavePlan& plan, uint8_t* xring,
                                   unsigned* counters, int* status, long long spinMax,
                                   cudaStream_t s, int stallTest, unsigned long long* trace) {
-    WaveArgs a = wave_base_args(k, plan.nBands, plan.Q);
-    a.cost = pv.cost;
-    a.img = pv.img;
-    a.part[0] = pv.agg;
-    a.part[1] = partB;
-    a.xring = xring;
-    a.prod = counters;
-    a.cons = counters + 2 * plan.nBands;
+    WaveArgs a{};
+    a.job = wave_job(pv, partB, k, plan.R, xring, counters);
+    a.jobs = nullptr;
+    a.table = nullptr;
+    a.nTickets = 2 * plan.nBands;
+    a.Wmax = k.W;
     a.ticket = counters + 4 * plan.nBands;
     a.status = status;
+    a.Dp = k.Dp;
+    a.QI = a.QX = plan.Q;
     a.spinMax = spinMax;
     a.stallTest = stallTest;
     a.trace = trace;
     cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned) * plan.counterWords, s);
     if (e != cudaSuccess) return e;
     int dummy = 0;
-    return dispatch_wave(a, plan.R, diag ? 3 : 1, wrap, plan.smem, plan.grid, s, &dummy);
+    return dispatch_wave(a, plan.R, diag ? 3 : 1, wrap, k.D == k.Dp, plan.smem, plan.grid, s, &dummy);
+}
+
+cudaError_t wave_batch_plan(int Wmax, int Dp, int R, bool wrap, bool full, bool diag, int numSMs,
+                            WavePlan* plan) {
+    return plan_class(Wmax, Dp, R, wrap, full, diag, numSMs, plan);
+}
+
+cudaError_t launch_aggregate_wave_batch(const WaveJob* d_jobs, const uint32_t* d_table, int nTickets,
+                                        int nStreams, int Wmax, int Dp, bool wrap, bool full,
+                                        bool diag, const WavePlan& plan, unsigned* ticket,
+                                        int* status, long long spinMax, cudaStream_t s) {
+    // every band waits only on earlier tickets, and a band's successor is at
+    // most nStreams tickets later, so nStreams + 1 running CTAs always include
+    // it: no hand-off can wait on a band that has no CTA
+    const int grid = std::min(nTickets, plan.grid);
+    if (grid < std::min(nTickets, nStreams + 1)) return cudaErrorInvalidConfiguration;
+    WaveArgs a{};
+    a.jobs = d_jobs;
+    a.table = d_table;
+    a.nTickets = nTickets;
+    a.Wmax = Wmax;
+    a.ticket = ticket;
+    a.status = status;
+    a.Dp = Dp;
+    a.QI = a.QX = plan.Q;
+    a.spinMax = spinMax;
+    a.stallTest = 0;
+    a.trace = nullptr;
+    int dummy = 0;
+    return dispatch_wave(a, plan.R, diag ? 3 : 1, wrap, full, plan.smem, grid, s, &dummy);
 }
 
 }  // namespace lumen

@@ -27,10 +27,9 @@ cudaError_t wave_launch_np(const WaveArgs& a, bool wrap, bool full, int smem, in
 }
 
 template <int KP>
-cudaError_t wave_dispatch_kp(const WaveArgs& a, int R, int NP, bool wrap, int smem, int grid,
-                             cudaStream_t s, int* perSM) {
+cudaError_t wave_dispatch_kp(const WaveArgs& a, int R, int NP, bool wrap, bool full, int smem,
+                             int grid, cudaStream_t s, int* perSM) {
     constexpr int KW = KP;
-    const bool full = (a.D == a.Dp);
     if (R == 4) return NP == 3 ? wave_launch_np<KW, 3, 4>(a, wrap, full, smem, grid, s, perSM)
                                : wave_launch_np<KW, 1, 4>(a, wrap, full, smem, grid, s, perSM);
     if (R == 8) return NP == 3 ? wave_launch_np<KW, 3, 8>(a, wrap, full, smem, grid, s, perSM)
@@ -44,8 +43,8 @@ cudaError_t wave_dispatch_kp(const WaveArgs& a, int R, int NP, bool wrap, int sm
 
 #define LUMEN_WAVE_INSTANCE(KP)                                                                \
     namespace lumen {                                                                          \
-    cudaError_t wave_dispatch_##KP(const WaveArgs& a, int R, int NP, bool wrap, int smem,      \
-                                   int grid, cudaStream_t s, int* perSM) {                     \
-        return wave_dispatch_kp<KP>(a, R, NP, wrap, smem, grid, s, perSM);                     \
+    cudaError_t wave_dispatch_##KP(const WaveArgs& a, int R, int NP, bool wrap, bool full,     \
+                                   int smem, int grid, cudaStream_t s, int* perSM) {           \
+        return wave_dispatch_kp<KP>(a, R, NP, wrap, full, smem, grid, s, perSM);               \
     }                                                                                          \
     }

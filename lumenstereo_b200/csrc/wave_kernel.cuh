@@ -60,23 +60,36 @@ constexpr int kWE = 4;     // export progress published every kWE pixels
 // flight: a deeper pipeline adds lag to every band hand-off, which costs more
 // than it hides.
 
-struct WaveArgs {
+// One stereo pair of a launch: its volumes, exchange rings and parameters.
+struct WaveJob {
     const uint8_t* cost;     // [H][W][Dp]
     const uint8_t* img;      // [H][W] left gray image (adaptive P2)
     uint16_t* part[2];       // per-sweep partial sums, [H][W][Dp]
     uint8_t* xring;          // [2][nBands][kWK][SB] exchange rings
     unsigned* prod;          // [2][nBands] pixels band b has exported
     unsigned* cons;          // [2][nBands] pixels of band b's ring band b+1 has copied
-    unsigned* ticket;        // next band ticket
-    int* status;
-    int W, H, D, Dp;
+    int W, H, D, nBands;     // nBands: bands per sweep
     int P1, P2, costScale;
     uint32_t p1x2, bsub;
-    int nBands;              // bands per sweep
+};
+
+// A launch: one pair (`job`, tickets t -> sweep t & 1, band t >> 1) or a batch
+// of pairs of one kernel class (`jobs`, tickets through `table`, each entry
+// pair << 20 | sweep << 19 | band, every band listed after the band before it
+// in its own sweep).
+struct WaveArgs {
+    WaveJob job;             // the pair when jobs == nullptr
+    const WaveJob* jobs;     // batch: [pairs]
+    const uint32_t* table;   // batch: [nTickets]
+    int nTickets;
+    int Wmax;                // widest image (shared-memory carve-up)
+    unsigned* ticket;        // next ticket
+    int* status;
+    int Dp;
     int QI, QX;              // import / export ring slots (16 or 8)
     long long spinMax;
-    int stallTest;           // 1: the first band with a predecessor waits on a pixel never exported
-    unsigned long long* trace;  // optional [2*nBands][4] band timeline
+    int stallTest;           // 1: ticket 2 (a band with a predecessor) waits on a pixel never exported
+    unsigned long long* trace;  // optional [nTickets][4] band timeline
 };
 
 // Band timeline record (diagnostics, lumen_sgbm_debug_trace): per ticket t,
@@ -294,7 +307,7 @@ wave_kernel(WaveArgs a) {
     constexpr int CPV = DP / 16;         // 16-byte cost chunks per pixel
     static_assert(CPV <= 32, "one cost chunk per lane");
     extern __shared__ __align__(128) uint8_t sm[];
-    const WaveSmem L = wave_smem(a.W, DP, R, NP, a.QI, a.QX);
+    const WaveSmem L = wave_smem(a.Wmax, DP, R, NP, a.QI, a.QX);
     const int QI = a.QI, QX = a.QX;
     uint8_t* simg = sm + L.img;
     const uint32_t* p2lut = reinterpret_cast<const uint32_t*>(sm + L.lut);
@@ -305,38 +318,57 @@ wave_kernel(WaveArgs a) {
     unsigned* sctr = reinterpret_cast<unsigned*>(sm + L.misc) + 8;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int W = a.W, H = a.H;
     const int off = lane * 2 * KW;  // first disparity of this lane
 
-    // adaptive P2 (src/sgbm_kernels.cu:301-310) as a table of |dI|, replicated in both halves
-    for (int g = threadIdx.x; g < 256; g += blockDim.x)
-        reinterpret_cast<uint32_t*>(sm + L.lut)[g] =
-            ((uint32_t)max(a.P1 + 1, a.P2 * 8 / max(8, g)) & 0xFFFFu) * 0x10001u;
     if (threadIdx.x == 0) sflag[1] = 0;
     for (int i = threadIdx.x; i < SB / 4; i += blockDim.x)
         reinterpret_cast<uint32_t*>(sm + L.zero)[i] = 0u;
     __syncthreads();
 
     LaneMasks<KW> mk;
-    make_lane_masks<KW>(lane, a.D, mk);
+    int lutP1 = -1, lutP2 = -1, maskD = -1;  // parameters the table and masks were built for
 
     for (;;) {
         if (threadIdx.x == 0) {
             int t = (int)atomicAdd(a.ticket, 1u);
-            if (*(volatile int*)a.status != 0) t = 2 * a.nBands;
+            if (*(volatile int*)a.status != 0) t = a.nTickets;
             sflag[0] = t;
             sflag[2] = 0; sflag[3] = 0; sflag[4] = 0;
         }
         if (threadIdx.x < 4) sctr[threadIdx.x] = 0u;
         __syncthreads();
         const int t = sflag[0];
-        if (t >= 2 * a.nBands) break;
+        if (t >= a.nTickets) break;
         unsigned long long tTaken = 0;
         if (a.trace && threadIdx.x == 0) tTaken = wave_now();
-        const int sw = t & 1, b = t >> 1;
+        int sw, b;
+        WaveJob J;
+        if (a.jobs) {
+            const uint32_t e = a.table[t];
+            J = a.jobs[e >> 20];
+            sw = (e >> 19) & 1;
+            b = (int)(e & 0x7FFFFu);
+        } else {
+            J = a.job;
+            sw = t & 1;
+            b = t >> 1;
+        }
+        const int W = J.W, H = J.H;
+        if (J.P1 != lutP1 || J.P2 != lutP2) {
+            // adaptive P2 (src/sgbm_kernels.cu:301-310) as a table of |dI|, replicated in both halves
+            for (int g = threadIdx.x; g < 256; g += blockDim.x)
+                reinterpret_cast<uint32_t*>(sm + L.lut)[g] =
+                    ((uint32_t)max(J.P1 + 1, J.P2 * 8 / max(8, g)) & 0xFFFFu) * 0x10001u;
+            lutP1 = J.P1;
+            lutP2 = J.P2;
+        }
+        if (J.D != maskD) {
+            make_lane_masks<KW>(lane, J.D, mk);
+            maskD = J.D;
+        }
         const int v0 = b * R;
         const int lastActive = min(R - 1, H - 1 - v0);
-        const bool hasPrev = b > 0, hasNext = b + 1 < a.nBands;
+        const bool hasPrev = b > 0, hasNext = b + 1 < J.nBands;
         // ---- stage sweep-oriented image rows v0-1 .. v0+R-1 ----
         for (int i = threadIdx.x; i < (R + 1) * W; i += blockDim.x) {
             const int rr = i / W, u = i - rr * W;
@@ -344,7 +376,7 @@ wave_kernel(WaveArgs a) {
             uint8_t val = 0;
             if (vv >= 0 && vv < H) {
                 const int x = sw ? W - 1 - u : u, y = sw ? H - 1 - vv : vv;
-                val = a.img[(size_t)y * W + x];
+                val = J.img[(size_t)y * W + x];
             }
             simg[rr * L.Wp + u] = val;
         }
@@ -372,13 +404,13 @@ wave_kernel(WaveArgs a) {
             uint8_t* const costRing = sm + L.cost + r * kWPF * DP;
             const uint8_t* irow = simg + (r + 1) * L.Wp;
             const uint8_t* iprev = simg + r * L.Wp;
-            uint16_t* pout = (sw ? a.part[1] : a.part[0]) + ((size_t)y * W + (sw ? W - 1 : 0)) * DP + off;
+            uint16_t* pout = (sw ? J.part[1] : J.part[0]) + ((size_t)y * W + (sw ? W - 1 : 0)) * DP + off;
             const ptrdiff_t pstep = sw ? -(ptrdiff_t)DP : (ptrdiff_t)DP;
             // Cost prefetch: when a lane's 2*KW cost bytes are a multiple of 4 it
             // copies exactly its own bytes (no cross-lane dependency); otherwise
             // the first DP/16 lanes copy 16-byte chunks and the warp syncs.
             constexpr bool OWN = (KW % 2) == 0;
-            const uint8_t* cgrow = a.cost + (size_t)y * W * DP;
+            const uint8_t* cgrow = J.cost + (size_t)y * W * DP;
             auto prefetch = [&](int step) {
                 const int p = step - LAG * r + kWPF - 1;
                 if (rowOn && p >= 0 && p < W) {
@@ -424,9 +456,9 @@ wave_kernel(WaveArgs a) {
                 if (!OWN) __syncwarp();
                 uint32_t Cw[KW];
                 load_cost_words<KW>(costRing + (uc % kWPF) * DP + off, Cw);
-                if (WRAP || a.costScale != 1) {
+                if (WRAP || J.costScale != 1) {
 #pragma unroll
-                    for (int w = 0; w < KW; ++w) Cw[w] = scale_cost<WRAP>(Cw[w], a.costScale);
+                    for (int w = 0; w < KW; ++w) Cw[w] = scale_cost<WRAP>(Cw[w], J.costScale);
                 }
                 // ---- adaptive P2 of this pixel: H path, V, D1 (u-1, v-1), D2 (u+1, v-1) ----
                 const int cur = irow[uc];
@@ -435,7 +467,7 @@ wave_kernel(WaveArgs a) {
                                          p2lut[abs(cur - iprev[min(uc + 1, W - 1)])]};
                 // ---- horizontal path ----
                 uint32_t LnH[KW];
-                wave_step<KW, 32, WRAP, FULL>(LH, Cw, minH, p2h, a.p1x2, a.bsub, mk, LnH);
+                wave_step<KW, 32, WRAP, FULL>(LH, Cw, minH, p2h, J.p1x2, J.bsub, mk, LnH);
                 // ---- vertical / diagonal paths from the previous row ----
                 uint32_t Ln[NP][KW], mn[NP];
 #pragma unroll
@@ -446,7 +478,7 @@ wave_kernel(WaveArgs a) {
                     uint32_t Lp[KW];
                     load_words<KW>(reinterpret_cast<const uint16_t*>(slot + pth * 2 * DP) + off, Lp);
                     const uint32_t mp = reinterpret_cast<const uint32_t*>(slot + NP * 2 * DP)[pth];
-                    wave_step<KW, 32, WRAP, FULL>(Lp, Cw, mp, p2v[pth], a.p1x2, a.bsub, mk, Ln[pth]);
+                    wave_step<KW, 32, WRAP, FULL>(Lp, Cw, mp, p2v[pth], J.p1x2, J.bsub, mk, Ln[pth]);
                 }
                 // a row that has not reached its first pixel ran on dummy data: its
                 // horizontal-path state must stay at its start value (0)
@@ -494,9 +526,9 @@ wave_kernel(WaveArgs a) {
         } else if (warp == RW) {
             // ===================== import warp: previous band's last row =====================
             if (hasPrev) {
-                const uint8_t* xin = a.xring + ((size_t)(sw * a.nBands + b - 1) * kWK) * SB;
-                const unsigned* iprod = a.prod + sw * a.nBands + (b - 1);
-                unsigned* icons = a.cons + sw * a.nBands + (b - 1);
+                const uint8_t* xin = J.xring + ((size_t)(sw * J.nBands + b - 1) * kWK) * SB;
+                const unsigned* iprod = J.prod + sw * J.nBands + (b - 1);
+                unsigned* icons = J.cons + sw * J.nBands + (b - 1);
                 unsigned prodSeen = 0, r0Seen = 0;
                 const uint32_t impA = w_smem_addr(sm + L.imp);
                 for (int p = 0; p < W && ok; ++p) {
@@ -530,9 +562,9 @@ wave_kernel(WaveArgs a) {
         } else {
             // ===================== export warp: this band's last row =====================
             if (hasNext) {
-                uint8_t* xout = a.xring + ((size_t)(sw * a.nBands + b) * kWK) * SB;
-                unsigned* oprod = a.prod + sw * a.nBands + b;
-                const unsigned* ocons = a.cons + sw * a.nBands + b;
+                uint8_t* xout = J.xring + ((size_t)(sw * J.nBands + b) * kWK) * SB;
+                unsigned* oprod = J.prod + sw * J.nBands + b;
+                const unsigned* ocons = J.cons + sw * J.nBands + b;
                 unsigned availSeen = 0, consSeen = 0;
                 for (int u = 0; u < W && ok; ++u) {
                     ok = w_wait_cta(&sctr[2], (unsigned)(u + 1), availSeen, sflag + 1, a.status, a.spinMax);

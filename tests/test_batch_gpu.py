@@ -1,0 +1,65 @@
+"""Batched form (lumen_sgbm_batch_*): every pair of a mixed batch — sizes,
+disparity ranges, cost modes, path sets and parameters that wrap uint16 —
+gives exactly the disparity map of the plain device call for the same pair,
+whether the batch runs as one launch group, is split by a small device-memory
+budget into several, or is replayed from a captured CUDA graph.  Disparity maps
+are integers (1/16 px): the tolerance is zero."""
+import numpy as np
+import pytest
+
+from lumenstereo_b200 import MatchingCostMode, StereoBatch, StereoParams, StereoSGBM, synth
+
+pytestmark = pytest.mark.gpu
+
+MIX = [  # (w, h, params)
+    (160, 96, dict(maxDisparity=48, numDirections=8, matchingCostMode=MatchingCostMode.Census)),
+    (131, 53, dict(maxDisparity=64, numDirections=4)),
+    (200, 120, dict(maxDisparity=128, numDirections=8)),
+    (96, 40, dict(minDisparity=5, maxDisparity=37, numDirections=8, uniquenessRatio=0)),
+    (150, 70, dict(maxDisparity=150, numDirections=8, matchingCostMode=MatchingCostMode.Census)),
+    (120, 64, dict(maxDisparity=64, numDirections=8)),
+    (64, 48, dict(maxDisparity=16, numDirections=8, blockSize=19)),  # uint16 wrap
+    (310, 20, dict(maxDisparity=290, numDirections=8, matchingCostMode=MatchingCostMode.Census)),
+]
+
+
+def _pairs(torch):
+    out = []
+    for i, (w, h, kw) in enumerate(MIX):
+        left, right, _ = synth.make_pair(synth.PairSpec(w, h, 4, 1, min(40, kw["maxDisparity"] - 1), 2.0, 300 + i))
+        p = StereoParams(speckleWindowSize=0, **kw)
+        out.append((p, torch.from_numpy(left).cuda(), torch.from_numpy(right).cuda(), w, h))
+    return out
+
+
+def _plain(torch, pairs):
+    refs = []
+    for p, dl, dr, w, h in pairs:
+        o = torch.empty((h, w), dtype=torch.int16, device="cuda")
+        with StereoSGBM(p) as s:
+            s.compute_device(dl.data_ptr(), dr.data_ptr(), w, h, o.data_ptr())
+            torch.cuda.synchronize()
+        refs.append(o.cpu().numpy())
+    return refs
+
+
+@pytest.mark.parametrize("rows,graph,budget", [(0, False, 0), (4, False, 0), (16, True, 0), (8, True, 24 << 20)])
+def test_batch_matches_plain_calls(rows, graph, budget):
+    torch = pytest.importorskip("torch")
+    pairs = _pairs(torch)
+    refs = _plain(torch, pairs)
+    outs = [torch.full((h, w), 0x7ABC, dtype=torch.int16, device="cuda") for _, _, _, w, h in pairs]
+    with StereoBatch(rows_per_band=rows, use_graph=graph, budget_bytes=budget) as b:
+        for (p, dl, dr, w, h), o in zip(pairs, outs):
+            b.add(p, dl.data_ptr(), dr.data_ptr(), w, h, o.data_ptr())
+        for rep in range(2):  # the second run replays (graph) or reuses the plan
+            for o in outs:
+                o.fill_(0x7ABC)
+            b.run()
+            b.sync()
+            for i, (o, ref) in enumerate(zip(outs, refs)):
+                assert np.array_equal(o.cpu().numpy(), ref), (i, rep)
+        info = b.info()
+        if budget:
+            assert info["groups"] > 4, info  # the 24 MiB budget splits the larger classes
+        assert info["launches"] > 0
