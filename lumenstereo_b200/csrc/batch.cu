@@ -53,6 +53,7 @@ struct BatchGroup {
     int Wmax = 0;
     WavePlan plan{};
     int nTickets = 0;
+    int window = 0;  // ticket distance the oldest unfinished ticket may need running
     size_t ctrOff = 0, ctrWords = 0;  // pool offset / size of the group's counters (prod, cons, ticket)
     size_t jobsOff = 0, tableOff = 0;  // offsets in the descriptor buffer
 };
@@ -124,8 +125,7 @@ static lumen_status batch_plan(lumen_sgbm_batch* b) {
         const BatchPair& q = b->pairs[i];
         cls[std::make_tuple(q.Dp, q.diag, q.wrap, q.full)].push_back(i);
     }
-    // groups: one class each, cut by the budget and by the hand-off bound
-    // (2 * pairs + 1 <= resident CTAs)
+    // groups: one class each, cut by the budget
     b->groups.clear();
     size_t poolNeed = 0;
     for (auto& kv : cls) {
@@ -137,7 +137,6 @@ static lumen_status batch_plan(lumen_sgbm_batch* b) {
         g.wrap = wrap;
         g.full = full;
         size_t bytes = 0;
-        int cap = 0;
         auto flush = [&]() {
             if (!g.pairs.empty()) {
                 poolNeed = std::max(poolNeed, bytes);
@@ -160,8 +159,7 @@ static lumen_status batch_plan(lumen_sgbm_batch* b) {
             if (e != cudaSuccess)
                 return bfail(LUMEN_ERR_INVALID_ARGUMENT,
                              std::string("batch: no sweep configuration for a pair: ") + cudaGetErrorString(e));
-            cap = pl.grid;
-            if (!g.pairs.empty() && (bytes + need > b->budget || 2 * (int)(g.pairs.size() + 1) + 1 > cap)) flush();
+            if (!g.pairs.empty() && bytes + need > b->budget) flush();
             if (need > b->budget)
                 return bfail(LUMEN_ERR_OUT_OF_BUDGET, "batch: one pair needs more device memory than the budget");
             // offsets within the group's slice of the pool
@@ -204,21 +202,45 @@ static lumen_status batch_plan(lumen_sgbm_batch* b) {
     for (BatchGroup& g : b->groups) {
         WaveJob* jobs = reinterpret_cast<WaveJob*>(host.data() + g.jobsOff);
         uint32_t* table = reinterpret_cast<uint32_t*>(host.data() + g.tableOff);
-        int maxB = 0;
         for (int j = 0; j < (int)g.pairs.size(); ++j) {
             const BatchPair& q = b->pairs[g.pairs[j]];
             PairView pv{reinterpret_cast<const uint8_t*>(base + q.oCost), q.left,
                         reinterpret_cast<uint16_t*>(base + q.oAgg)};
             jobs[j] = wave_job(pv, reinterpret_cast<uint16_t*>(base + q.oPartB), q.k, R, base + q.oRing,
                                reinterpret_cast<unsigned*>(base + q.oCtr));
-            maxB = std::max(maxB, q.nBands);
         }
+        // Chunks of pairs, tickets band-major within a chunk (the chunk's
+        // wavefronts overlap), chunk after chunk.  A band may need the next
+        // wave_lookahead_bands(W) bands of its pair and sweep running, which
+        // band-major order puts up to 2 * n * lookahead tickets later in a
+        // chunk of n pairs: chunks stay small enough for that window to fit
+        // in the resident CTAs.
         int t = 0;
-        for (int band = 0; band < maxB; ++band)
-            for (int j = 0; j < (int)g.pairs.size(); ++j)
-                if (band < b->pairs[g.pairs[j]].nBands)
-                    for (int sw = 0; sw < 2; ++sw)
-                        table[t++] = ((uint32_t)j << 20) | ((uint32_t)sw << 19) | (uint32_t)band;
+        g.window = 0;
+        for (int j0 = 0; j0 < (int)g.pairs.size();) {
+            int j1 = j0, Wc = 0, nb = 0;
+            while (j1 < (int)g.pairs.size()) {
+                const BatchPair& q = b->pairs[g.pairs[j1]];
+                const int w2 = std::max(Wc, q.W);
+                if (j1 > j0 && 2 * (j1 - j0 + 1) * wave_lookahead_bands(w2) + 1 > g.plan.grid) break;
+                Wc = w2;
+                nb = std::max(nb, q.nBands);
+                ++j1;
+            }
+            int chunkTickets = 0;
+            for (int j = j0; j < j1; ++j) chunkTickets += 2 * b->pairs[g.pairs[j]].nBands;
+            // needs stay inside the chunk
+            const int win = std::min(2 * (j1 - j0) * wave_lookahead_bands(Wc), chunkTickets);
+            if (win + 1 > g.plan.grid)
+                return bfail(LUMEN_ERR_INVALID_ARGUMENT, "batch: a pair is too wide for the resident sweep CTAs");
+            g.window = std::max(g.window, win);
+            for (int band = 0; band < nb; ++band)
+                for (int j = j0; j < j1; ++j)
+                    if (band < b->pairs[g.pairs[j]].nBands)
+                        for (int sw = 0; sw < 2; ++sw)
+                            table[t++] = ((uint32_t)j << 20) | ((uint32_t)sw << 19) | (uint32_t)band;
+            j0 = j1;
+        }
     }
     BCU(cudaMemcpy(b->desc, host.data(), dOff, cudaMemcpyHostToDevice));
     b->planned = true;
@@ -259,7 +281,7 @@ static lumen_status batch_enqueue(lumen_sgbm_batch* b, cudaStream_t s) {
         // one aggregation launch over all bands of the group
         BCU(launch_aggregate_wave_batch(reinterpret_cast<const WaveJob*>(desc + g.jobsOff),
                                         reinterpret_cast<const uint32_t*>(desc + g.tableOff), g.nTickets,
-                                        2 * (int)g.pairs.size(), g.Wmax, g.Dp, g.wrap, g.full, g.diag, g.plan,
+                                        g.window, g.Wmax, g.Dp, g.wrap, g.full, g.diag, g.plan,
                                         ticket, b->status, b->spinMax, s));
         nl += 1;
         // selection and post-processing

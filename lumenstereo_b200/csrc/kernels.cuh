@@ -92,12 +92,14 @@ cudaError_t wave_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSM
 // live in device memory (see wave_kernel.cuh for their layout).
 struct WaveJob;
 size_t wave_ring_bytes(int nBands, int Dp, bool diag);
+// bands below a band that must run for it to finish a row of W pixels
+int wave_lookahead_bands(int W);
 WaveJob wave_job(const PairView& pv, uint16_t* partB, const SgmConsts& k, int R, uint8_t* xring,
                  unsigned* counters);
 cudaError_t wave_batch_plan(int Wmax, int Dp, int R, bool wrap, bool full, bool diag, int numSMs,
                             WavePlan* plan);
 cudaError_t launch_aggregate_wave_batch(const WaveJob* d_jobs, const uint32_t* d_table, int nTickets,
-                                        int nStreams, int Wmax, int Dp, bool wrap, bool full,
+                                        int window, int Wmax, int Dp, bool wrap, bool full,
                                         bool diag, const WavePlan& plan, unsigned* ticket,
                                         int* status, long long spinMax, cudaStream_t s);
 cudaError_t launch_aggregate_wave(const PairView& pv, uint16_t* partB, const SgmConsts& k,

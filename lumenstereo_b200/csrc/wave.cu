@@ -87,6 +87,9 @@ cudaError_t wave_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSM
     if (e != cudaSuccess) return e;
     plan->nBands = (k.H + R - 1) / R;
     plan->grid = std::min(2 * plan->nBands, plan->grid);
+    // tickets alternate the two sweeps band by band
+    if (plan->grid < std::min(2 * plan->nBands, 2 * wave_lookahead_bands(k.W) + 1))
+        return cudaErrorInvalidConfiguration;
     plan->ringBytes = wave_ring_bytes(plan->nBands, k.Dp, diag);
     plan->counterWords = 4 * (size_t)plan->nBands + 32;
     return cudaSuccess;
@@ -132,20 +135,30 @@ cudaError_t launch_aggregate_wave(const PairView& pv, uint16_t* partB, const Sgm
     return dispatch_wave(a, plan.R, diag ? 3 : 1, wrap, k.D == k.Dp, plan.smem, plan.grid, s, &dummy);
 }
 
+int wave_lookahead_bands(int W) {
+    // A band's export waits for the next band to consume its ring (kWK
+    // pixels), so a band that has no CTA stalls the band above it after
+    // kWK pixels, that one after about 2 * kWK, and so on: a band can finish
+    // a row of W pixels once the ceil(W / kWK) bands below it run too (one
+    // more for the in-band row lag and the import queue).
+    return (W + kWK - 1) / kWK + 1;
+}
+
 cudaError_t wave_batch_plan(int Wmax, int Dp, int R, bool wrap, bool full, bool diag, int numSMs,
                             WavePlan* plan) {
     return plan_class(Wmax, Dp, R, wrap, full, diag, numSMs, plan);
 }
 
 cudaError_t launch_aggregate_wave_batch(const WaveJob* d_jobs, const uint32_t* d_table, int nTickets,
-                                        int nStreams, int Wmax, int Dp, bool wrap, bool full,
+                                        int window, int Wmax, int Dp, bool wrap, bool full,
                                         bool diag, const WavePlan& plan, unsigned* ticket,
                                         int* status, long long spinMax, cudaStream_t s) {
-    // every band waits only on earlier tickets, and a band's successor is at
-    // most nStreams tickets later, so nStreams + 1 running CTAs always include
-    // it: no hand-off can wait on a band that has no CTA
+    // A CTA takes a ticket only while it runs, and the oldest unfinished
+    // ticket needs at most the next `window` tickets running (the bands it
+    // waits on and the bands whose ring back-pressure it feels): with
+    // window + 1 resident CTAs the oldest ticket always completes.
     const int grid = std::min(nTickets, plan.grid);
-    if (grid < std::min(nTickets, nStreams + 1)) return cudaErrorInvalidConfiguration;
+    if (grid < std::min(nTickets, window + 1)) return cudaErrorInvalidConfiguration;
     WaveArgs a{};
     a.jobs = d_jobs;
     a.table = d_table;

@@ -63,3 +63,27 @@ def test_batch_matches_plain_calls(rows, graph, budget):
         if budget:
             assert info["groups"] > 4, info  # the 24 MiB budget splits the larger classes
         assert info["launches"] > 0
+
+
+@pytest.mark.parametrize("rows", [4, 8])
+def test_batch_many_wide_pairs(rows):
+    """24 pairs of one class, 2048 px wide and tall enough (160 rows) that a
+    band can only finish while the bands several ring lengths below it run:
+    the tickets exceed the resident CTAs, so the batch is cut into chunks
+    whose hand-off window fits them.  Exact against the plain call."""
+    torch = pytest.importorskip("torch")
+    pairs = []
+    for i in range(24):
+        left, right, _ = synth.make_pair(synth.PairSpec(2048, 160, 4, 1, 40, 2.0, 500 + i))
+        p = StereoParams(maxDisparity=64, numDirections=4, speckleWindowSize=0, P2=400 + 100 * (i % 5))
+        pairs.append((p, torch.from_numpy(left).cuda(), torch.from_numpy(right).cuda(), 2048, 160))
+    refs = _plain(torch, pairs)
+    outs = [torch.full((h, w), 0x7ABC, dtype=torch.int16, device="cuda") for _, _, _, w, h in pairs]
+    with StereoBatch(rows_per_band=rows, use_graph=True) as b:
+        for (p, dl, dr, w, h), o in zip(pairs, outs):
+            b.add(p, dl.data_ptr(), dr.data_ptr(), w, h, o.data_ptr())
+        b.run()
+        b.sync()
+        for i, (o, ref) in enumerate(zip(outs, refs)):
+            assert np.array_equal(o.cpu().numpy(), ref), i
+        assert b.info()["groups"] == 1
