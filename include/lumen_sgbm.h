@@ -224,6 +224,62 @@ lumen_status lumen_sgbm_batch_sync(lumen_sgbm_batch* b, void* stream);
 lumen_status lumen_sgbm_batch_info(const lumen_sgbm_batch* b, size_t* device_bytes, int* groups,
                                    unsigned long long* launches);
 
+/* ---- served form (no counterpart in the reference's API) ----
+ *
+ * A server owns a device arena of device_budget_bytes (allocated once), the
+ * resident rectification maps of registered calibration ids, and a thread
+ * that batches queued requests continuously: whenever one of max_inflight
+ * batch slots is free it admits waiting requests in arrival order while their
+ * buffers fit in the arena (at most max_batch_pairs per batch) and launches
+ * them through the batched kernels; a batch admitted while another runs
+ * overlaps with it on the device.  Each result is bit-exact with
+ * lumen_sgbm_compute on the same (rectified) pair. */
+typedef struct lumen_server lumen_server;
+typedef struct lumen_server_options {
+    size_t device_budget_bytes; /* arena size; default 40 GiB */
+    int max_batch_pairs;        /* default 32 */
+    int rows_per_band;          /* 4, 8 (default) or 16 */
+    int max_inflight;           /* batch slots on the device at once, 1..8; default 2 */
+    int watchdog_ms;            /* host deadline of a batch, 0 = none; default 60000 */
+    long long spin_limit;       /* device-side wait limit, 0 = default (2^24) */
+} lumen_server_options;
+typedef struct lumen_request_info {
+    lumen_status status;
+    double latency_ms;  /* submit -> result in the caller's buffer */
+    double queue_ms;    /* submit -> admission */
+    double device_ms;   /* the batch's device time */
+    int batch_pairs;    /* requests in the batch */
+    unsigned long long batch_id;
+} lumen_request_info;
+typedef struct lumen_server_stats {
+    unsigned long long submitted, completed, rejected, failed, batches, watchdog_expired;
+    size_t budget_bytes, admitted_bytes, peak_admitted_bytes;
+    int queue_depth, peak_queue_depth, inflight_batches, peak_batch_pairs;
+} lumen_server_stats;
+void lumen_server_options_default(lumen_server_options* o);
+lumen_status lumen_server_create(const lumen_server_options* o, lumen_server** out);
+/* Finishes every queued request, then frees the server. */
+lumen_status lumen_server_destroy(lumen_server* s);
+/* Uploads the four CV_32FC1 maps of a calibration once (NULL maps: the pairs
+ * are pre-rectified); an id is bound once. */
+lumen_status lumen_server_set_calibration(lumen_server* s, int calib_id, int width, int height,
+                                          const float* map0x, const float* map0y,
+                                          const float* map1x, const float* map1y);
+/* Queues one gray pair (host buffers, width*height bytes each, copied before
+ * the call returns); calib_id -1 = already rectified.  `out` (width*height
+ * int16) is written before lumen_server_wait reports the request done and
+ * must stay valid until then.  Invalid parameters and requests larger than
+ * the budget are rejected here, the server keeps serving. */
+lumen_status lumen_server_submit(lumen_server* s, const lumen_stereo_params* params, int calib_id,
+                                 const uint8_t* left, const uint8_t* right, int width, int height,
+                                 int16_t* out, unsigned long long* request_id);
+/* Waits for a request (timeout_ms < 0: no limit) and releases its id; returns
+ * the request's status (LUMEN_ERR_TIMEOUT also when the wait itself ran out,
+ * with the id kept). */
+lumen_status lumen_server_wait(lumen_server* s, unsigned long long request_id, int timeout_ms,
+                               lumen_request_info* info);
+lumen_status lumen_server_get_stats(lumen_server* s, lumen_server_stats* out);
+
 /* ---- Census cost volume without device allocation.  No counterpart in the
  * reference: it serves callers that cannot call cudaMalloc (a real-time loop
  * that must not take cudaMalloc's implicit device synchronisation, a plugin host

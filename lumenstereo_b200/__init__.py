@@ -23,7 +23,7 @@ import numpy as np
 
 from . import _lib
 
-__all__ = ["MatchingCostMode", "StereoParams", "StereoSGBM", "StereoBatch", "StereoRectifier",
+__all__ = ["MatchingCostMode", "StereoParams", "StereoSGBM", "StereoBatch", "StereoServer", "StereoRectifier",
            "StereoException", "CudaException", "kSgbmMaxDisparityRange",
            "middleburyMatcherMaxDisparity", "rectify_image_gpu", "bgr_to_gray"]
 
@@ -348,6 +348,92 @@ class StereoBatch:
     def close(self) -> None:
         if self._h:
             _lib.lib().lumen_sgbm_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+class StereoServer:
+    """Served form: a request loop with continuous batching over a device
+    arena of ``budget_bytes`` (lumen_server_* in include/lumen_sgbm.h).
+
+        with StereoServer(budget_bytes=8 << 30) as srv:
+            srv.set_calibration(3, w, h, m0x, m0y, m1x, m1y)   # resident maps
+            rid = srv.submit(params, left, right, calib_id=3)   # returns at once
+            disparity, info = srv.wait(rid)                     # info: latency_ms, ...
+    """
+
+    def __init__(self, budget_bytes: int = 40 << 30, max_batch_pairs: int = 32, rows_per_band: int = 8,
+                 max_inflight: int = 2, watchdog_ms: int = 60000, spin_limit: int = 0):
+        o = _lib.CServerOptions()
+        _lib.lib().lumen_server_options_default(C.byref(o))
+        o.device_budget_bytes = budget_bytes
+        o.max_batch_pairs = max_batch_pairs
+        o.rows_per_band = rows_per_band
+        o.max_inflight = max_inflight
+        o.watchdog_ms = watchdog_ms
+        o.spin_limit = spin_limit
+        self._h = C.c_void_p()
+        self._outs = {}
+        _check(_lib.lib().lumen_server_create(C.byref(o), C.byref(self._h)))
+
+    def set_calibration(self, calib_id: int, width: int, height: int, map0x=None, map0y=None,
+                        map1x=None, map1y=None) -> None:
+        maps = [None if m is None else np.ascontiguousarray(m, dtype=np.float32)
+                for m in (map0x, map0y, map1x, map1y)]
+        for m in maps:
+            if m is not None and m.shape != (height, width):
+                raise StereoException("maps must be height x width float32")
+        ptrs = [None if m is None else m.ctypes.data for m in maps]
+        _check(_lib.lib().lumen_server_set_calibration(self._h, calib_id, width, height, *ptrs))
+
+    def submit(self, params: StereoParams, left: np.ndarray, right: np.ndarray, calib_id: int = -1,
+               out: np.ndarray | None = None) -> int:
+        """Queues a gray uint8 pair (copied before returning); returns its id."""
+        left = np.ascontiguousarray(left, dtype=np.uint8)
+        right = np.ascontiguousarray(right, dtype=np.uint8)
+        if left.ndim != 2 or left.shape != right.shape:
+            raise StereoException("Left and right images must have the same size")
+        h, w = left.shape
+        if out is None:
+            out = np.empty((h, w), np.int16)
+        c = params.to_c()
+        rid = C.c_ulonglong(0)
+        _check(_lib.lib().lumen_server_submit(self._h, C.byref(c), calib_id, left.ctypes.data,
+                                              right.ctypes.data, w, h, out.ctypes.data, C.byref(rid)))
+        self._outs[rid.value] = out
+        return rid.value
+
+    def wait(self, request_id: int, timeout_ms: int = -1):
+        """(disparity, info) of a request; raises the request's error."""
+        info = _lib.CRequestInfo()
+        info.status = -1  # stays -1 when the wait itself runs out (the id is kept)
+        st = _lib.lib().lumen_server_wait(self._h, request_id, timeout_ms, C.byref(info))
+        if st != _lib.OK and info.status != -1:
+            self._outs.pop(request_id, None)
+        _check(st)
+        out = self._outs.pop(request_id)
+        return out, {"latency_ms": info.latency_ms, "queue_ms": info.queue_ms, "device_ms": info.device_ms,
+                     "batch_pairs": info.batch_pairs, "batch_id": info.batch_id}
+
+    def stats(self) -> dict:
+        s = _lib.CServerStats()
+        _check(_lib.lib().lumen_server_get_stats(self._h, C.byref(s)))
+        return {n: getattr(s, n) for n, _ in _lib.CServerStats._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            _lib.lib().lumen_server_destroy(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):

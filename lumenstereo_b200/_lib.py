@@ -34,6 +34,25 @@ class CParams(C.Structure):
     _fields_ = [(n, C.c_int32) for n in PARAM_FIELDS]
 
 
+class CServerOptions(C.Structure):
+    _fields_ = [("device_budget_bytes", C.c_size_t), ("max_batch_pairs", C.c_int),
+                ("rows_per_band", C.c_int), ("max_inflight", C.c_int), ("watchdog_ms", C.c_int),
+                ("spin_limit", C.c_longlong)]
+
+
+class CRequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("latency_ms", C.c_double), ("queue_ms", C.c_double),
+                ("device_ms", C.c_double), ("batch_pairs", C.c_int), ("batch_id", C.c_ulonglong)]
+
+
+class CServerStats(C.Structure):
+    _fields_ = [(n, C.c_ulonglong) for n in ("submitted", "completed", "rejected", "failed", "batches",
+                                              "watchdog_expired")] + \
+               [(n, C.c_size_t) for n in ("budget_bytes", "admitted_bytes", "peak_admitted_bytes")] + \
+               [(n, C.c_int) for n in ("queue_depth", "peak_queue_depth", "inflight_batches",
+                                       "peak_batch_pairs")]
+
+
 def _declare(lib):
     vp, i, sz = C.c_void_p, C.c_int, C.c_size_t
     sig = {
@@ -77,6 +96,13 @@ def _declare(lib):
         "lumen_sgbm_batch_run": (i, [vp, vp]),
         "lumen_sgbm_batch_sync": (i, [vp, vp]),
         "lumen_sgbm_batch_info": (i, [vp, C.POINTER(sz), C.POINTER(C.c_int), C.POINTER(C.c_ulonglong)]),
+        "lumen_server_options_default": (None, [C.POINTER(CServerOptions)]),
+        "lumen_server_create": (i, [C.POINTER(CServerOptions), C.POINTER(vp)]),
+        "lumen_server_destroy": (i, [vp]),
+        "lumen_server_set_calibration": (i, [vp, i, i, i, vp, vp, vp, vp]),
+        "lumen_server_submit": (i, [vp, C.POINTER(CParams), i, vp, vp, i, i, vp, C.POINTER(C.c_ulonglong)]),
+        "lumen_server_wait": (i, [vp, C.c_ulonglong, i, C.POINTER(CRequestInfo)]),
+        "lumen_server_get_stats": (i, [vp, C.POINTER(CServerStats)]),
         "lumen_census_cost_noalloc": (i, [vp, vp, i, i, i, i, vp, i, vp]),
         "lumen_census_cost_noalloc_max_pixels": (sz, []),
     }

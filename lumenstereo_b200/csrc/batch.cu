@@ -5,70 +5,37 @@
 // batch groups its pairs by kernel class (padded disparity count, path set,
 // arithmetic mode, full padding) and runs each group's aggregation as ONE
 // persistent launch of the lockstep row-band sweeps over the bands of all its
-// pairs (wave_kernel.cuh, tickets in band-major order), so the wavefronts of
-// different pairs fill the GPU together.  Cost volumes and the selection run
-// per pair around it.  Buffers come from one pooled device allocation reused
-// group after group, sized by a device-memory budget; with graphs enabled the
-// whole run is captured once into a CUDA graph and replayed.  Every pair's
-// output equals lumen_sgbm_compute_device's for the same pair bit for bit.
+// pairs (wave_kernel.cuh, tickets in band-major order within chunks), so the
+// wavefronts of different pairs fill the GPU together.  Cost volumes and the
+// selection run per pair around it.  Buffers come from one pooled device
+// allocation reused group after group, sized by a device-memory budget; with
+// graphs enabled the whole run is captured once into a CUDA graph and
+// replayed.  Every pair's output equals lumen_sgbm_compute_device's for the
+// same pair bit for bit.
+//
+// The launch core (batch_pair_*, batch_group_by_class, batch_describe,
+// batch_enqueue_groups) is shared with the served form (server.cu).
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <map>
-#include <sstream>
 #include <string>
 #include <tuple>
 #include <vector>
 
 #include "../../include/lumen_sgbm.h"
+#include "batch_core.cuh"
 #include "common.cuh"
 #include "kernels.cuh"
 #include "wave_kernel.cuh"
 
-using namespace lumen;
+namespace lumen {
 
 namespace {
 
-struct BatchPair {
-    lumen_stereo_params p;
-    const uint8_t* left;
-    const uint8_t* right;
-    int W, H;
-    int16_t* out;
-    // derived
-    int D, Dp, r, cap;
-    bool census, diag, wrap, full;
-    SgmConsts k;
-    int nBands;
-    // pool offsets (bytes)
-    size_t oCost, oAgg, oPartB, oDispL, oDispR, oAux0, oAux1, oRing, oCtr;
-};
-
-struct BatchGroup {
-    int Dp;
-    bool diag, wrap, full;
-    std::vector<int> pairs;
-    int Wmax = 0;
-    WavePlan plan{};
-    int nTickets = 0;
-    int window = 0;  // ticket distance the oldest unfinished ticket may need running
-    size_t ctrOff = 0, ctrWords = 0;  // pool offset / size of the group's counters (prod, cons, ticket)
-    size_t jobsOff = 0, tableOff = 0;  // offsets in the descriptor buffer
-};
-
 lumen_status bfail(lumen_status s, const std::string& m) { return set_error(s, m); }
-
-#define BCU(call)                                                                              \
-    do {                                                                                       \
-        cudaError_t e_ = (call);                                                               \
-        if (e_ != cudaSuccess)                                                                 \
-            return bfail(LUMEN_ERR_CUDA, std::string("CUDA error in ") + #call + ": " +       \
-                                             cudaGetErrorString(e_));                          \
-    } while (0)
-
-size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 // Same rule as the plain call: every uint16 quantity provably stays in range.
 bool batch_no_wrap(const lumen_stereo_params& p, int cs, int nPaths) {
@@ -80,7 +47,243 @@ bool batch_no_wrap(const lumen_stereo_params& p, int cs, int nPaths) {
     return cmax <= 65535 && lmax + p.P1 <= 65535 && lmax + p2max <= 65535 && lmax * nPaths <= 65535;
 }
 
+size_t ctr_bytes(int nBands) { return (4 * (size_t)nBands + 32) * 4; }
+
 }  // namespace
+
+#define BCU(call)                                                                              \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return bfail(LUMEN_ERR_CUDA, std::string("CUDA error in ") + #call + ": " +       \
+                                             cudaGetErrorString(e_));                          \
+    } while (0)
+
+lumen_status batch_pair_init(BatchPair& q, const lumen_stereo_params* p, const uint8_t* d_left,
+                             const uint8_t* d_right, int width, int height, int16_t* d_out) {
+    if (!p) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "NULL parameters");
+    if (!d_left || !d_right || width <= 0 || height <= 0)
+        return bfail(LUMEN_ERR_INVALID_ARGUMENT, "Input images are empty");
+    if (!d_out) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "output buffer is NULL");
+    const int D = p->maxDisparity - p->minDisparity;
+    if (D < 1)
+        return bfail(LUMEN_ERR_INVALID_ARGUMENT,
+                     "Invalid disparity range: maxDisparity must be greater than minDisparity");
+    if (D > LUMEN_MAX_DISPARITY_RANGE)
+        return bfail(LUMEN_ERR_RANGE_EXCEEDS_LIMIT,
+                     "Disparity range (maxDisparity - minDisparity) exceeds GPU limit (512). Reduce the search range.");
+    if (p->minDisparity < 0) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "minDisparity must be >= 0");
+    if (p->blockSize < 0 || p->blockSize > 21) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "blockSize must be in [0, 21]");
+    if (width < 2) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "image width must be at least 2");
+    if ((long long)p->maxDisparity * 16 > 32767)
+        return bfail(LUMEN_ERR_INVALID_ARGUMENT, "maxDisparity*16 must fit int16 disparities");
+    q = BatchPair{};
+    q.p = *p;
+    q.left = d_left;
+    q.right = d_right;
+    q.W = width;
+    q.H = height;
+    q.out = d_out;
+    q.D = D;
+    q.Dp = padded_d(D);
+    q.census = p->matchingCostMode == 1;
+    q.diag = p->numDirections >= 8;
+    q.r = p->blockSize / 2;
+    q.cap = std::max(1, p->preFilterCap);
+    const int cs = q.census ? std::max(1, (p->blockSize * p->blockSize * 2 * p->preFilterCap) / 255)
+                            : p->blockSize * p->blockSize;
+    q.wrap = !batch_no_wrap(*p, cs, q.diag ? 8 : 4);
+    q.full = q.D == q.Dp;
+    q.k.W = width; q.k.H = height; q.k.D = D; q.k.Dp = q.Dp;
+    q.k.P1 = p->P1; q.k.P2 = p->P2; q.k.costScale = cs;
+    q.k.p1x2 = ((uint32_t)p->P1 & 0xFFFFu) * 0x10001u;
+    q.k.bsub = ((uint32_t)(0xFFFF - p->P1) & 0xFFFFu) * 0x10001u;
+    return LUMEN_OK;
+}
+
+size_t batch_pair_layout(BatchPair& q, int R, size_t start) {
+    const size_t N = (size_t)q.W * q.H, ND = N * q.Dp;
+    q.nBands = (q.H + R - 1) / R;
+    size_t o = start;
+    auto take = [&](size_t n) { const size_t r0 = o; o += align256(n); return r0; };
+    q.oCost = take(ND);
+    q.oAgg = take(ND * 2);
+    q.oPartB = take(ND * 2);
+    q.oDispL = take(N * 2);
+    q.oDispR = take(N * 2);
+    q.oAux0 = take(q.census ? N * 4 : N);
+    q.oAux1 = take(q.census ? N * 4 : N);
+    q.oRing = take(wave_ring_bytes(q.nBands, q.Dp, q.diag));
+    q.oCtr = take(ctr_bytes(q.nBands));
+    return o;
+}
+
+size_t batch_pair_bytes(const BatchPair& q, int R) {
+    BatchPair t = q;
+    return batch_pair_layout(t, R, 0);
+}
+
+bool batch_same_class(const BatchPair& a, const BatchPair& b) {
+    return a.Dp == b.Dp && a.diag == b.diag && a.wrap == b.wrap && a.full == b.full;
+}
+
+void batch_group_by_class(const std::vector<BatchPair>& pairs, const std::vector<int>& idx,
+                          std::vector<BatchGroup>& groups) {
+    std::map<std::tuple<int, bool, bool, bool>, std::vector<int>> cls;
+    for (int i : idx) {
+        const BatchPair& q = pairs[i];
+        cls[std::make_tuple(q.Dp, q.diag, q.wrap, q.full)].push_back(i);
+    }
+    for (auto& kv : cls) {
+        BatchGroup g;
+        g.Dp = std::get<0>(kv.first);
+        g.diag = std::get<1>(kv.first);
+        g.wrap = std::get<2>(kv.first);
+        g.full = std::get<3>(kv.first);
+        g.pairs = kv.second;
+        // longest wavefront span first: the last chunk of the launch, whose
+        // latency is the launch's tail, holds the shortest pairs
+        std::stable_sort(g.pairs.begin(), g.pairs.end(), [&](int a, int b) {
+            return pairs[a].W + 2 * pairs[a].H > pairs[b].W + 2 * pairs[b].H;
+        });
+        for (int i : g.pairs) g.Wmax = std::max(g.Wmax, pairs[i].W);
+        groups.push_back(g);
+    }
+}
+
+lumen_status batch_describe(const std::vector<BatchPair>& pairs, std::vector<BatchGroup>& groups,
+                            int R, int numSMs, std::vector<uint8_t>& host) {
+    size_t dOff = 0;
+    for (BatchGroup& g : groups) {
+        cudaError_t e = wave_batch_plan(g.Wmax, g.Dp, R, g.wrap, g.full, g.diag, numSMs, &g.plan);
+        if (e != cudaSuccess)
+            return bfail(LUMEN_ERR_INVALID_ARGUMENT,
+                         std::string("batch: no sweep configuration for a group: ") + cudaGetErrorString(e));
+        g.nTickets = 0;
+        for (int i : g.pairs) g.nTickets += 2 * pairs[i].nBands;
+        g.jobsOff = dOff;
+        dOff = align256(dOff + sizeof(WaveJob) * g.pairs.size());
+        g.tableOff = dOff;
+        dOff = align256(dOff + sizeof(uint32_t) * (size_t)g.nTickets + 4);  // + the ticket counter
+    }
+    host.assign(dOff, 0);
+    for (BatchGroup& g : groups) {
+        WaveJob* jobs = reinterpret_cast<WaveJob*>(host.data() + g.jobsOff);
+        uint32_t* table = reinterpret_cast<uint32_t*>(host.data() + g.tableOff);
+        for (int j = 0; j < (int)g.pairs.size(); ++j) {
+            const BatchPair& q = pairs[g.pairs[j]];
+            PairView pv{reinterpret_cast<const uint8_t*>(q.base + q.oCost), q.left,
+                        reinterpret_cast<uint16_t*>(q.base + q.oAgg)};
+            jobs[j] = wave_job(pv, reinterpret_cast<uint16_t*>(q.base + q.oPartB), q.k, R, q.base + q.oRing,
+                               reinterpret_cast<unsigned*>(q.base + q.oCtr));
+        }
+        // Chunks of pairs, tickets band-major within a chunk (the chunk's
+        // wavefronts overlap), chunk after chunk.  A band may need the next
+        // wave_lookahead_bands(W) bands of its pair and sweep running, which
+        // band-major order puts up to 2 * n * lookahead tickets later in a
+        // chunk of n pairs: chunks stay small enough for that window to fit
+        // in the resident CTAs.
+        int t = 0;
+        g.window = 0;
+        for (int j0 = 0; j0 < (int)g.pairs.size();) {
+            int j1 = j0, Wc = 0, nb = 0;
+            while (j1 < (int)g.pairs.size()) {
+                const BatchPair& q = pairs[g.pairs[j1]];
+                const int w2 = std::max(Wc, q.W);
+                if (j1 > j0 && 2 * (j1 - j0 + 1) * wave_lookahead_bands(w2) + 1 > g.plan.grid) break;
+                Wc = w2;
+                nb = std::max(nb, q.nBands);
+                ++j1;
+            }
+            int chunkTickets = 0;
+            for (int j = j0; j < j1; ++j) chunkTickets += 2 * pairs[g.pairs[j]].nBands;
+            // needs stay inside the chunk
+            const int win = std::min(2 * (j1 - j0) * wave_lookahead_bands(Wc), chunkTickets);
+            if (win + 1 > g.plan.grid)
+                return bfail(LUMEN_ERR_INVALID_ARGUMENT, "batch: a pair is too wide for the resident sweep CTAs");
+            g.window = std::max(g.window, win);
+            for (int band = 0; band < nb; ++band)
+                for (int j = j0; j < j1; ++j)
+                    if (band < pairs[g.pairs[j]].nBands)
+                        for (int sw = 0; sw < 2; ++sw)
+                            table[t++] = ((uint32_t)j << 20) | ((uint32_t)sw << 19) | (uint32_t)band;
+            j0 = j1;
+        }
+    }
+    return LUMEN_OK;
+}
+
+lumen_status batch_enqueue_groups(const std::vector<BatchPair>& pairs,
+                                  const std::vector<BatchGroup>& groups, const uint8_t* desc,
+                                  const uint32_t* magic, int* status, long long spinMax,
+                                  cudaStream_t s, cudaStream_t agg, cudaEvent_t* evs,
+                                  unsigned long long* launches) {
+    unsigned long long nl = 0;
+    int gi = 0;
+    for (const BatchGroup& g : groups) {
+        // counters of the group's pairs and the group's ticket
+        for (int i : g.pairs) {
+            const BatchPair& q = pairs[i];
+            BCU(cudaMemsetAsync(q.base + q.oCtr, 0, ctr_bytes(q.nBands), s));
+        }
+        unsigned* ticket = reinterpret_cast<unsigned*>(const_cast<uint8_t*>(desc) + g.tableOff +
+                                                       sizeof(uint32_t) * (size_t)g.nTickets);
+        BCU(cudaMemsetAsync(ticket, 0, 4, s));
+        // cost volumes
+        for (int i : g.pairs) {
+            const BatchPair& q = pairs[i];
+            uint8_t* cost = q.base + q.oCost;
+            if (q.census) {
+                uint32_t* c0 = reinterpret_cast<uint32_t*>(q.base + q.oAux0);
+                uint32_t* c1 = reinterpret_cast<uint32_t*>(q.base + q.oAux1);
+                launch_census(q.left, q.right, q.W, q.H, c0, c1, s);
+                BCU(launch_census_cost(c0, c1, q.W, q.H, q.D, q.Dp, q.p.minDisparity, cost, s));
+            } else {
+                uint8_t* p0 = q.base + q.oAux0;
+                uint8_t* p1 = q.base + q.oAux1;
+                launch_prefilter(q.left, q.right, q.W, q.H, q.cap, p0, p1, s);
+                const int wide = (long long)(2 * q.r + 1) * (2 * q.r + 1) * 2 * q.cap > 65535;
+                BCU(launch_sad_cost(p0, p1, q.W, q.H, q.D, q.Dp, q.p.minDisparity, q.r, magic, wide, cost, s));
+            }
+            nl += 2;
+        }
+        // one aggregation launch over all bands of the group
+        cudaStream_t as = s;
+        if (agg) {
+            BCU(cudaEventRecord(evs[2 * gi], s));
+            BCU(cudaStreamWaitEvent(agg, evs[2 * gi], 0));
+            as = agg;
+        }
+        BCU(launch_aggregate_wave_batch(reinterpret_cast<const WaveJob*>(desc + g.jobsOff),
+                                        reinterpret_cast<const uint32_t*>(desc + g.tableOff), g.nTickets,
+                                        g.window, g.Wmax, g.Dp, g.wrap, g.full, g.diag, g.plan, ticket,
+                                        status, spinMax, as));
+        if (agg) {
+            BCU(cudaEventRecord(evs[2 * gi + 1], agg));
+            BCU(cudaStreamWaitEvent(s, evs[2 * gi + 1], 0));
+        }
+        nl += 1;
+        // selection and post-processing
+        for (int i : g.pairs) {
+            const BatchPair& q = pairs[i];
+            int16_t* dl = reinterpret_cast<int16_t*>(q.base + q.oDispL);
+            int16_t* dr = reinterpret_cast<int16_t*>(q.base + q.oDispR);
+            BCU(launch_select(reinterpret_cast<uint16_t*>(q.base + q.oAgg), reinterpret_cast<uint16_t*>(q.base + q.oPartB),
+                              q.wrap, q.W, q.H, q.D, q.Dp, q.p.minDisparity, q.p.uniquenessRatio, dl, dr, s));
+            const int lr = q.p.disp12MaxDiff >= 0 ? q.p.disp12MaxDiff * 16 : -1;
+            const int spk = q.p.speckleWindowSize > 0 ? std::min(q.p.speckleWindowSize, 25) : 0;
+            BCU(launch_post(dl, dr, q.W, q.H, lr, spk, q.p.speckleRange * 16, q.out, (size_t)q.W, nullptr, s));
+            nl += 2;
+        }
+        ++gi;
+    }
+    if (launches) *launches = nl;
+    return LUMEN_OK;
+}
+
+}  // namespace lumen
+
+using namespace lumen;
 
 struct lumen_sgbm_batch {
     std::vector<BatchPair> pairs;
@@ -115,27 +318,22 @@ static void batch_release(lumen_sgbm_batch* b) {
     b->planned = false;
 }
 
-// Buffers, groups, job descriptors and ticket tables for the current pairs.
+// Buffers, groups, job descriptors and ticket tables for the current pairs:
+// each class is cut into groups by the budget, and every group's buffers are
+// laid out from the start of one pool that the groups reuse in turn.
 static lumen_status batch_plan(lumen_sgbm_batch* b) {
     batch_release(b);
     const int R = b->rows ? b->rows : 8;
-    // classes
-    std::map<std::tuple<int, bool, bool, bool>, std::vector<int>> cls;
-    for (int i = 0; i < (int)b->pairs.size(); ++i) {
-        const BatchPair& q = b->pairs[i];
-        cls[std::make_tuple(q.Dp, q.diag, q.wrap, q.full)].push_back(i);
-    }
-    // groups: one class each, cut by the budget
+    std::vector<int> all(b->pairs.size());
+    for (int i = 0; i < (int)all.size(); ++i) all[i] = i;
+    std::vector<BatchGroup> classes;
+    batch_group_by_class(b->pairs, all, classes);
     b->groups.clear();
     size_t poolNeed = 0;
-    for (auto& kv : cls) {
-        const int Dp = std::get<0>(kv.first);
-        const bool diag = std::get<1>(kv.first), wrap = std::get<2>(kv.first), full = std::get<3>(kv.first);
-        BatchGroup g;
-        g.Dp = Dp;
-        g.diag = diag;
-        g.wrap = wrap;
-        g.full = full;
+    for (const BatchGroup& c : classes) {
+        BatchGroup g = c;
+        g.pairs.clear();
+        g.Wmax = 0;
         size_t bytes = 0;
         auto flush = [&]() {
             if (!g.pairs.empty()) {
@@ -146,159 +344,37 @@ static lumen_status batch_plan(lumen_sgbm_batch* b) {
             g.Wmax = 0;
             bytes = 0;
         };
-        for (int i : kv.second) {
+        for (int i : c.pairs) {
             BatchPair& q = b->pairs[i];
-            const size_t N = (size_t)q.W * q.H, ND = N * Dp;
-            q.nBands = (q.H + R - 1) / R;
-            const size_t need = align256(ND) + 2 * align256(ND * 2) + 2 * align256(N * 2) +
-                                2 * align256(q.census ? N * 4 : N) +
-                                align256(wave_ring_bytes(q.nBands, Dp, diag)) +
-                                align256((4 * (size_t)q.nBands + 32) * 4);
-            WavePlan pl{};
-            cudaError_t e = wave_batch_plan(std::max(g.Wmax, q.W), Dp, R, wrap, full, diag, b->numSMs, &pl);
-            if (e != cudaSuccess)
-                return bfail(LUMEN_ERR_INVALID_ARGUMENT,
-                             std::string("batch: no sweep configuration for a pair: ") + cudaGetErrorString(e));
+            const size_t need = batch_pair_bytes(q, R);
             if (!g.pairs.empty() && bytes + need > b->budget) flush();
             if (need > b->budget)
                 return bfail(LUMEN_ERR_OUT_OF_BUDGET, "batch: one pair needs more device memory than the budget");
-            // offsets within the group's slice of the pool
-            size_t o = bytes;
-            auto take = [&](size_t n) { const size_t r0 = o; o += align256(n); return r0; };
-            q.oCost = take(ND);
-            q.oAgg = take(ND * 2);
-            q.oPartB = take(ND * 2);
-            q.oDispL = take(N * 2);
-            q.oDispR = take(N * 2);
-            q.oAux0 = take(q.census ? N * 4 : N);
-            q.oAux1 = take(q.census ? N * 4 : N);
-            q.oRing = take(wave_ring_bytes(q.nBands, Dp, diag));
-            q.oCtr = take((4 * (size_t)q.nBands + 32) * 4);
-            bytes = o;
+            bytes = batch_pair_layout(q, R, bytes);
             g.pairs.push_back(i);
             g.Wmax = std::max(g.Wmax, q.W);
         }
         flush();
     }
-    // plans and descriptor layout
-    size_t dOff = 0;
-    for (BatchGroup& g : b->groups) {
-        cudaError_t e = wave_batch_plan(g.Wmax, g.Dp, R, g.wrap, g.full, g.diag, b->numSMs, &g.plan);
-        if (e != cudaSuccess) return bfail(LUMEN_ERR_CUDA, std::string("batch plan: ") + cudaGetErrorString(e));
-        g.nTickets = 0;
-        for (int i : g.pairs) g.nTickets += 2 * b->pairs[i].nBands;
-        g.jobsOff = dOff;
-        dOff = align256(dOff + sizeof(WaveJob) * g.pairs.size());
-        g.tableOff = dOff;
-        dOff = align256(dOff + sizeof(uint32_t) * (size_t)g.nTickets + 4);  // + the ticket counter
-    }
     BCU(cudaMalloc(&b->pool, std::max<size_t>(poolNeed, 256)));
     b->poolBytes = poolNeed;
-    BCU(cudaMalloc(&b->desc, std::max<size_t>(dOff, 256)));
-    b->descBytes = dOff;
-    // job descriptors and band-major ticket tables
-    uint8_t* base = static_cast<uint8_t*>(b->pool);
-    std::vector<uint8_t> host(dOff, 0);
-    for (BatchGroup& g : b->groups) {
-        WaveJob* jobs = reinterpret_cast<WaveJob*>(host.data() + g.jobsOff);
-        uint32_t* table = reinterpret_cast<uint32_t*>(host.data() + g.tableOff);
-        for (int j = 0; j < (int)g.pairs.size(); ++j) {
-            const BatchPair& q = b->pairs[g.pairs[j]];
-            PairView pv{reinterpret_cast<const uint8_t*>(base + q.oCost), q.left,
-                        reinterpret_cast<uint16_t*>(base + q.oAgg)};
-            jobs[j] = wave_job(pv, reinterpret_cast<uint16_t*>(base + q.oPartB), q.k, R, base + q.oRing,
-                               reinterpret_cast<unsigned*>(base + q.oCtr));
-        }
-        // Chunks of pairs, tickets band-major within a chunk (the chunk's
-        // wavefronts overlap), chunk after chunk.  A band may need the next
-        // wave_lookahead_bands(W) bands of its pair and sweep running, which
-        // band-major order puts up to 2 * n * lookahead tickets later in a
-        // chunk of n pairs: chunks stay small enough for that window to fit
-        // in the resident CTAs.
-        int t = 0;
-        g.window = 0;
-        for (int j0 = 0; j0 < (int)g.pairs.size();) {
-            int j1 = j0, Wc = 0, nb = 0;
-            while (j1 < (int)g.pairs.size()) {
-                const BatchPair& q = b->pairs[g.pairs[j1]];
-                const int w2 = std::max(Wc, q.W);
-                if (j1 > j0 && 2 * (j1 - j0 + 1) * wave_lookahead_bands(w2) + 1 > g.plan.grid) break;
-                Wc = w2;
-                nb = std::max(nb, q.nBands);
-                ++j1;
-            }
-            int chunkTickets = 0;
-            for (int j = j0; j < j1; ++j) chunkTickets += 2 * b->pairs[g.pairs[j]].nBands;
-            // needs stay inside the chunk
-            const int win = std::min(2 * (j1 - j0) * wave_lookahead_bands(Wc), chunkTickets);
-            if (win + 1 > g.plan.grid)
-                return bfail(LUMEN_ERR_INVALID_ARGUMENT, "batch: a pair is too wide for the resident sweep CTAs");
-            g.window = std::max(g.window, win);
-            for (int band = 0; band < nb; ++band)
-                for (int j = j0; j < j1; ++j)
-                    if (band < b->pairs[g.pairs[j]].nBands)
-                        for (int sw = 0; sw < 2; ++sw)
-                            table[t++] = ((uint32_t)j << 20) | ((uint32_t)sw << 19) | (uint32_t)band;
-            j0 = j1;
-        }
-    }
-    BCU(cudaMemcpy(b->desc, host.data(), dOff, cudaMemcpyHostToDevice));
+    for (BatchPair& q : b->pairs) q.base = static_cast<uint8_t*>(b->pool);
+    std::vector<uint8_t> host;
+    lumen_status st = batch_describe(b->pairs, b->groups, R, b->numSMs, host);
+    if (st != LUMEN_OK) return st;
+    BCU(cudaMalloc(&b->desc, std::max<size_t>(host.size(), 256)));
+    b->descBytes = host.size();
+    BCU(cudaMemcpy(b->desc, host.data(), host.size(), cudaMemcpyHostToDevice));
     b->planned = true;
     return LUMEN_OK;
 }
 
-// Every launch of one run, enqueued on `s`.
 static lumen_status batch_enqueue(lumen_sgbm_batch* b, cudaStream_t s) {
-    uint8_t* base = static_cast<uint8_t*>(b->pool);
-    uint8_t* desc = static_cast<uint8_t*>(b->desc);
     unsigned long long nl = 0;
-    for (const BatchGroup& g : b->groups) {
-        // counters of the group's pairs and the group's ticket
-        for (int i : g.pairs) {
-            const BatchPair& q = b->pairs[i];
-            BCU(cudaMemsetAsync(base + q.oCtr, 0, (4 * (size_t)q.nBands + 32) * 4, s));
-        }
-        unsigned* ticket = reinterpret_cast<unsigned*>(desc + g.tableOff + sizeof(uint32_t) * (size_t)g.nTickets);
-        BCU(cudaMemsetAsync(ticket, 0, 4, s));
-        // cost volumes
-        for (int i : g.pairs) {
-            const BatchPair& q = b->pairs[i];
-            uint8_t* cost = base + q.oCost;
-            if (q.census) {
-                uint32_t* c0 = reinterpret_cast<uint32_t*>(base + q.oAux0);
-                uint32_t* c1 = reinterpret_cast<uint32_t*>(base + q.oAux1);
-                launch_census(q.left, q.right, q.W, q.H, c0, c1, s);
-                BCU(launch_census_cost(c0, c1, q.W, q.H, q.D, q.Dp, q.p.minDisparity, cost, s));
-            } else {
-                uint8_t* p0 = base + q.oAux0;
-                uint8_t* p1 = base + q.oAux1;
-                launch_prefilter(q.left, q.right, q.W, q.H, q.cap, p0, p1, s);
-                const int wide = (long long)(2 * q.r + 1) * (2 * q.r + 1) * 2 * q.cap > 65535;
-                BCU(launch_sad_cost(p0, p1, q.W, q.H, q.D, q.Dp, q.p.minDisparity, q.r, b->magic, wide, cost, s));
-            }
-            nl += 2;
-        }
-        // one aggregation launch over all bands of the group
-        BCU(launch_aggregate_wave_batch(reinterpret_cast<const WaveJob*>(desc + g.jobsOff),
-                                        reinterpret_cast<const uint32_t*>(desc + g.tableOff), g.nTickets,
-                                        g.window, g.Wmax, g.Dp, g.wrap, g.full, g.diag, g.plan,
-                                        ticket, b->status, b->spinMax, s));
-        nl += 1;
-        // selection and post-processing
-        for (int i : g.pairs) {
-            const BatchPair& q = b->pairs[i];
-            int16_t* dl = reinterpret_cast<int16_t*>(base + q.oDispL);
-            int16_t* dr = reinterpret_cast<int16_t*>(base + q.oDispR);
-            BCU(launch_select(reinterpret_cast<uint16_t*>(base + q.oAgg), reinterpret_cast<uint16_t*>(base + q.oPartB),
-                              q.wrap, q.W, q.H, q.D, q.Dp, q.p.minDisparity, q.p.uniquenessRatio, dl, dr, s));
-            const int lr = q.p.disp12MaxDiff >= 0 ? q.p.disp12MaxDiff * 16 : -1;
-            const int spk = q.p.speckleWindowSize > 0 ? std::min(q.p.speckleWindowSize, 25) : 0;
-            BCU(launch_post(dl, dr, q.W, q.H, lr, spk, q.p.speckleRange * 16, q.out, (size_t)q.W, nullptr, s));
-            nl += 2;
-        }
-    }
+    lumen_status st = batch_enqueue_groups(b->pairs, b->groups, static_cast<const uint8_t*>(b->desc), b->magic,
+                                           b->status, b->spinMax, s, nullptr, nullptr, &nl);
     b->launches = nl;
-    return LUMEN_OK;
+    return st;
 }
 
 extern "C" lumen_status lumen_sgbm_batch_create(lumen_sgbm_batch** out) {
@@ -341,43 +417,10 @@ extern "C" lumen_status lumen_sgbm_batch_add(lumen_sgbm_batch* b, const lumen_st
                                              const uint8_t* d_left, const uint8_t* d_right, int width,
                                              int height, int16_t* d_out) {
     if (!b || !p) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "lumen_sgbm_batch_add: NULL argument");
-    if (!d_left || !d_right || width <= 0 || height <= 0)
-        return bfail(LUMEN_ERR_INVALID_ARGUMENT, "Input images are empty");
-    if (!d_out) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "output buffer is NULL");
-    const int D = p->maxDisparity - p->minDisparity;
-    if (D < 1)
-        return bfail(LUMEN_ERR_INVALID_ARGUMENT,
-                     "Invalid disparity range: maxDisparity must be greater than minDisparity");
-    if (D > LUMEN_MAX_DISPARITY_RANGE)
-        return bfail(LUMEN_ERR_RANGE_EXCEEDS_LIMIT,
-                     "Disparity range (maxDisparity - minDisparity) exceeds GPU limit (512). Reduce the search range.");
-    if (p->minDisparity < 0) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "minDisparity must be >= 0");
-    if (p->blockSize < 0 || p->blockSize > 21) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "blockSize must be in [0, 21]");
-    if (width < 2) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "image width must be at least 2");
-    if ((long long)p->maxDisparity * 16 > 32767)
-        return bfail(LUMEN_ERR_INVALID_ARGUMENT, "maxDisparity*16 must fit int16 disparities");
     if (b->pairs.size() >= 4095) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "a batch holds at most 4095 pairs");
-    BatchPair q{};
-    q.p = *p;
-    q.left = d_left;
-    q.right = d_right;
-    q.W = width;
-    q.H = height;
-    q.out = d_out;
-    q.D = D;
-    q.Dp = padded_d(D);
-    q.census = p->matchingCostMode == 1;
-    q.diag = p->numDirections >= 8;
-    q.r = p->blockSize / 2;
-    q.cap = std::max(1, p->preFilterCap);
-    const int cs = q.census ? std::max(1, (p->blockSize * p->blockSize * 2 * p->preFilterCap) / 255)
-                            : p->blockSize * p->blockSize;
-    q.wrap = !batch_no_wrap(*p, cs, q.diag ? 8 : 4);
-    q.full = q.D == q.Dp;
-    q.k.W = width; q.k.H = height; q.k.D = D; q.k.Dp = q.Dp;
-    q.k.P1 = p->P1; q.k.P2 = p->P2; q.k.costScale = cs;
-    q.k.p1x2 = ((uint32_t)p->P1 & 0xFFFFu) * 0x10001u;
-    q.k.bsub = ((uint32_t)(0xFFFF - p->P1) & 0xFFFFu) * 0x10001u;
+    BatchPair q;
+    lumen_status st = batch_pair_init(q, p, d_left, d_right, width, height, d_out);
+    if (st != LUMEN_OK) return st;
     b->pairs.push_back(q);
     b->planned = false;
     return LUMEN_OK;

@@ -160,6 +160,37 @@ def mix_item(seed: int):
     return spec, dmax, census, ndir
 
 
+def calibration_maps(calib_id: int, w: int, h: int):
+    """Rectification maps of a synthetic calibration (seed 500 + calib_id):
+    focal length f ~ U(1000, 2000) px, principal point at the centre, radial
+    distortion k1 ~ U(-0.1, 0.1), and per camera a rectifying rotation with
+    angles ~ U(-2, 2) degrees about each axis.  For every rectified pixel the
+    map holds the raw pixel it samples, the pinhole model with one radial
+    term: ray K^-1 (u, v, 1), rotated by R^T, projected, distorted by
+    (1 + k1 r^2) and mapped through K.  Returns float32 HxW arrays
+    (map0x, map0y, map1x, map1y), the inputs of StereoRectifier."""
+    rng = np.random.Generator(np.random.PCG64(500 + calib_id))
+    f = rng.uniform(1000.0, 2000.0)
+    k1 = rng.uniform(-0.1, 0.1)
+    cx, cy = (w - 1) / 2.0, (h - 1) / 2.0
+    u, v = np.meshgrid(np.arange(w, dtype=np.float64), np.arange(h, dtype=np.float64))
+    x, y = (u - cx) / f, (v - cy) / f
+    maps = []
+    for _ in range(2):
+        ax, ay, az = np.deg2rad(rng.uniform(-2.0, 2.0, 3))
+        rx = np.array([[1, 0, 0], [0, np.cos(ax), -np.sin(ax)], [0, np.sin(ax), np.cos(ax)]])
+        ry = np.array([[np.cos(ay), 0, np.sin(ay)], [0, 1, 0], [-np.sin(ay), 0, np.cos(ay)]])
+        rz = np.array([[np.cos(az), -np.sin(az), 0], [np.sin(az), np.cos(az), 0], [0, 0, 1]])
+        rt = (rz @ ry @ rx).T
+        X = rt[0, 0] * x + rt[0, 1] * y + rt[0, 2]
+        Y = rt[1, 0] * x + rt[1, 1] * y + rt[1, 2]
+        Z = rt[2, 0] * x + rt[2, 1] * y + rt[2, 2]
+        xp, yp = X / Z, Y / Z
+        d = 1.0 + k1 * (xp * xp + yp * yp)
+        maps += [(f * xp * d + cx).astype(np.float32), (f * yp * d + cy).astype(np.float32)]
+    return tuple(maps)
+
+
 def random_pair(w: int, h: int, seed: int, shift: int = 7):
     """Small random pair for unit tests: right = left shifted by ``shift`` px
     plus noise (cheap, no scene model)."""
