@@ -1,10 +1,8 @@
 // select.cu -- disparity selection and post-processing.
 //
-// select_team_kernel / select_row_kernel replace selectDisparityWTA +
-//                selectDisparityRight (src/sgbm_kernels.cu:748-856): the team
-//                kernel stages a row tile in shared memory and serves both
-//                views from it; the row kernel handles tiles too large for
-//                shared memory.
+// select_slide_kernel replaces selectDisparityWTA + selectDisparityRight
+//                (src/sgbm_kernels.cu:748-856): both views in one read of
+//                the aggregated volume.
 // post_kernel    replaces consistencyCheck + speckleFilter + medianFilter3x3
 //                and the device-to-device copy back (src/sgbm_kernels.cu:
 //                862-1013, src/sgbm_gpu.cu:460-515) with one tiled pass.
@@ -35,240 +33,164 @@ __device__ __forceinline__ int16_t subpixel_disp(float c0, float c1, float c2, i
 }
 
 // ---------------------------------------------------------------------------
-// select_team_kernel: the same two selections with teams of 8 lanes per pixel
-// (4 pixels per warp); a lane owns KS packed uint16x2 words (2*KS
-// disparities).  The left view takes the min with __vminu2, the first index
-// of the min with __vcmpeq2, and the second order statistic as the min with
-// that one element removed (the multiset statistic the reference's running
-// second-minimum computes, src/sgbm_kernels.cu:764-777); team reductions are
-// 3-step xor butterflies.  The right view gathers agg[y][xr+minD+d][d] from
-// the staged tile, rows padded to Dp+2 elements so that the diagonal spreads
-// over the shared-memory banks.
+// select_slide_kernel: both selections in ONE read of every aggregated vector.
+// A CTA owns an image row; teams of TL lanes walk contiguous segments of it
+// pixel by pixel, a lane holding M = 2*KS consecutive disparities of the
+// pixel (the sum of the two partial volumes).
+//  * left view: every element becomes a key (cost << 16 | d); the two
+//    smallest keys of the pixel (lane pairs merged by an xor butterfly) give
+//    the minimum, its first index (ties to the smaller d, like the
+//    reference's strict < scan, src/sgbm_kernels.cu:764-777) and the second
+//    order statistic (the min with that one element removed);
+//  * right view: right pixel xr collects keys from (x, d) with x - d =
+//    xr + minD, a diagonal of the volume.  The team keeps a sliding array of
+//    M*TL partial minima, slot d standing for xr = x - minD - d: stepping to
+//    x + 1 moves every slot up by one (in registers: the loop is unrolled M
+//    times, the physical register of a slot rotates with the step, and only
+//    the slot that crosses into the next lane moves, by one shuffle), then
+//    takes the min with the new pixel's keys.  The slot that leaves the top
+//    of the team holds a complete right pixel; it and the partial slots at a
+//    segment's two ends go to a row array in shared memory by atomicMin.
+// Subpixel neighbours are re-read from the (L1/L2-resident) volumes.  The
+// 1/16-px outputs equal the reference's bit for bit.
 // ---------------------------------------------------------------------------
 template <int KS>
-__global__ void __launch_bounds__(256)
-select_team_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict__ aggB, int wrap,
-                   int W, int D, int Dp, int minD, int UR, int T, int16_t* __restrict__ dispL,
-                   int16_t* __restrict__ dispR) {
-    extern __shared__ __align__(16) uint16_t sa[];
-    const int pitch = Dp + 2;
-    const int y = blockIdx.y;
-    const int x0 = blockIdx.x * T;
-    const int loadHi = min(W, x0 + T + D - 1);
-    const int nload = max(0, loadHi - x0);
-    {
-        const uint4* srcA = reinterpret_cast<const uint4*>(agg + ((size_t)y * W + x0) * Dp);
-        const uint4* srcB = aggB ? reinterpret_cast<const uint4*>(aggB + ((size_t)y * W + x0) * Dp) : nullptr;
-        const int per = Dp / 8;  // uint4 per pixel
-        for (int i = threadIdx.x; i < nload * per; i += blockDim.x) {
-            const int px = i / per, q = i - px * per;
-            uint4 v = srcA[i];
-            if (srcB) {
-                const uint4 w = srcB[i];
-                v = wrap ? make_uint4(__vadd2(v.x, w.x), __vadd2(v.y, w.y), __vadd2(v.z, w.z), __vadd2(v.w, w.w))
-                         : make_uint4(v.x + w.x, v.y + w.y, v.z + w.z, v.w + w.w);
+__device__ __forceinline__ void slide_load(const uint16_t* __restrict__ a, const uint16_t* __restrict__ b,
+                                           bool wrap, uint32_t (&w)[KS]) {
+    if constexpr (KS % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < KS / 4; ++i) {
+            uint4 v = __ldg(reinterpret_cast<const uint4*>(a) + i);
+            if (b) {
+                const uint4 u = __ldg(reinterpret_cast<const uint4*>(b) + i);
+                v = wrap ? make_uint4(__vadd2(v.x, u.x), __vadd2(v.y, u.y), __vadd2(v.z, u.z), __vadd2(v.w, u.w))
+                         : make_uint4(v.x + u.x, v.y + u.y, v.z + u.z, v.w + u.w);
             }
-            uint32_t* d = reinterpret_cast<uint32_t*>(sa + (size_t)px * pitch + q * 8);
-            d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+            w[4 * i] = v.x; w[4 * i + 1] = v.y; w[4 * i + 2] = v.z; w[4 * i + 3] = v.w;
         }
-    }
-    __syncthreads();
-    const int lane = threadIdx.x & 31, tl = lane & 7;
-    const int tteam = (threadIdx.x >> 5) * 4 + (lane >> 3);
-    const int nTeams = blockDim.x >> 3;
-    const int d0 = tl * 2 * KS;
-    const int Tr = (T + nTeams - 1) / nTeams * nTeams;  // uniform trip count for all teams
-    // ---------------- left view ----------------
-    for (int px = tteam; px < Tr; px += nTeams) {
-        const int x = x0 + px;
-        const bool ok = px < T && x < W;
-        const int pxc = ok ? px : 0;
-        const uint32_t* v32 = reinterpret_cast<const uint32_t*>(sa + (size_t)pxc * pitch) + tl * KS;
-        uint32_t w[KS];
+    } else {
+        static_assert(KS % 2 == 0, "lanes hold an even number of words");
 #pragma unroll
-        for (int k = 0; k < KS; ++k) {
-            uint32_t val = ok && nload > 0 ? v32[k] : 0xFFFFFFFFu;
-            if (d0 + 2 * k >= D) val |= 0x0000FFFFu;
-            if (d0 + 2 * k + 1 >= D) val |= 0xFFFF0000u;
-            w[k] = val;
-        }
-        uint32_t m = w[0];
-#pragma unroll
-        for (int k = 1; k < KS; ++k) m = __vminu2(m, w[k]);
-        m = min(m & 0xFFFFu, m >> 16);
-        m = min(m, __shfl_xor_sync(kFullMask, m, 4));
-        m = min(m, __shfl_xor_sync(kFullMask, m, 2));
-        m = min(m, __shfl_xor_sync(kFullMask, m, 1));
-        const uint32_t best = m, bx2 = best * 0x10001u;
-        uint32_t first = 0xFFFFu;
-#pragma unroll
-        for (int k = KS - 1; k >= 0; --k) {
-            const uint32_t eq = __vcmpeq2(w[k], bx2);
-            const uint32_t idx = (eq & 0xFFFFu) ? (uint32_t)(d0 + 2 * k)
-                                                : ((eq >> 16) ? (uint32_t)(d0 + 2 * k + 1) : 0xFFFFu);
-            first = min(first, idx);
-        }
-        first = min(first, __shfl_xor_sync(kFullMask, first, 4));
-        first = min(first, __shfl_xor_sync(kFullMask, first, 2));
-        first = min(first, __shfl_xor_sync(kFullMask, first, 1));
-        const int bestD = (int)first;
-        // second order statistic: min with the element at bestD removed
-        uint32_t m2 = 0xFFFFFFFFu;
-#pragma unroll
-        for (int k = 0; k < KS; ++k) {
-            uint32_t val = w[k];
-            if (d0 + 2 * k == bestD) val |= 0x0000FFFFu;
-            if (d0 + 2 * k + 1 == bestD) val |= 0xFFFF0000u;
-            m2 = __vminu2(m2, val);
-        }
-        m2 = min(m2 & 0xFFFFu, m2 >> 16);
-        m2 = min(m2, __shfl_xor_sync(kFullMask, m2, 4));
-        m2 = min(m2, __shfl_xor_sync(kFullMask, m2, 2));
-        m2 = min(m2, __shfl_xor_sync(kFullMask, m2, 1));
-        if (ok && tl == 0) {
-            const uint16_t* v = sa + (size_t)px * pitch;
-            int16_t out;
-            if (UR > 0 && m2 != 0xFFFFu && m2 <= best + (best * (uint32_t)UR) / 100u) {
-                out = -1;
-            } else if (bestD > 0 && bestD < D - 1) {
-                out = subpixel_disp((float)v[bestD - 1], (float)v[bestD], (float)v[bestD + 1],
-                                    bestD, D, minD);
-            } else {
-                out = subpixel_disp(0.f, 0.f, 0.f, bestD, D, minD);
+        for (int i = 0; i < KS / 2; ++i) {
+            uint2 v = __ldg(reinterpret_cast<const uint2*>(a) + i);
+            if (b) {
+                const uint2 u = __ldg(reinterpret_cast<const uint2*>(b) + i);
+                v = wrap ? make_uint2(__vadd2(v.x, u.x), __vadd2(v.y, u.y)) : make_uint2(v.x + u.x, v.y + u.y);
             }
-            dispL[(size_t)y * W + x] = out;
-        }
-    }
-    // ---------------- right view ----------------
-    for (int px = tteam; px < Tr; px += nTeams) {
-        const int xr = x0 - minD + px;
-        const bool ok = px < T && xr >= 0 && xr < W;
-        uint32_t key = 0xFFFFFFFFu;
-#pragma unroll
-        for (int j = 0; j < 2 * KS; ++j) {
-            const int d = d0 + j;
-            const int lx = x0 + px + d;
-            if (ok && d < D && lx < W) {
-                const uint32_t c = sa[(size_t)(px + d) * pitch + d];
-                key = min(key, (c << 16) | (uint32_t)d);
-            }
-        }
-        key = min(key, __shfl_xor_sync(kFullMask, key, 4));
-        key = min(key, __shfl_xor_sync(kFullMask, key, 2));
-        key = min(key, __shfl_xor_sync(kFullMask, key, 1));
-        if (ok && tl == 0) {
-            const int bestD = key == 0xFFFFFFFFu ? 0 : (int)(key & 0xFFFFu);
-            int16_t out;
-            if (bestD > 0 && bestD < D - 1) {
-                const uint16_t* v = sa + (size_t)(px + bestD) * pitch;
-                out = subpixel_disp((float)v[bestD - 1], (float)v[bestD], (float)v[bestD + 1],
-                                    bestD, D, minD);
-            } else {
-                out = subpixel_disp(0.f, 0.f, 0.f, bestD, D, minD);
-            }
-            dispR[(size_t)y * W + xr] = out;
+            w[2 * i] = v.x; w[2 * i + 1] = v.y;
         }
     }
 }
 
-constexpr size_t kSelectSmemMax = 227 * 1024;  // opt-in shared memory per block on sm_100
-
-template <int KS>
-static cudaError_t launch_select_team(const uint16_t* agg, const uint16_t* aggB, bool wrap, int W,
-                                      int H, int D, int Dp, int minD, int UR, int16_t* dispL,
-                                      int16_t* dispR, cudaStream_t s, bool* launched) {
-    int T = 0;
-    size_t smem = 0;
-    for (int t : {128, 64, 32}) {
-        const size_t b = (size_t)(t + D - 1) * (Dp + 2) * 2;
-        if (b <= kSelectSmemMax) { T = t; smem = b; break; }
-    }
-    *launched = false;
-    // a tile stages T + D - 1 pixels for T outputs: past ~2.5x re-reads the row
-    // kernel, which reads every vector once, is faster
-    if (T == 0 || 2 * (T + D - 1) > 5 * T) return cudaSuccess;
-    cudaError_t e = cudaFuncSetAttribute(select_team_kernel<KS>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    dim3 g((W + minD + T - 1) / T, H);
-    select_team_kernel<KS><<<g, 256, smem, s>>>(agg, aggB, wrap, W, D, Dp, minD, UR, T, dispL, dispR);
-    *launched = true;
-    return cudaGetLastError();
+__device__ __forceinline__ uint32_t vol_cost(const uint16_t* __restrict__ a, const uint16_t* __restrict__ b,
+                                             size_t i) {
+    uint32_t c = __ldg(a + i);
+    if (b) c = (c + __ldg(b + i)) & 0xFFFFu;
+    return c;
 }
 
-// ---------------------------------------------------------------------------
-// select_row_kernel: both selections for one image row per CTA (the
-// fallback when a tile of the team kernel does not fit in shared memory):
-// each aggregated vector is read once; the left view is a warp per pixel
-// with lane l holding d = l + 32 j, the right view a shared-memory
-// atomicMin over (cost << 16 | d) keys of right pixel xr = x - minD - d
-// (ties to the smaller d), whose subpixel neighbours are then read at the left
-// pixel xr + minD + bestD (src/sgbm_kernels.cu:839-845).
-// ---------------------------------------------------------------------------
-template <int NJ>
+template <int TL, int KS, bool FULL>
 __global__ void __launch_bounds__(256)
-select_row_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict__ aggB, int W,
-                  int D, int Dp, int minD, int UR, int16_t* __restrict__ dispL,
-                  int16_t* __restrict__ dispR) {
-    extern __shared__ uint32_t rec[];  // [W] right-view keys
+select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict__ aggB, int wrap,
+                    int W, int D, int Dp, int minD, int UR, int S, int16_t* __restrict__ dispL,
+                    int16_t* __restrict__ dispR) {
+    constexpr int M = 2 * KS;
+    constexpr uint32_t INF = 0xFFFFFFFFu;
+    extern __shared__ uint32_t rec[];  // [W] right-view keys of the row
     const int y = blockIdx.x;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int i = threadIdx.x; i < W; i += blockDim.x) rec[i] = 0xFFFFFFFFu;
+    for (int i = threadIdx.x; i < W; i += blockDim.x) rec[i] = INF;
     __syncthreads();
-    const uint16_t* rowA = agg + (size_t)y * W * Dp;
-    const uint16_t* rowB = aggB ? aggB + (size_t)y * W * Dp : nullptr;
-    auto cost_at = [&](int x, int d) -> uint32_t {
-        const size_t i = (size_t)x * Dp + d;
-        uint32_t c = rowA[i];
-        if (rowB) c = (c + rowB[i]) & 0xFFFFu;
-        return c;
-    };
-    for (int x = warp; x < W; x += nw) {
-        uint32_t key[NJ];
-        uint32_t kl = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    const int tl = lane & (TL - 1);
+    const int xs = (threadIdx.x / TL) * S;
+    const int d0 = tl * M;
+    const int nv = FULL ? M : min(max(D - d0, 0), M);
+    const size_t rowOff = (size_t)y * W * Dp;
+    const uint16_t* rowA = agg + rowOff + d0;
+    const uint16_t* rowB = aggB ? aggB + rowOff + d0 : nullptr;
+    uint32_t R[M];
 #pragma unroll
-        for (int j = 0; j < NJ; ++j) {
-            const int d = lane + 32 * j;
-            uint32_t k = 0xFFFFFFFFu;
-            if (d < D) k = (cost_at(x, d) << 16) | (uint32_t)d;
-            key[j] = k;
-            kl = min(kl, k);
-        }
-        const uint32_t kmin = __reduce_min_sync(kFullMask, kl);
-        const uint32_t best = kmin >> 16;
-        const int bestD = (int)(kmin & 0xFFFFu);
-        uint32_t m2 = 0xFFFFu;
+    for (int j = 0; j < M; ++j) R[j] = INF;
+    uint32_t wn[KS];
+    if (xs < W) slide_load<KS>(rowA + (size_t)xs * Dp, rowB ? rowB + (size_t)xs * Dp : nullptr, wrap, wn);
+    for (int s = 0; s < S; s += M) {
 #pragma unroll
-        for (int j = 0; j < NJ; ++j)
-            if (key[j] != 0xFFFFFFFFu && (int)(key[j] & 0xFFFFu) != bestD) m2 = min(m2, key[j] >> 16);
-        const uint32_t second = __reduce_min_sync(kFullMask, m2);
-        if (lane == 0) {
-            int16_t out;
-            if (UR > 0 && second != 0xFFFFu && second <= best + (best * (uint32_t)UR) / 100u) {
-                out = -1;
-            } else if (bestD > 0 && bestD < D - 1) {
-                out = subpixel_disp((float)cost_at(x, bestD - 1), (float)best, (float)cost_at(x, bestD + 1),
-                                    bestD, D, minD);
-            } else {
-                out = subpixel_disp(0.f, 0.f, 0.f, bestD, D, minD);
+        for (int u = 0; u < M; ++u) {
+            const int x = xs + s + u;
+            const bool px = x < W;
+            uint32_t w[KS];
+#pragma unroll
+            for (int k = 0; k < KS; ++k) w[k] = wn[k];
+            if (x + 1 < W && (s + u + 1) < S)
+                slide_load<KS>(rowA + (size_t)(x + 1) * Dp, rowB ? rowB + (size_t)(x + 1) * Dp : nullptr, wrap, wn);
+            // slide by one: the slot leaving this lane (logical M-1, physical
+            // (M-1-u) mod M) enters the next lane as its logical slot 0 and
+            // this lane's logical 0 takes the previous lane's
+            const int q = (M - 1 - u + M) % M;
+            const uint32_t leaving = R[q];
+            const uint32_t incoming = __shfl_up_sync(kFullMask, leaving, 1, TL);
+            R[q] = tl == 0 ? INF : incoming;
+            const uint32_t pxmask = px ? 0u : INF;
+            uint32_t k1 = INF, k2 = INF;
+#pragma unroll
+            for (int j = 0; j < M; ++j) {
+                const uint32_t c = (j & 1) ? (w[j >> 1] & 0xFFFF0000u) : (w[j >> 1] << 16);
+                uint32_t key = (c + (uint32_t)(d0 + j)) | pxmask;
+                if (!FULL) key |= (j < nv) ? 0u : INF;
+                const int p = ((j - u - 1) % M + M) % M;  // logical j after the slide
+                R[p] = min(R[p], key);
+                k2 = min(k2, max(k1, key));
+                k1 = min(k1, key);
             }
-            dispL[(size_t)y * W + x] = out;
-        }
+            // complete right pixel: the top slot of the team
+            if (tl == TL - 1) {
+                const int xr = x - minD - (M * TL - 1);
+                if (xr >= 0 && xr < W) atomicMin(&rec[xr], R[(M - 1 - u - 1 + 2 * M) % M]);
+            }
+            // left view: merge the lanes' two smallest keys
 #pragma unroll
-        for (int j = 0; j < NJ; ++j) {
-            const int xr = x - minD - (lane + 32 * j);
-            if (key[j] != 0xFFFFFFFFu && xr >= 0) atomicMin(&rec[xr], key[j]);
+            for (int o = TL / 2; o >= 1; o >>= 1) {
+                const uint32_t b1 = __shfl_xor_sync(kFullMask, k1, o);
+                const uint32_t b2 = __shfl_xor_sync(kFullMask, k2, o);
+                k2 = min(max(k1, b1), min(k2, b2));
+                k1 = min(k1, b1);
+            }
+            if (tl == 0 && px) {
+                const uint32_t best = k1 >> 16, second = k2 >> 16;
+                const int bestD = (int)(k1 & 0xFFFFu);
+                int16_t out;
+                if (UR > 0 && second != 0xFFFFu && second <= best + (best * (uint32_t)UR) / 100u) {
+                    out = -1;
+                } else if (bestD > 0 && bestD < D - 1) {
+                    const size_t i0 = rowOff + (size_t)x * Dp + bestD;
+                    out = subpixel_disp((float)vol_cost(agg, aggB, i0 - 1), (float)best,
+                                        (float)vol_cost(agg, aggB, i0 + 1), bestD, D, minD);
+                } else {
+                    out = subpixel_disp(0.f, 0.f, 0.f, bestD, D, minD);
+                }
+                dispL[(size_t)y * W + x] = out;
+            }
+        }
+    }
+    // the partial slots at the segment's end (S is a multiple of M, so the
+    // rotation is back at phase 0: logical j is physical j)
+    {
+        const int xe = xs + S - 1;
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+            const int xr = xe - minD - (d0 + j);
+            if (R[j] != INF && xr >= 0 && xr < W) atomicMin(&rec[xr], R[j]);
         }
     }
     __syncthreads();
     for (int xr = threadIdx.x; xr < W; xr += blockDim.x) {
         const uint32_t k = rec[xr];
-        const int bestD = k == 0xFFFFFFFFu ? 0 : (int)(k & 0xFFFFu);
+        const int bestD = k == INF ? 0 : (int)(k & 0xFFFFu);
         int16_t out;
         if (bestD > 0 && bestD < D - 1) {
-            const int lx = xr + minD + bestD;
-            out = subpixel_disp((float)cost_at(lx, bestD - 1), (float)(k >> 16), (float)cost_at(lx, bestD + 1),
-                                bestD, D, minD);
+            const size_t i0 = rowOff + (size_t)(xr + minD + bestD) * Dp + bestD;
+            out = subpixel_disp((float)vol_cost(agg, aggB, i0 - 1), (float)(k >> 16),
+                                (float)vol_cost(agg, aggB, i0 + 1), bestD, D, minD);
         } else {
             out = subpixel_disp(0.f, 0.f, 0.f, bestD, D, minD);
         }
@@ -276,19 +198,24 @@ select_row_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict__
     }
 }
 
-template <int NJ>
-static cudaError_t launch_select_row(const uint16_t* agg, const uint16_t* aggB, int W, int H, int D,
-                                     int Dp, int minD, int UR, int16_t* dispL, int16_t* dispR,
-                                     cudaStream_t s) {
+template <int TL, int KS>
+static cudaError_t launch_select_slide(const uint16_t* agg, const uint16_t* aggB, bool wrap, int W, int H,
+                                       int D, int Dp, int minD, int UR, int16_t* dispL, int16_t* dispR,
+                                       cudaStream_t s) {
+    constexpr int M = 2 * KS, kTeams = 256 / TL;
+    const int seg = (W + kTeams - 1) / kTeams;
+    const int S = (seg + M - 1) / M * M;
     const size_t smem = (size_t)W * 4;
+    auto kern = D == Dp ? select_slide_kernel<TL, KS, true> : select_slide_kernel<TL, KS, false>;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(select_row_kernel<NJ>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    select_row_kernel<NJ><<<H, 256, smem, s>>>(agg, aggB, W, D, Dp, minD, UR, dispL, dispR);
+    kern<<<H, 256, smem, s>>>(agg, aggB, wrap ? 1 : 0, W, D, Dp, minD, UR, S, dispL, dispR);
     return cudaGetLastError();
 }
+
+constexpr size_t kSelectSmemMax = 227 * 1024;  // opt-in shared memory per block on sm_100
 
 bool select_needs_summed_volume(int D, int Dp) {
     (void)D;
@@ -315,28 +242,16 @@ void launch_sum_volumes(const uint16_t* a, const uint16_t* b, uint16_t* dst, siz
 cudaError_t launch_select(const uint16_t* agg, const uint16_t* aggB, bool wrap, int W, int H,
                           int D, int Dp, int minD, int UR, int16_t* dispL, int16_t* dispR,
                           cudaStream_t s) {
-    bool launched = false;
-    cudaError_t e = cudaSuccess;
-    switch (Dp / 16) {
-    case 4: e = launch_select_team<4>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, &launched); break;
-    case 8: e = launch_select_team<8>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, &launched); break;
-    case 12: e = launch_select_team<12>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, &launched); break;
-    case 16: e = launch_select_team<16>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, &launched); break;
-    case 20: e = launch_select_team<20>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, &launched); break;
-    default: break;
-    }
-    if (e != cudaSuccess || launched) return e;
-    // the row kernel sums uint16 values mod 2^16 whether or not they can wrap
-    if ((size_t)W * 4 > kSelectSmemMax) return cudaErrorInvalidValue;
-    switch (Dp / 32) {
-    case 2: return launch_select_row<2>(agg, aggB, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 4: return launch_select_row<4>(agg, aggB, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 6: return launch_select_row<6>(agg, aggB, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 8: return launch_select_row<8>(agg, aggB, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 10: return launch_select_row<10>(agg, aggB, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 12: return launch_select_row<12>(agg, aggB, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 14: return launch_select_row<14>(agg, aggB, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 16: return launch_select_row<16>(agg, aggB, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    if ((size_t)W * 4 > kSelectSmemMax) return cudaErrorInvalidValue;  // W > 58112: no row array
+    switch (Dp / 64) {
+    case 1: return launch_select_slide<8, 4>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 2: return launch_select_slide<8, 8>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 3: return launch_select_slide<8, 12>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 4: return launch_select_slide<8, 16>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 5: return launch_select_slide<8, 20>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 6: return launch_select_slide<16, 12>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 7: return launch_select_slide<16, 14>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 8: return launch_select_slide<16, 16>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
     default: return cudaErrorInvalidValue;
     }
 }
