@@ -202,9 +202,12 @@ lumen_status lumen_bgr_to_gray(const uint8_t* bgr, size_t stride, uint8_t* gray,
  * pitch width, 1/16 px, -1 invalid).  lumen_sgbm_batch_run enqueues every pair
  * on `stream`: cost volumes per pair, one persistent aggregation launch per
  * group of pairs of one kernel class (the wavefronts of all its pairs share
- * the GPU), then selection per pair.  The first run after an add, a clear or
- * an option change plans and allocates one pooled buffer (groups are cut so
- * each fits device_budget_bytes, default 48 GiB) and, with graphs enabled,
+ * the GPU), then selection per pair; consecutive groups overlap on the device
+ * (one group's sweep beside the next one's cost volumes and the previous one's
+ * selections, on internal streams joined back into `stream`).  The first run
+ * after an add, a clear or an option change plans and allocates one pooled
+ * buffer of at most device_budget_bytes (default 80 GiB; groups are cut to
+ * fit it, two at a time when possible) and, with graphs enabled,
  * captures the run into a CUDA graph that later runs replay.  Outputs equal
  * lumen_sgbm_compute_device's bit for bit.  lumen_sgbm_batch_sync waits for
  * `stream` and reports a device-side timeout. */

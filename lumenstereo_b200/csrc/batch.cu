@@ -8,9 +8,11 @@
 // pairs (wave_kernel.cuh, tickets in band-major order within chunks), so the
 // wavefronts of different pairs fill the GPU together.  Cost volumes and the
 // selection run per pair around it.  Buffers come from one pooled device
-// allocation reused group after group, sized by a device-memory budget; with
-// graphs enabled the whole run is captured once into a CUDA graph and
-// replayed.  Every pair's output equals lumen_sgbm_compute_device's for the
+// allocation sized by a device-memory budget, in two regions that alternate
+// between consecutive groups so that groups overlap on the device (one
+// group's sweep beside the next one's cost volumes and the previous one's
+// selections); with graphs enabled the whole run is captured once into a
+// CUDA graph and replayed.  Every pair's output equals lumen_sgbm_compute_device's for the
 // same pair bit for bit.
 //
 // The launch core (batch_pair_*, batch_group_by_class, batch_describe,
@@ -213,6 +215,63 @@ lumen_status batch_describe(const std::vector<BatchPair>& pairs, std::vector<Bat
     return LUMEN_OK;
 }
 
+lumen_status batch_enqueue_costs(const std::vector<BatchPair>& pairs, const BatchGroup& g, const uint8_t* desc,
+                                 const uint32_t* magic, cudaStream_t s, unsigned long long* launches) {
+    // counters of the group's pairs and the group's ticket
+    for (int i : g.pairs) {
+        const BatchPair& q = pairs[i];
+        BCU(cudaMemsetAsync(q.base + q.oCtr, 0, ctr_bytes(q.nBands), s));
+    }
+    unsigned* ticket = reinterpret_cast<unsigned*>(const_cast<uint8_t*>(desc) + g.tableOff +
+                                                   sizeof(uint32_t) * (size_t)g.nTickets);
+    BCU(cudaMemsetAsync(ticket, 0, 4, s));
+    for (int i : g.pairs) {
+        const BatchPair& q = pairs[i];
+        uint8_t* cost = q.base + q.oCost;
+        if (q.census) {
+            uint32_t* c0 = reinterpret_cast<uint32_t*>(q.base + q.oAux0);
+            uint32_t* c1 = reinterpret_cast<uint32_t*>(q.base + q.oAux1);
+            launch_census(q.left, q.right, q.W, q.H, c0, c1, s);
+            BCU(launch_census_cost(c0, c1, q.W, q.H, q.D, q.Dp, q.p.minDisparity, cost, s));
+        } else {
+            uint8_t* p0 = q.base + q.oAux0;
+            uint8_t* p1 = q.base + q.oAux1;
+            launch_prefilter(q.left, q.right, q.W, q.H, q.cap, p0, p1, s);
+            const int wide = (long long)(2 * q.r + 1) * (2 * q.r + 1) * 2 * q.cap > 65535;
+            BCU(launch_sad_cost(p0, p1, q.W, q.H, q.D, q.Dp, q.p.minDisparity, q.r, magic, wide, cost, s));
+        }
+        *launches += 2;
+    }
+    return LUMEN_OK;
+}
+
+lumen_status batch_enqueue_wave(const BatchGroup& g, const uint8_t* desc, int* status, long long spinMax,
+                                cudaStream_t s, unsigned long long* launches) {
+    unsigned* ticket = reinterpret_cast<unsigned*>(const_cast<uint8_t*>(desc) + g.tableOff +
+                                                   sizeof(uint32_t) * (size_t)g.nTickets);
+    BCU(launch_aggregate_wave_batch(reinterpret_cast<const WaveJob*>(desc + g.jobsOff),
+                                    reinterpret_cast<const uint32_t*>(desc + g.tableOff), g.nTickets, g.window,
+                                    g.Wmax, g.Dp, g.wrap, g.full, g.diag, g.plan, ticket, status, spinMax, s));
+    *launches += 1;
+    return LUMEN_OK;
+}
+
+lumen_status batch_enqueue_selects(const std::vector<BatchPair>& pairs, const BatchGroup& g, cudaStream_t s,
+                                   unsigned long long* launches) {
+    for (int i : g.pairs) {
+        const BatchPair& q = pairs[i];
+        int16_t* dl = reinterpret_cast<int16_t*>(q.base + q.oDispL);
+        int16_t* dr = reinterpret_cast<int16_t*>(q.base + q.oDispR);
+        BCU(launch_select(reinterpret_cast<uint16_t*>(q.base + q.oAgg), reinterpret_cast<uint16_t*>(q.base + q.oPartB),
+                          q.wrap, q.W, q.H, q.D, q.Dp, q.p.minDisparity, q.p.uniquenessRatio, dl, dr, s));
+        const int lr = q.p.disp12MaxDiff >= 0 ? q.p.disp12MaxDiff * 16 : -1;
+        const int spk = q.p.speckleWindowSize > 0 ? std::min(q.p.speckleWindowSize, 25) : 0;
+        BCU(launch_post(dl, dr, q.W, q.H, lr, spk, q.p.speckleRange * 16, q.out, (size_t)q.W, nullptr, s));
+        *launches += 2;
+    }
+    return LUMEN_OK;
+}
+
 lumen_status batch_enqueue_groups(const std::vector<BatchPair>& pairs,
                                   const std::vector<BatchGroup>& groups, const uint8_t* desc,
                                   const uint32_t* magic, int* status, long long spinMax,
@@ -221,32 +280,8 @@ lumen_status batch_enqueue_groups(const std::vector<BatchPair>& pairs,
     unsigned long long nl = 0;
     int gi = 0;
     for (const BatchGroup& g : groups) {
-        // counters of the group's pairs and the group's ticket
-        for (int i : g.pairs) {
-            const BatchPair& q = pairs[i];
-            BCU(cudaMemsetAsync(q.base + q.oCtr, 0, ctr_bytes(q.nBands), s));
-        }
-        unsigned* ticket = reinterpret_cast<unsigned*>(const_cast<uint8_t*>(desc) + g.tableOff +
-                                                       sizeof(uint32_t) * (size_t)g.nTickets);
-        BCU(cudaMemsetAsync(ticket, 0, 4, s));
-        // cost volumes
-        for (int i : g.pairs) {
-            const BatchPair& q = pairs[i];
-            uint8_t* cost = q.base + q.oCost;
-            if (q.census) {
-                uint32_t* c0 = reinterpret_cast<uint32_t*>(q.base + q.oAux0);
-                uint32_t* c1 = reinterpret_cast<uint32_t*>(q.base + q.oAux1);
-                launch_census(q.left, q.right, q.W, q.H, c0, c1, s);
-                BCU(launch_census_cost(c0, c1, q.W, q.H, q.D, q.Dp, q.p.minDisparity, cost, s));
-            } else {
-                uint8_t* p0 = q.base + q.oAux0;
-                uint8_t* p1 = q.base + q.oAux1;
-                launch_prefilter(q.left, q.right, q.W, q.H, q.cap, p0, p1, s);
-                const int wide = (long long)(2 * q.r + 1) * (2 * q.r + 1) * 2 * q.cap > 65535;
-                BCU(launch_sad_cost(p0, p1, q.W, q.H, q.D, q.Dp, q.p.minDisparity, q.r, magic, wide, cost, s));
-            }
-            nl += 2;
-        }
+        lumen_status st = batch_enqueue_costs(pairs, g, desc, magic, s, &nl);
+        if (st != LUMEN_OK) return st;
         // one aggregation launch over all bands of the group
         cudaStream_t as = s;
         if (agg) {
@@ -254,27 +289,14 @@ lumen_status batch_enqueue_groups(const std::vector<BatchPair>& pairs,
             BCU(cudaStreamWaitEvent(agg, evs[2 * gi], 0));
             as = agg;
         }
-        BCU(launch_aggregate_wave_batch(reinterpret_cast<const WaveJob*>(desc + g.jobsOff),
-                                        reinterpret_cast<const uint32_t*>(desc + g.tableOff), g.nTickets,
-                                        g.window, g.Wmax, g.Dp, g.wrap, g.full, g.diag, g.plan, ticket,
-                                        status, spinMax, as));
+        st = batch_enqueue_wave(g, desc, status, spinMax, as, &nl);
+        if (st != LUMEN_OK) return st;
         if (agg) {
             BCU(cudaEventRecord(evs[2 * gi + 1], agg));
             BCU(cudaStreamWaitEvent(s, evs[2 * gi + 1], 0));
         }
-        nl += 1;
-        // selection and post-processing
-        for (int i : g.pairs) {
-            const BatchPair& q = pairs[i];
-            int16_t* dl = reinterpret_cast<int16_t*>(q.base + q.oDispL);
-            int16_t* dr = reinterpret_cast<int16_t*>(q.base + q.oDispR);
-            BCU(launch_select(reinterpret_cast<uint16_t*>(q.base + q.oAgg), reinterpret_cast<uint16_t*>(q.base + q.oPartB),
-                              q.wrap, q.W, q.H, q.D, q.Dp, q.p.minDisparity, q.p.uniquenessRatio, dl, dr, s));
-            const int lr = q.p.disp12MaxDiff >= 0 ? q.p.disp12MaxDiff * 16 : -1;
-            const int spk = q.p.speckleWindowSize > 0 ? std::min(q.p.speckleWindowSize, 25) : 0;
-            BCU(launch_post(dl, dr, q.W, q.H, lr, spk, q.p.speckleRange * 16, q.out, (size_t)q.W, nullptr, s));
-            nl += 2;
-        }
+        st = batch_enqueue_selects(pairs, g, s, &nl);
+        if (st != LUMEN_OK) return st;
         ++gi;
     }
     if (launches) *launches = nl;
@@ -291,7 +313,7 @@ struct lumen_sgbm_batch {
     bool planned = false;
     int rows = 0;       // rows per band (0: 8)
     int useGraph = 0;
-    size_t budget = 48ull << 30;
+    size_t budget = 80ull << 30;
     int numSMs = 148;
     long long spinMax = 1ll << 22;
     void* pool = nullptr;
@@ -301,6 +323,11 @@ struct lumen_sgbm_batch {
     uint32_t* magic = nullptr;
     int* status = nullptr;
     cudaStream_t capStream = nullptr;
+    // overlapped runs: sweeps on aggS, at the highest priority, selections on
+    // selS, cost volumes on the caller's stream
+    bool overlap = false;
+    cudaStream_t aggS = nullptr, selS = nullptr;
+    std::vector<cudaEvent_t> evs;  // fork, 2 joins, then 3 per group
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     unsigned long long launches = 0;  // kernels per run
@@ -313,14 +340,23 @@ static void batch_release(lumen_sgbm_batch* b) {
     b->graph = nullptr;
     if (b->pool) cudaFree(b->pool);
     if (b->desc) cudaFree(b->desc);
+    for (cudaEvent_t e : b->evs) cudaEventDestroy(e);
+    b->evs.clear();
+    b->overlap = false;
     b->pool = b->desc = nullptr;
     b->poolBytes = b->descBytes = 0;
     b->planned = false;
 }
 
-// Buffers, groups, job descriptors and ticket tables for the current pairs:
-// each class is cut into groups by the budget, and every group's buffers are
-// laid out from the start of one pool that the groups reuse in turn.
+// Buffers, groups, job descriptors and ticket tables for the current pairs.
+// Each class is cut into groups whose buffers fit a cap.  Overlapped runs lay
+// the groups out alternately in two regions of the pool (even groups in the
+// first, odd in the second), so that one group's sweep runs beside the next
+// group's cost volumes and the previous group's selections; a group reuses
+// its region once the group two before it has been selected.  The cap is the
+// budget when the two largest alternate groups fit it together, else half the
+// budget.  When even that fails (a single pair above half the budget), the
+// groups run one after the other in one region of budget bytes.
 static lumen_status batch_plan(lumen_sgbm_batch* b) {
     batch_release(b);
     const int R = b->rows ? b->rows : 8;
@@ -328,33 +364,67 @@ static lumen_status batch_plan(lumen_sgbm_batch* b) {
     for (int i = 0; i < (int)all.size(); ++i) all[i] = i;
     std::vector<BatchGroup> classes;
     batch_group_by_class(b->pairs, all, classes);
-    b->groups.clear();
-    size_t poolNeed = 0;
-    for (const BatchGroup& c : classes) {
-        BatchGroup g = c;
-        g.pairs.clear();
-        g.Wmax = 0;
-        size_t bytes = 0;
-        auto flush = [&]() {
-            if (!g.pairs.empty()) {
-                poolNeed = std::max(poolNeed, bytes);
-                b->groups.push_back(g);
-            }
+    std::vector<size_t> gbytes;
+    bool tooBig = false;
+    auto cut = [&](size_t cap) {
+        b->groups.clear();
+        gbytes.clear();
+        tooBig = false;
+        for (const BatchGroup& c : classes) {
+            BatchGroup g = c;
             g.pairs.clear();
             g.Wmax = 0;
-            bytes = 0;
-        };
-        for (int i : c.pairs) {
-            BatchPair& q = b->pairs[i];
-            const size_t need = batch_pair_bytes(q, R);
-            if (!g.pairs.empty() && bytes + need > b->budget) flush();
-            if (need > b->budget)
-                return bfail(LUMEN_ERR_OUT_OF_BUDGET, "batch: one pair needs more device memory than the budget");
-            bytes = batch_pair_layout(q, R, bytes);
-            g.pairs.push_back(i);
-            g.Wmax = std::max(g.Wmax, q.W);
+            size_t bytes = 0;
+            auto flush = [&]() {
+                if (!g.pairs.empty()) {
+                    b->groups.push_back(g);
+                    gbytes.push_back(bytes);
+                }
+                g.pairs.clear();
+                g.Wmax = 0;
+                bytes = 0;
+            };
+            for (int i : c.pairs) {
+                const size_t need = batch_pair_bytes(b->pairs[i], R);
+                if (need > cap) tooBig = true;
+                if (!g.pairs.empty() && bytes + need > cap) flush();
+                bytes += need;
+                g.pairs.push_back(i);
+                g.Wmax = std::max(g.Wmax, b->pairs[i].W);
+            }
+            flush();
         }
-        flush();
+    };
+    auto regions = [&](size_t* even, size_t* odd) {
+        *even = *odd = 0;
+        for (size_t gi = 0; gi < gbytes.size(); ++gi) {
+            size_t& r = gi % 2 ? *odd : *even;
+            r = std::max(r, gbytes[gi]);
+        }
+    };
+    cut(b->budget);
+    if (tooBig) return bfail(LUMEN_ERR_OUT_OF_BUDGET, "batch: one pair needs more device memory than the budget");
+    size_t even = 0, odd = 0;
+    regions(&even, &odd);
+    if (b->groups.size() > 1 && even + odd > b->budget) {
+        cut(b->budget / 2);
+        regions(&even, &odd);
+        if (tooBig) {  // no two groups fit side by side: one region, groups in turn
+            cut(b->budget);
+            regions(&even, &odd);
+            odd = 0;
+        }
+    }
+    b->overlap = b->groups.size() > 1 && odd > 0;
+    size_t poolNeed = 0;
+    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+        size_t o = b->overlap && gi % 2 ? even : 0;
+        for (int i : b->groups[gi].pairs) o = batch_pair_layout(b->pairs[i], R, o);
+        poolNeed = std::max(poolNeed, o);
+    }
+    if (b->overlap) {
+        b->evs.resize(3 + 3 * b->groups.size(), nullptr);
+        for (cudaEvent_t& e : b->evs) BCU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     BCU(cudaMalloc(&b->pool, std::max<size_t>(poolNeed, 256)));
     b->poolBytes = poolNeed;
@@ -371,10 +441,40 @@ static lumen_status batch_plan(lumen_sgbm_batch* b) {
 
 static lumen_status batch_enqueue(lumen_sgbm_batch* b, cudaStream_t s) {
     unsigned long long nl = 0;
-    lumen_status st = batch_enqueue_groups(b->pairs, b->groups, static_cast<const uint8_t*>(b->desc), b->magic,
-                                           b->status, b->spinMax, s, nullptr, nullptr, &nl);
+    const uint8_t* desc = static_cast<const uint8_t*>(b->desc);
+    if (!b->overlap) {
+        lumen_status st = batch_enqueue_groups(b->pairs, b->groups, desc, b->magic, b->status, b->spinMax, s,
+                                               nullptr, nullptr, &nl);
+        b->launches = nl;
+        return st;
+    }
+    // fork the sweep and selection streams off `s` (inside a capture too)
+    cudaEvent_t* ev = b->evs.data();
+    BCU(cudaEventRecord(ev[0], s));
+    BCU(cudaStreamWaitEvent(b->aggS, ev[0], 0));
+    BCU(cudaStreamWaitEvent(b->selS, ev[0], 0));
+    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+        const BatchGroup& g = b->groups[gi];
+        cudaEvent_t costsDone = ev[3 + 3 * gi], sweepDone = ev[4 + 3 * gi], selDone = ev[5 + 3 * gi];
+        if (gi >= 2) BCU(cudaStreamWaitEvent(s, ev[5 + 3 * (gi - 2)], 0));  // its region is free again
+        lumen_status st = batch_enqueue_costs(b->pairs, g, desc, b->magic, s, &nl);
+        if (st != LUMEN_OK) return st;
+        BCU(cudaEventRecord(costsDone, s));
+        BCU(cudaStreamWaitEvent(b->aggS, costsDone, 0));
+        st = batch_enqueue_wave(g, desc, b->status, b->spinMax, b->aggS, &nl);
+        if (st != LUMEN_OK) return st;
+        BCU(cudaEventRecord(sweepDone, b->aggS));
+        BCU(cudaStreamWaitEvent(b->selS, sweepDone, 0));
+        st = batch_enqueue_selects(b->pairs, g, b->selS, &nl);
+        if (st != LUMEN_OK) return st;
+        BCU(cudaEventRecord(selDone, b->selS));
+    }
+    BCU(cudaEventRecord(ev[1], b->aggS));
+    BCU(cudaEventRecord(ev[2], b->selS));
+    BCU(cudaStreamWaitEvent(s, ev[1], 0));
+    BCU(cudaStreamWaitEvent(s, ev[2], 0));
     b->launches = nl;
-    return st;
+    return LUMEN_OK;
 }
 
 extern "C" lumen_status lumen_sgbm_batch_create(lumen_sgbm_batch** out) {
@@ -393,6 +493,11 @@ extern "C" lumen_status lumen_sgbm_batch_create(lumen_sgbm_batch** out) {
     if (e == cudaSuccess) e = cudaMalloc(&b->magic, 443 * sizeof(uint32_t));
     if (e == cudaSuccess) e = launch_magic(b->magic, 443, 0);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->capStream, cudaStreamNonBlocking);
+    int prLeast = 0, prGreatest = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prLeast, &prGreatest);
+    // sweeps first: their CTAs wait on one another, the other kernels do not
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&b->aggS, cudaStreamNonBlocking, prGreatest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->selS, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
         lumen_sgbm_batch_destroy(b);
@@ -409,6 +514,8 @@ extern "C" lumen_status lumen_sgbm_batch_destroy(lumen_sgbm_batch* b) {
     if (b->status) cudaFree(b->status);
     if (b->magic) cudaFree(b->magic);
     if (b->capStream) cudaStreamDestroy(b->capStream);
+    if (b->aggS) cudaStreamDestroy(b->aggS);
+    if (b->selS) cudaStreamDestroy(b->selS);
     delete b;
     return LUMEN_OK;
 }

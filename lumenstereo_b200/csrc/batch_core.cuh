@@ -60,6 +60,15 @@ void batch_group_by_class(const std::vector<BatchPair>& pairs, const std::vector
 // `host` (resized); descriptor offsets go into the groups.
 lumen_status batch_describe(const std::vector<BatchPair>& pairs, std::vector<BatchGroup>& groups,
                             int R, int numSMs, std::vector<uint8_t>& host);
+// The three phases of one group: counters and cost volumes, the persistent
+// sweep launch, selection and post-processing (each adds its kernels to
+// *launches).
+lumen_status batch_enqueue_costs(const std::vector<BatchPair>& pairs, const BatchGroup& g, const uint8_t* desc,
+                                 const uint32_t* magic, cudaStream_t s, unsigned long long* launches);
+lumen_status batch_enqueue_wave(const BatchGroup& g, const uint8_t* desc, int* status, long long spinMax,
+                                cudaStream_t s, unsigned long long* launches);
+lumen_status batch_enqueue_selects(const std::vector<BatchPair>& pairs, const BatchGroup& g, cudaStream_t s,
+                                   unsigned long long* launches);
 // Enqueues, group after group, the cost volumes, the sweep launch and the
 // selection/post-processing of every pair; `desc` holds the uploaded
 // descriptors.  Sweep launches may go to their own stream `agg` (NULL: `s`),

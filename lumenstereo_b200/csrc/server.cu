@@ -445,7 +445,10 @@ extern "C" lumen_status lumen_server_create(const lumen_server_options* opt, lum
     S->st.budget_bytes = o.device_budget_bytes;
     e = cudaMalloc(&S->magic, 443 * sizeof(uint32_t));
     if (e == cudaSuccess) e = launch_magic(S->magic, 443, 0);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->agg, cudaStreamNonBlocking);
+    int prLeast = 0, prGreatest = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prLeast, &prGreatest);
+    // sweeps first: their CTAs wait on one another, the other kernels do not
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&S->agg, cudaStreamNonBlocking, prGreatest);
     S->slots.resize(o.max_inflight);
     for (Slot& sl : S->slots) {
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sl.s, cudaStreamNonBlocking);
