@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(synth.WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--schedule", type=int, default=0, help="aggregation schedule (0 = auto)")
+    ap.add_argument("--rows", type=int, default=0,
+                    help="rows per band of the fused sweeps with --schedule 3/4 (0 = default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve"],
                     help="plain: one pair per call (default); batch: the 64-pair mixed stream; "
@@ -227,6 +229,8 @@ def run_ours(args):
     sgbm = StereoSGBM(params)
     if args.schedule:
         sgbm.set_schedule(args.schedule)
+        if args.rows:
+            sgbm.set_tuning(32, args.rows)
     stream = torch.cuda.current_stream(dev)
     sptr = stream.cuda_stream
     dl = torch.from_numpy(left).to(dev)

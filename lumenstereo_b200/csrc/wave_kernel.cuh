@@ -32,9 +32,11 @@
 //    0 and R-1 through shared-memory counters (acquire/release at CTA scope),
 //    so global-memory latency never stalls a step;
 //  * bands are handed out by a ticket counter in dependency order (band b of a
-//    sweep after band b-1), so every wait is on a band a running CTA owns (or
-//    one that the lowest running tickets can free a CTA for): no co-residency
-//    requirement, any grid of at least three CTAs.
+//    sweep after band b-1), and a CTA takes a ticket only while it runs.  A
+//    band waits on the band above it (its input) and, through the exchange
+//    ring's back-pressure, on the next wave_lookahead_bands(W) bands below it;
+//    all of those tickets lie within a window after its own, so a grid of
+//    window + 1 resident CTAs always lets the oldest unfinished band finish.
 // Every wait is bounded: on timeout the CTA records LUMEN_ERR_TIMEOUT in
 // *status and stops; CTAs that see a non-zero status stop taking bands.
 //
