@@ -116,13 +116,14 @@ lumen_status lumen_sgbm_debug_set_paths(lumen_sgbm* h, uint32_t path_mask);
  * per direction, 2 = two fused wavefront sweeps (rows of a band in lockstep),
  * 3 = two fused wavefront sweeps with decoupled row warps and ticket-ordered
  * bands, 4 = two fused wavefront sweeps with lockstep row bands and helper
- * warps for the band hand-offs (the default).  Outputs are identical for
- * every schedule. */
+ * warps for the band hand-offs (the default), 5 = schedule 4 with consecutive
+ * bands in thread-block clusters of up to 8 CTAs that hand rows over through
+ * distributed shared memory.  Outputs are identical for every schedule. */
 lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule);
 /* Pin the fused-sweep configuration: lanes per pixel (8, 16 or 32) and warps
  * per thread block (2, 4, 8 or 16; rows per band = warps * 32 / lanes).
  * Schedules 3 and 4 use 32 lanes and take `warps` as their rows per band
- * (schedule 3: 4 or 8; schedule 4: 4, 8 or 16).  0, 0 restores the automatic
+ * (schedule 3: 4 or 8; schedules 4 and 5: 4, 8 or 16).  0, 0 restores the automatic
  * choice.  Values are identical for every setting. */
 lumen_status lumen_sgbm_set_tuning(lumen_sgbm* h, int lanes_per_pixel, int warps_per_block);
 /* The schedule and configuration the last compute used: {schedule, lanes, warps}. */

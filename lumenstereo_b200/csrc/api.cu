@@ -281,8 +281,8 @@ extern "C" lumen_status lumen_sgbm_debug_set_paths(lumen_sgbm* h, uint32_t mask)
 
 extern "C" lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule) {
     if (!h) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL handle");
-    if (schedule < 0 || schedule > 4)
-        return fail(LUMEN_ERR_INVALID_ARGUMENT, "schedule must be 0, 1, 2, 3 or 4");
+    if (schedule < 0 || schedule > 5)
+        return fail(LUMEN_ERR_INVALID_ARGUMENT, "schedule must be 0, 1, 2, 3, 4 or 5");
     h->schedule = schedule;
     return LUMEN_OK;
 }
@@ -458,6 +458,19 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
     if (sched == 0) sched = sweepable ? 4 : 1;
     if (sched >= 2 && !sweepable) sched = 1;          // single-path debug masks: per-direction kernels
     WavePlan plan4{};
+    if (sched == 5) {
+        // row bands in thread-block clusters: the largest cluster that plans
+        const int R = (cfg.T == 32 && (cfg.NW == 4 || cfg.NW == 8 || cfg.NW == 16)) ? cfg.NW : 8;
+        bool planned = false;
+        for (int cl : {8, 4, 2}) {
+            if (wave_plan(k, R, wrap, mask == 0xFFu, h->numSMs, &plan4, cl) == cudaSuccess) {
+                planned = true;
+                break;
+            }
+        }
+        if (planned) cfg = SweepConfig{32, plan4.R};
+        else sched = 4;
+    }
     if (sched == 4) {
         const int R = (cfg.T == 32 && (cfg.NW == 4 || cfg.NW == 8 || cfg.NW == 16)) ? cfg.NW : 8;
         if (wave_plan(k, R, wrap, mask == 0xFFu, h->numSMs, &plan4) == cudaSuccess ||
@@ -481,7 +494,7 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
     }
     if (sched == 2 && !sweep_fits(W, Dp, cfg)) sched = 1;  // very wide images: per-direction kernels
     const uint16_t* aggB = nullptr;
-    if (sched == 4) {
+    if (sched == 4 || sched == 5) {
         LCU(h->partB.ensure(ND * 2));
         LCU(h->xring.ensure(plan4.ringBytes));
         LCU(h->counters.ensure(sizeof(unsigned) * plan4.counterWords));
@@ -650,6 +663,7 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
         for (int i = 0; i < nr; ++i) cands.push_back({3, SweepConfig{32, rs[i]}});
         const int nw = wave_rows_options(Dp, rs, 4);
         for (int i = 0; i < nw; ++i) cands.push_back({4, SweepConfig{32, rs[i]}});
+        for (int i = 0; i < nw; ++i) cands.push_back({5, SweepConfig{32, rs[i]}});
     }
     const SweepConfig savedForced = h->forced;
     const int savedSched = h->schedule;

@@ -65,6 +65,8 @@ struct Sweep2Plan {
     int M;                 // exchange rows per sweep
     int grid;              // CTAs launched (persistent, ticket-scheduled)
     int smem;              // dynamic shared memory per CTA
+    int CL = 1;            // CTAs per thread-block cluster (1: none)
+    int nTickets = 0;      // tickets of a single-pair launch
     size_t ringBytes;      // exchange rows, both sweeps
     size_t counterWords;   // prod + cons + ticket
 };
@@ -82,11 +84,16 @@ struct WavePlan {
     int nBands;            // bands per sweep
     int grid;              // CTAs launched (persistent, ticket-scheduled)
     int smem;              // dynamic shared memory per CTA
+    int CL = 1;            // CTAs per thread-block cluster (1: none)
+    int nTickets = 0;      // tickets of a single-pair launch
     size_t ringBytes;      // exchange rings, both sweeps
     size_t counterWords;   // prod + cons + ticket
 };
 int wave_rows_options(int Dp, int* out, int max);
-cudaError_t wave_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSMs, WavePlan* plan);
+// CL > 1: consecutive bands of a sweep run in thread-block clusters of CL CTAs
+// (hand-offs inside a cluster through distributed shared memory).
+cudaError_t wave_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSMs, WavePlan* plan,
+                      int CL = 1);
 // Batched form: one launch over the bands of several pairs of one kernel
 // class (padded disparity count, path set, arithmetic mode).  d_jobs / d_table
 // live in device memory (see wave_kernel.cuh for their layout).

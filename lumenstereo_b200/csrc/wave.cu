@@ -47,7 +47,7 @@ int wave_rows_options(int Dp, int* out, int max) {
 // Shared-memory fit (largest helper rings) and occupancy of one kernel class
 // at a widest image Wmax.
 static cudaError_t plan_class(int Wmax, int Dp, int R, bool wrap, bool full, bool diag, int numSMs,
-                              WavePlan* plan) {
+                              WavePlan* plan, int CL = 1) {
     if (R != 4 && R != 8 && R != 16) return cudaErrorInvalidValue;
     const int NP = diag ? 3 : 1;
     int dev = 0, maxSmem = 0;
@@ -67,6 +67,7 @@ static cudaError_t plan_class(int Wmax, int Dp, int R, bool wrap, bool full, boo
     a.Dp = Dp;
     a.Wmax = Wmax;
     a.QI = a.QX = Q;
+    a.CL = CL;
     int perSM = 0;
     cudaError_t e = dispatch_wave(a, R, NP, wrap, full, L.total, 0, nullptr, &perSM);
     if (e != cudaSuccess) return e;
@@ -74,7 +75,9 @@ static cudaError_t plan_class(int Wmax, int Dp, int R, bool wrap, bool full, boo
     plan->R = R;
     plan->Q = Q;
     plan->smem = L.total;
-    plan->grid = perSM * numSMs;  // capacity; callers clamp to their ticket count
+    plan->CL = CL;
+    // capacity; callers clamp to their ticket count
+    plan->grid = CL > 1 ? perSM * CL : perSM * numSMs;
     return cudaSuccess;
 }
 
@@ -82,14 +85,22 @@ size_t wave_ring_bytes(int nBands, int Dp, bool diag) {
     return 2 * (size_t)nBands * kWK * (size_t)wave_slot_bytes(Dp, diag ? 3 : 1);
 }
 
-cudaError_t wave_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSMs, WavePlan* plan) {
-    cudaError_t e = plan_class(k.W, k.Dp, R, wrap, k.D == k.Dp, diag, numSMs, plan);
+cudaError_t wave_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSMs, WavePlan* plan,
+                      int CL) {
+    if (CL != 1 && CL != 2 && CL != 4 && CL != 8) return cudaErrorInvalidValue;
+    cudaError_t e = plan_class(k.W, k.Dp, R, wrap, k.D == k.Dp, diag, numSMs, plan, CL);
     if (e != cudaSuccess) return e;
     plan->nBands = (k.H + R - 1) / R;
-    plan->grid = std::min(2 * plan->nBands, plan->grid);
-    // tickets alternate the two sweeps band by band
-    if (plan->grid < std::min(2 * plan->nBands, 2 * wave_lookahead_bands(k.W) + 1))
-        return cudaErrorInvalidConfiguration;
+    // tickets alternate the two sweeps; with clusters a ticket holds CL
+    // consecutive bands.  The oldest unfinished ticket needs the tickets
+    // holding the next wave_lookahead_bands(W) bands of its sweep running.
+    const int perTicket = CL;
+    const int groups = (plan->nBands + perTicket - 1) / perTicket;
+    plan->nTickets = 2 * groups;
+    const int window = 2 * ((wave_lookahead_bands(k.W) + perTicket - 1) / perTicket + 1);
+    const int capTickets = plan->grid / CL;  // resident CTAs (clusters) that take tickets
+    if (capTickets < std::min(plan->nTickets, window + 1)) return cudaErrorInvalidConfiguration;
+    plan->grid = std::min(plan->nTickets, capTickets) * CL;
     plan->ringBytes = wave_ring_bytes(plan->nBands, k.Dp, diag);
     plan->counterWords = 4 * (size_t)plan->nBands + 32;
     return cudaSuccess;
@@ -120,7 +131,8 @@ cudaError_t launch_aggregate_wave(const PairView& pv, uint16_t* partB, const Sgm
     a.job = wave_job(pv, partB, k, plan.R, xring, counters);
     a.jobs = nullptr;
     a.table = nullptr;
-    a.nTickets = 2 * plan.nBands;
+    a.nTickets = plan.nTickets;
+    a.CL = plan.CL;
     a.Wmax = k.W;
     a.ticket = counters + 4 * plan.nBands;
     a.status = status;

@@ -206,12 +206,58 @@ def test_parity_schedule4_wide_image(oracle_mod):
         assert_subpix_close(disp, ref_disp)
 
 
-@pytest.mark.parametrize("schedule", [3, 4])
+@pytest.mark.parametrize("size", [(131, 53), (97, 150)])
+@pytest.mark.parametrize("rows", [4, 8, 16])
+@pytest.mark.parametrize("D", [40, 128, 150, 290, 512])
+def test_parity_schedule5_clusters(D, rows, size, oracle_mod):
+    """Row bands in thread-block clusters (schedule 5): hand-offs inside a
+    cluster through distributed shared memory, between clusters through the
+    global rings; tickets whose last cluster ranks have no band (partial
+    clusters) included.  Bit for bit equal to the oracle."""
+    w, h = size
+    left, right, _ = synth.make_pair(synth.PairSpec(w, h, 4, 1, min(D - 1, 40), 2.0, 180 + D))
+    for mode, nd in ((0, 8), (1, 4)):
+        pd = params_dict(maxDisparity=D, numDirections=nd, matchingCostMode=mode,
+                         speckleWindowSize=0)
+        with StereoSGBM(to_params(pd)) as s:
+            s.set_schedule(5)
+            s.set_tuning(32, rows)
+            s.retain_intermediates(True)
+            disp = s.compute(left, right)
+            agg = s.intermediate("agg", (h, w, D), np.uint16)
+            used = s.get_tuning()
+        # clusters whenever the band height fits at all (D = 512 with 16 rows
+        # per band leaves no room for them, and falls back)
+        assert used[0] == 5 or used[2] != rows, used
+        ref_disp, ref = oracle_mod.sgbm(pd, left, right, intermediates=True)
+        assert np.array_equal(agg, ref["agg"]), (mode, nd)
+        assert_subpix_close(disp, ref_disp)
+
+
+def test_parity_schedule5_wide_image(oracle_mod):
+    """Rows longer than the global exchange ring, several clusters per sweep."""
+    left, right, _ = synth.make_pair(synth.PairSpec(700, 100, 4, 1, 30, 2.0, 98))
+    for nd in (4, 8):
+        pd = params_dict(maxDisparity=48, numDirections=nd, speckleWindowSize=0)
+        with StereoSGBM(to_params(pd)) as s:
+            s.set_schedule(5)
+            s.set_tuning(32, 4)
+            s.retain_intermediates(True)
+            disp = s.compute(left, right)
+            agg = s.intermediate("agg", (100, 700, 48), np.uint16)
+        ref_disp, ref = oracle_mod.sgbm(pd, left, right, intermediates=True)
+        assert np.array_equal(agg, ref["agg"]), nd
+        assert_subpix_close(disp, ref_disp)
+
+
+@pytest.mark.parametrize("schedule", [3, 4, 5])
 def test_fused_sweep_timeout_reports_error(schedule):
     """A device-side wait that runs out ends the launch with a timeout status,
-    not a hang: one wait of the second band is made unsatisfiable and the wait
-    limit is cut, so the launch gives up quickly; the handle then recovers."""
-    left, right = synth.random_pair(300, 64, seed=3)
+    not a hang: one wait of a band that imports through the global ring is
+    made unsatisfiable and the wait limit is cut, so the launch gives up
+    quickly; the handle then recovers.  (With clusters the stalled band is the
+    first of the second cluster: the image is tall enough for it.)"""
+    left, right = synth.random_pair(300, 64 if schedule < 5 else 200, seed=3)
     p = StereoParams(maxDisparity=64, numDirections=8, speckleWindowSize=0)
     with StereoSGBM(p) as s:
         s.set_schedule(schedule)
@@ -338,14 +384,14 @@ def test_schedules_agree_full_size(wl):
                      matchingCostMode=MatchingCostMode.Census if w.census else MatchingCostMode.SAD,
                      speckleWindowSize=0)
     outs = []
-    for schedule in (1, 2, 3, 4):
+    for schedule in (1, 2, 3, 4, 5):
         with StereoSGBM(p) as s:
             s.set_schedule(schedule)
             s.retain_intermediates(True)
             d = s.compute(left, right)
             agg = s.intermediate("agg", left.shape + (w.max_disparity,), np.uint16)
             outs.append((d, agg))
-    for k in (1, 2, 3):
+    for k in (1, 2, 3, 4):
         assert np.array_equal(outs[0][1], outs[k][1]), k
         assert np.array_equal(outs[0][0], outs[k][0]), k
 
