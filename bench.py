@@ -575,7 +575,7 @@ def run_serve(args):
     for item in pool:
         plain_one(item)
     plain_rate = len(pool) / (time.perf_counter() - t0)
-    srv = StereoServer(budget_bytes=40 << 30, max_batch_pairs=32, rows_per_band=8, max_inflight=2)
+    srv = StereoServer(budget_bytes=40 << 30, max_batch_pairs=32, rows_per_band=16, max_inflight=2)
     for key, (w, h, m) in maps.items():
         srv.set_calibration(key, w, h, *m)
     # warm-up pass, and the bit-exact check of every pool pair
@@ -629,7 +629,8 @@ def run_serve(args):
            "config": {"workload": f"served_stream_pool_{len(pool)}_pairs", "seeds": f"10000..{9999 + len(pool)}",
                       "calibrations": "16 ids (seed % 16), rectified on the device from resident maps",
                       "arrivals": "Poisson", "requests_per_rate": args.requests,
-                      "budget_bytes": 40 << 30, "max_batch_pairs": 32, "max_inflight": 2},
+                      "budget_bytes": 40 << 30, "max_batch_pairs": 32, "max_inflight": 2,
+                      "rows_per_band": 16},
            "p50_ms": best["p50_ms"], "p99_ms": best["p99_ms"], "p999_ms": best["p999_ms"],
            "rates": sweep,
            "plain_serial": {"value": plain_rate, "unit": "pairs/s",

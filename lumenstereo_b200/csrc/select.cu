@@ -247,8 +247,9 @@ cudaError_t launch_select(const uint16_t* agg, const uint16_t* aggB, bool wrap, 
     case 1: return launch_select_slide<8, 4>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
     case 2: return launch_select_slide<8, 8>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
     case 3: return launch_select_slide<8, 12>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 4: return launch_select_slide<8, 16>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 5: return launch_select_slide<8, 20>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    // wider pixels spread over 16 lanes: 16-20 words per lane cost occupancy
+    case 4: return launch_select_slide<16, 8>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 5: return launch_select_slide<16, 10>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
     case 6: return launch_select_slide<16, 12>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
     case 7: return launch_select_slide<16, 14>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
     case 8: return launch_select_slide<16, 16>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
