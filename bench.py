@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--rows", type=int, default=0,
                     help="rows per band of the fused sweeps with --schedule 3/4 (0 = default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve"],
+    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve", "epilogue"],
                     help="plain: one pair per call (default); batch: the 64-pair mixed stream; "
                          "serve: Poisson request stream through the served form")
     ap.add_argument("--pairs", type=int, default=0,
@@ -647,6 +647,55 @@ def run_serve(args):
     sgbm.close()
 
 
+# ---------------------------------------------------------------------------
+# Either side of the disparity map: disparity -> depth at 1920x1080 and the
+# device-generated rectification maps at 2880x1988, against the HBM roofline
+# (depth: 2 B read + 4 B written per pixel; maps: 8 B written per pixel).
+# ---------------------------------------------------------------------------
+def run_epilogue(args):
+    import torch
+    from lumenstereo_b200 import disparity_to_depth_device, rectify_maps_device
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    peak, kind = measured_peaks()
+    stream = torch.cuda.current_stream()
+    res = {"metric": "GB/s of the depth and map-generation kernels", "unit": "GB/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "data": "synthetic",
+           "dtype": "f32", "vs_baseline": None, "peak_gbs": peak, "peak_kind": kind}
+
+    def timed(fn):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / args.steps
+
+    W, H = 1920, 1080
+    disp = torch.randint(-16, 128 * 16, (H, W), dtype=torch.int16, device="cuda")
+    depth = torch.empty((H, W), dtype=torch.float32, device="cuda")
+    ms = timed(lambda: disparity_to_depth_device(disp.data_ptr(), W, H, 1400.0, 0.12, depth.data_ptr(),
+                                                 0.0, stream.cuda_stream))
+    res["depth"] = {"workload": f"{W}x{H}", "ms": ms, "gbs": W * H * 6 / ms / 1e6,
+                    "frac": W * H * 6 / ms / 1e6 / peak}
+    W, H = 2880, 1988
+    K = np.array([[1500.0, 0, 1440], [0, 1500.0, 994], [0, 0, 1]])
+    R = np.eye(3)
+    P = np.hstack([K, np.zeros((3, 1))])
+    mx = torch.empty((H, W), dtype=torch.float32, device="cuda")
+    my = torch.empty((H, W), dtype=torch.float32, device="cuda")
+    ms = timed(lambda: rectify_maps_device(K, [0.05, -0.01, 1e-4, -1e-4, 0.0], R, P, W, H, mx.data_ptr(),
+                                           my.data_ptr(), stream.cuda_stream))
+    res["maps"] = {"workload": f"{W}x{H}", "ms": ms, "gbs": W * H * 8 / ms / 1e6,
+                   "frac": W * H * 8 / ms / 1e6 / peak}
+    res["value"] = res["depth"]["gbs"]
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -655,6 +704,8 @@ def main():
         run_batch(args)
     elif args.mode == "serve":
         run_serve(args)
+    elif args.mode == "epilogue":
+        run_epilogue(args)
     else:
         run_ours(args)
 

@@ -195,6 +195,23 @@ lumen_status lumen_remap(const uint8_t* src, const float* map_x, const float* ma
 lumen_status lumen_bgr_to_gray(const uint8_t* bgr, size_t stride, uint8_t* gray, int width,
                                int height);
 
+/* ---- either side of the disparity map ---- */
+/* disparityToDepthGPU (src/depth_map.cu:74-102, 169-187): depth = f * B /
+ * (d / 16 + doffs) in the caller's units of B for positive 1/16-px
+ * disparities, 0 elsewhere.  Device buffers (strides in bytes, 0 = packed),
+ * asynchronous on `stream`. */
+lumen_status lumen_disparity_to_depth_device(const int16_t* d_disp, int width, int height,
+                                             size_t disp_stride, float focal_px, float baseline,
+                                             float disparity_offset_px, float* d_depth,
+                                             size_t depth_stride, void* stream);
+/* The CV_32FC1 maps cv::initUndistortRectifyMap produces for one camera
+ * (src/calibration.cpp:253-266), generated on the device: K row-major 3x3,
+ * dist = (k1, k2, p1, p2, k3) or NULL, R the rectifying rotation (3x3), P the
+ * new projection (3x4, row-major).  Device maps of width*height floats. */
+lumen_status lumen_rectify_maps_device(const double K[9], const double dist[5], const double R[9],
+                                       const double P[12], int width, int height, float* d_map_x,
+                                       float* d_map_y, void* stream);
+
 /* ---- batched form (no counterpart in the reference's API; LumenStereo's
  * callers loop over StereoSGBM::compute, e.g. tools/evaluate.cpp:158-160) ----
  *

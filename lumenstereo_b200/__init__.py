@@ -25,7 +25,8 @@ from . import _lib
 
 __all__ = ["MatchingCostMode", "StereoParams", "StereoSGBM", "StereoBatch", "StereoServer", "StereoRectifier",
            "StereoException", "CudaException", "kSgbmMaxDisparityRange",
-           "middleburyMatcherMaxDisparity", "rectify_image_gpu", "bgr_to_gray"]
+           "middleburyMatcherMaxDisparity", "rectify_image_gpu", "bgr_to_gray",
+           "disparity_to_depth_device", "rectify_maps_device"]
 
 # include/stereo/sgbm_limits.h:9
 kSgbmMaxDisparityRange = 512
@@ -512,3 +513,25 @@ def bgr_to_gray(bgr: np.ndarray) -> np.ndarray:
     g = np.empty((h, w), np.uint8)
     _check(_lib.lib().lumen_bgr_to_gray(b.ctypes.data, b.strides[0], g.ctypes.data, w, h))
     return g
+
+
+def disparity_to_depth_device(disp_ptr: int, width: int, height: int, focal_px: float, baseline: float,
+                              depth_ptr: int, disparity_offset_px: float = 0.0, stream: int = 0) -> None:
+    """disparityToDepthGPU (include/stereo/depth_map.h): packed device int16
+    disparity (1/16 px) -> packed device float32 depth, f * B / (d/16 + doffs)."""
+    _check(_lib.lib().lumen_disparity_to_depth_device(disp_ptr, width, height, 0, focal_px, baseline,
+                                                      disparity_offset_px, depth_ptr, 0, stream))
+
+
+def rectify_maps_device(K, dist, R, P, width: int, height: int, map_x_ptr: int, map_y_ptr: int,
+                        stream: int = 0) -> None:
+    """cv::initUndistortRectifyMap (CV_32FC1) for one camera, on the device."""
+    k = np.ascontiguousarray(K, dtype=np.float64).reshape(9)
+    r = np.ascontiguousarray(R, dtype=np.float64).reshape(9)
+    p = np.ascontiguousarray(P, dtype=np.float64).reshape(12)
+    d = None if dist is None else np.ascontiguousarray(np.asarray(dist, np.float64).ravel()[:5])
+    if d is not None and d.size < 5:
+        d = np.concatenate([d, np.zeros(5 - d.size)])
+    _check(_lib.lib().lumen_rectify_maps_device(k.ctypes.data, None if d is None else d.ctypes.data,
+                                                r.ctypes.data, p.ctypes.data, width, height,
+                                                map_x_ptr, map_y_ptr, stream))

@@ -103,6 +103,8 @@ def _declare(lib):
         "lumen_server_submit": (i, [vp, C.POINTER(CParams), i, vp, vp, i, i, vp, C.POINTER(C.c_ulonglong)]),
         "lumen_server_wait": (i, [vp, C.c_ulonglong, i, C.POINTER(CRequestInfo)]),
         "lumen_server_get_stats": (i, [vp, C.POINTER(CServerStats)]),
+        "lumen_disparity_to_depth_device": (i, [vp, i, i, sz, C.c_float, C.c_float, C.c_float, vp, sz, vp]),
+        "lumen_rectify_maps_device": (i, [vp, vp, vp, vp, i, i, vp, vp, vp]),
         "lumen_census_cost_noalloc": (i, [vp, vp, i, i, i, i, vp, i, vp]),
         "lumen_census_cost_noalloc_max_pixels": (sz, []),
     }

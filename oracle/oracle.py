@@ -204,3 +204,37 @@ def ref_remap(src: np.ndarray, mapx: np.ndarray, mapy: np.ndarray) -> np.ndarray
     if rc != 0:
         raise RuntimeError(f"ref_remap_run failed ({rc})")
     return dst
+
+
+def disparity_to_depth(disp: np.ndarray, focal: float, baseline: float, doffs: float = 0.0) -> np.ndarray:
+    """disparityToDepthKernel (src/depth_map.cu:74-102) in IEEE float32:
+    f * B / (d / 16 + doffs) for d > 0 and a positive denominator, else 0."""
+    d = disp.astype(np.float32) / np.float32(16.0)
+    denom = d + np.float32(doffs)
+    fb = np.float32(focal) * np.float32(baseline)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        z = fb / denom
+    return np.where((disp > 0) & (denom > 0), z, np.float32(0.0)).astype(np.float32)
+
+
+def rectify_maps(K, dist, R, P, width: int, height: int):
+    """The maps of cv::initUndistortRectifyMap (CV_32FC1), restated in float64
+    numpy from the published pinhole + Brown-Conrady model: the ray
+    (P[:, :3] R)^-1 (u, v, 1), projected, distorted by (k1, k2, p1, p2, k3) and
+    mapped through K."""
+    K = np.asarray(K, np.float64).reshape(3, 3)
+    R = np.asarray(R, np.float64).reshape(3, 3)
+    P = np.asarray(P, np.float64).reshape(3, 4)
+    k = np.zeros(5) if dist is None else np.concatenate([np.asarray(dist, np.float64).ravel(), np.zeros(5)])[:5]
+    iR = np.linalg.inv(P[:, :3] @ R)
+    u, v = np.meshgrid(np.arange(width, dtype=np.float64), np.arange(height, dtype=np.float64))
+    X = iR[0, 0] * u + iR[0, 1] * v + iR[0, 2]
+    Y = iR[1, 0] * u + iR[1, 1] * v + iR[1, 2]
+    Z = iR[2, 0] * u + iR[2, 1] * v + iR[2, 2]
+    x, y = X / Z, Y / Z
+    x2, y2 = x * x, y * y
+    r2, xy2 = x2 + y2, 2 * x * y
+    s = 1 + ((k[4] * r2 + k[1]) * r2 + k[0]) * r2
+    xd = x * s + k[2] * xy2 + k[3] * (r2 + 2 * x2)
+    yd = y * s + k[2] * (r2 + 2 * y2) + k[3] * xy2
+    return ((K[0, 0] * xd + K[0, 2]).astype(np.float32), (K[1, 1] * yd + K[1, 2]).astype(np.float32))

@@ -1,0 +1,67 @@
+"""Either side of the disparity map (the next rows after the hot path):
+disparity -> depth (disparityToDepthGPU, src/depth_map.cu:74-102) and the
+rectification maps generated on the device (cv::initUndistortRectifyMap, the
+calls of src/calibration.cpp:253-266).
+
+CPU: the oracle's numpy restatement of the maps is pinned to maps OpenCV made
+(tests/golden/rectify_maps.npz, written by tests/golden/make_rectify_maps.py).
+GPU: the device maps agree with those within 2e-3 px (double on the device,
+float storage; OpenCV accumulates along the row); the device depth agrees
+with the IEEE float32 restatement within 4 ulp (the division is the
+fast-math one, like the reference's build)."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "rectify_maps.npz")
+
+
+def _cams():
+    z = np.load(GOLD)
+    w, h = int(z["width"]), int(z["height"])
+    for c in range(2):
+        for cam in (0, 1):
+            yield (w, h, z[f"c{c}_K{cam}"], z[f"c{c}_D{cam}"], z[f"c{c}_R{cam}"], z[f"c{c}_P{cam}"],
+                   z[f"c{c}_map{cam}x"], z[f"c{c}_map{cam}y"])
+
+
+def test_oracle_maps_match_opencv():
+    for w, h, K, D, R, P, mx, my in _cams():
+        ox, oy = oracle.rectify_maps(K, D, R, P, w, h)
+        assert np.abs(ox - mx).max() <= 1e-3 and np.abs(oy - my).max() <= 1e-3
+
+
+@pytest.mark.gpu
+def test_device_maps_match_opencv():
+    torch = pytest.importorskip("torch")
+    from lumenstereo_b200 import rectify_maps_device
+    for w, h, K, D, R, P, mx, my in _cams():
+        dx = torch.empty((h, w), dtype=torch.float32, device="cuda")
+        dy = torch.empty((h, w), dtype=torch.float32, device="cuda")
+        rectify_maps_device(K, D, R, P, w, h, dx.data_ptr(), dy.data_ptr())
+        torch.cuda.synchronize()
+        assert np.abs(dx.cpu().numpy() - mx).max() <= 2e-3
+        assert np.abs(dy.cpu().numpy() - my).max() <= 2e-3
+
+
+@pytest.mark.gpu
+def test_device_depth_matches_restatement():
+    torch = pytest.importorskip("torch")
+    from lumenstereo_b200 import disparity_to_depth_device
+    rng = np.random.Generator(np.random.PCG64(5))
+    disp = rng.integers(-20, 290 * 16, (123, 257)).astype(np.int16)
+    disp[0, :10] = [-1, 0, 1, 2, 16, -16, 32767, 5, 0, -32768]
+    for f, b, doffs in ((1400.0, 0.12, 0.0), (3997.684, 0.19395, 131.111), (800.0, 0.3, -3.0)):
+        dd = torch.from_numpy(disp).cuda()
+        out = torch.empty(disp.shape, dtype=torch.float32, device="cuda")
+        disparity_to_depth_device(dd.data_ptr(), disp.shape[1], disp.shape[0], f, b, out.data_ptr(), doffs)
+        torch.cuda.synchronize()
+        got = out.cpu().numpy()
+        ref = oracle.disparity_to_depth(disp, f, b, doffs)
+        assert np.array_equal(got == 0, ref == 0)
+        nz = ref != 0
+        ulp = np.abs(got[nz].view(np.int32) - ref[nz].view(np.int32))
+        assert ulp.max() <= 4, ulp.max()
