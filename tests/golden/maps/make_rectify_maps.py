@@ -1,10 +1,10 @@
-"""Generate tests/golden/rectify_maps.npz: rectification maps made by OpenCV
+"""Generate tests/golden/maps/rectify_maps.npz: rectification maps made by OpenCV
 itself (cv2.stereoRectify + cv2.initUndistortRectifyMap, CV_32FC1), the calls
 LumenStereo makes in computeRectification (src/calibration.cpp:230-266), for
 two seeded synthetic stereo calibrations at 96x72.  Stores K, D, R, P of
 both cameras and the four maps.  Run from the repository root (needs cv2):
 
-    python tests/golden/make_rectify_maps.py
+    python tests/golden/maps/make_rectify_maps.py
 """
 from __future__ import annotations
 

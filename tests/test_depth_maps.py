@@ -4,7 +4,7 @@ rectification maps generated on the device (cv::initUndistortRectifyMap, the
 calls of src/calibration.cpp:253-266).
 
 CPU: the oracle's numpy restatement of the maps is pinned to maps OpenCV made
-(tests/golden/rectify_maps.npz, written by tests/golden/make_rectify_maps.py).
+(tests/golden/maps/rectify_maps.npz, written by tests/golden/maps/make_rectify_maps.py).
 GPU: the device maps agree with those within 2e-3 px (double on the device,
 float storage; OpenCV accumulates along the row); the device depth agrees
 with the IEEE float32 restatement within 4 ulp (the division is the
@@ -16,7 +16,7 @@ import pytest
 
 from oracle import oracle
 
-GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "rectify_maps.npz")
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "maps", "rectify_maps.npz")
 
 
 def _cams():
