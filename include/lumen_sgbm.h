@@ -286,6 +286,15 @@ lumen_status lumen_server_destroy(lumen_server* s);
 lumen_status lumen_server_set_calibration(lumen_server* s, int calib_id, int width, int height,
                                           const float* map0x, const float* map0y,
                                           const float* map1x, const float* map1y);
+/* Same, from the calibration itself: the maps of both cameras are generated
+ * on the device (lumen_rectify_maps_device) from K, distortion (k1, k2, p1, p2,
+ * k3 or NULL), rectifying rotation and new projection, as
+ * src/calibration.cpp:230-266 gets them from OpenCV; no host maps. */
+lumen_status lumen_server_set_calibration_params(lumen_server* s, int calib_id, int width, int height,
+                                                 const double K0[9], const double D0[5],
+                                                 const double R0[9], const double P0[12],
+                                                 const double K1[9], const double D1[5],
+                                                 const double R1[9], const double P1[12]);
 /* Queues one gray pair (host buffers, width*height bytes each, copied before
  * the call returns); calib_id -1 = already rectified.  `out` (width*height
  * int16) is written before lumen_server_wait reports the request done and

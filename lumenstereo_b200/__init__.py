@@ -398,6 +398,19 @@ class StereoServer:
         ptrs = [None if m is None else m.ctypes.data for m in maps]
         _check(_lib.lib().lumen_server_set_calibration(self._h, calib_id, width, height, *ptrs))
 
+    def set_calibration_params(self, calib_id: int, width: int, height: int, K0, D0, R0, P0, K1, D1, R1,
+                               P1) -> None:
+        """Registers a calibration from its camera matrices; both cameras'
+        maps are generated on the device."""
+        arrs = []
+        for a, n in ((K0, 9), (D0, 5), (R0, 9), (P0, 12), (K1, 9), (D1, 5), (R1, 9), (P1, 12)):
+            v = np.zeros(n) if a is None else np.asarray(a, np.float64).ravel()
+            if v.size < n:
+                v = np.concatenate([v, np.zeros(n - v.size)])
+            arrs.append(np.ascontiguousarray(v[:n]))
+        _check(_lib.lib().lumen_server_set_calibration_params(self._h, calib_id, width, height,
+                                                              *[a.ctypes.data for a in arrs]))
+
     def submit(self, params: StereoParams, left: np.ndarray, right: np.ndarray, calib_id: int = -1,
                out: np.ndarray | None = None) -> int:
         """Queues a gray uint8 pair (copied before returning); returns its id."""

@@ -100,6 +100,7 @@ def _declare(lib):
         "lumen_server_create": (i, [C.POINTER(CServerOptions), C.POINTER(vp)]),
         "lumen_server_destroy": (i, [vp]),
         "lumen_server_set_calibration": (i, [vp, i, i, i, vp, vp, vp, vp]),
+        "lumen_server_set_calibration_params": (i, [vp, i, i, i] + [vp] * 8),
         "lumen_server_submit": (i, [vp, C.POINTER(CParams), i, vp, vp, i, i, vp, C.POINTER(C.c_ulonglong)]),
         "lumen_server_wait": (i, [vp, C.c_ulonglong, i, C.POINTER(CRequestInfo)]),
         "lumen_server_get_stats": (i, [vp, C.POINTER(CServerStats)]),

@@ -142,7 +142,8 @@ struct lumen_server {
     cudaStream_t agg = nullptr;
     std::vector<Slot> slots;
     struct Calib {
-        lumen_rectifier* rect;
+        lumen_rectifier* rect;  // maps uploaded from the host, or
+        float* maps;            // [4][H][W] maps generated on the device
         int W, H;
     };
     std::map<int, Calib> calib;
@@ -204,13 +205,20 @@ lumen_status slot_launch(lumen_server* S, Slot& sl, std::vector<Request*>& adm) 
             cudaMemcpyAsync(up + img, r->in + n, n, cudaMemcpyHostToDevice, sl.s) != cudaSuccess)
             return sfail(LUMEN_ERR_CUDA, "server: input upload failed");
         if (raw) {
-            lumen_rectifier* rect = nullptr;
+            lumen_server::Calib c{};
             {
                 std::lock_guard<std::mutex> g(S->calibMu);
-                rect = S->calib[r->calib].rect;
+                c = S->calib[r->calib];
             }
-            lumen_status rs = lumen_rectifier_rectify_device(rect, raw, raw + img, 1, dl, dr, sl.s);
-            if (rs != LUMEN_OK) return rs;
+            if (c.maps) {
+                const size_t m = (size_t)r->W * r->H;
+                launch_remap(raw, raw + img, c.maps, c.maps + m, c.maps + 2 * m, c.maps + 3 * m, dl, dr, r->W,
+                             r->H, 1, 2, sl.s);
+                if (cudaGetLastError() != cudaSuccess) return sfail(LUMEN_ERR_CUDA, "server: remap launch failed");
+            } else {
+                lumen_status rs = lumen_rectifier_rectify_device(c.rect, raw, raw + img, 1, dl, dr, sl.s);
+                if (rs != LUMEN_OK) return rs;
+            }
         }
         BatchPair q;
         lumen_status ps = batch_pair_init(q, &r->p, dl, dr, r->W, r->H, dOut);
@@ -496,7 +504,10 @@ extern "C" lumen_status lumen_server_destroy(lumen_server* S) {
         if (sl.dDesc) cudaFree(sl.dDesc);
         if (sl.hDesc) cudaFreeHost(sl.hDesc);
     }
-    for (auto& kv : S->calib) lumen_rectifier_destroy(kv.second.rect);
+    for (auto& kv : S->calib) {
+        if (kv.second.rect) lumen_rectifier_destroy(kv.second.rect);
+        if (kv.second.maps) cudaFree(kv.second.maps);
+    }
     if (S->agg) cudaStreamDestroy(S->agg);
     if (S->magic) cudaFree(S->magic);
     if (S->arenaBase) cudaFree(S->arenaBase);
@@ -519,7 +530,43 @@ extern "C" lumen_status lumen_server_set_calibration(lumen_server* S, int calib_
         lumen_rectifier_destroy(r);
         return sfail(LUMEN_ERR_INVALID_ARGUMENT, "calibration id already registered");
     }
-    S->calib[calib_id] = lumen_server::Calib{r, width, height};
+    S->calib[calib_id] = lumen_server::Calib{r, nullptr, width, height};
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_server_set_calibration_params(lumen_server* S, int calib_id, int width, int height,
+                                                            const double K0[9], const double D0[5],
+                                                            const double R0[9], const double P0[12],
+                                                            const double K1[9], const double D1[5],
+                                                            const double R1[9], const double P1[12]) {
+    if (!S) return sfail(LUMEN_ERR_INVALID_ARGUMENT, "NULL server");
+    if (calib_id < 0) return sfail(LUMEN_ERR_INVALID_ARGUMENT, "calibration ids are >= 0");
+    if (width <= 0 || height <= 0) return sfail(LUMEN_ERR_INVALID_ARGUMENT, "empty calibration image size");
+    {
+        std::lock_guard<std::mutex> g(S->calibMu);
+        if (S->calib.count(calib_id)) return sfail(LUMEN_ERR_INVALID_ARGUMENT, "calibration id already registered");
+    }
+    const size_t m = (size_t)width * height;
+    float* maps = nullptr;
+    cudaError_t e = cudaMalloc(&maps, 4 * m * sizeof(float));
+    if (e != cudaSuccess) return sfail(LUMEN_ERR_CUDA, std::string("calibration maps: ") + cudaGetErrorString(e));
+    cudaStream_t s = nullptr;
+    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    lumen_status st = e == cudaSuccess ? LUMEN_OK : sfail(LUMEN_ERR_CUDA, "calibration stream");
+    if (st == LUMEN_OK) st = lumen_rectify_maps_device(K0, D0, R0, P0, width, height, maps, maps + m, s);
+    if (st == LUMEN_OK) st = lumen_rectify_maps_device(K1, D1, R1, P1, width, height, maps + 2 * m, maps + 3 * m, s);
+    if (st == LUMEN_OK && cudaStreamSynchronize(s) != cudaSuccess) st = sfail(LUMEN_ERR_CUDA, "calibration maps");
+    if (s) cudaStreamDestroy(s);
+    if (st != LUMEN_OK) {
+        cudaFree(maps);
+        return st;
+    }
+    std::lock_guard<std::mutex> g(S->calibMu);
+    if (S->calib.count(calib_id)) {
+        cudaFree(maps);
+        return sfail(LUMEN_ERR_INVALID_ARGUMENT, "calibration id already registered");
+    }
+    S->calib[calib_id] = lumen_server::Calib{nullptr, maps, width, height};
     return LUMEN_OK;
 }
 

@@ -65,3 +65,31 @@ def test_device_depth_matches_restatement():
         nz = ref != 0
         ulp = np.abs(got[nz].view(np.int32) - ref[nz].view(np.int32))
         assert ulp.max() <= 4, ulp.max()
+
+
+@pytest.mark.gpu
+def test_served_calibration_from_params():
+    """A served calibration registered from camera matrices (maps generated on
+    the device) gives the plain path's result on the same maps."""
+    torch = pytest.importorskip("torch")
+    from lumenstereo_b200 import StereoParams, StereoRectifier, StereoServer, StereoSGBM, rectify_maps_device, synth
+    z = np.load(GOLD)
+    w, h = int(z["width"]), int(z["height"])
+    cam = {k: z[f"c0_{k}"] for k in ("K0", "D0", "R0", "P0", "K1", "D1", "R1", "P1")}
+    maps = []
+    for i in (0, 1):
+        dx = torch.empty((h, w), dtype=torch.float32, device="cuda")
+        dy = torch.empty((h, w), dtype=torch.float32, device="cuda")
+        rectify_maps_device(cam[f"K{i}"], cam[f"D{i}"], cam[f"R{i}"], cam[f"P{i}"], w, h, dx.data_ptr(), dy.data_ptr())
+        torch.cuda.synchronize()
+        maps += [dx.cpu().numpy(), dy.cpu().numpy()]
+    left, right, _ = synth.make_pair(synth.PairSpec(w, h, 4, 1, 20, 2.0, 77))
+    p = StereoParams(maxDisparity=32, numDirections=8, speckleWindowSize=0)
+    rl, rr = StereoRectifier(w, h, *maps).rectify(left, right)
+    with StereoSGBM(p) as s:
+        ref = s.compute(rl, rr)
+    with StereoServer(budget_bytes=256 << 20) as srv:
+        srv.set_calibration_params(7, w, h, cam["K0"], cam["D0"], cam["R0"], cam["P0"],
+                                   cam["K1"], cam["D1"], cam["R1"], cam["P1"])
+        out, _ = srv.wait(srv.submit(p, left, right, calib_id=7))
+    assert np.array_equal(out, ref)
