@@ -150,9 +150,10 @@ lumen_status lumen_sgbm_debug_copy(lumen_sgbm* h, int which, void* dst, size_t d
 /* Band timeline of the lockstep row-band sweeps (schedule 4) for the next
  * computes (enable = 1) or off (0).  lumen_sgbm_debug_trace_copy returns the
  * last such launch's records, 4 words per band ticket t (t = 2*band + sweep):
- * globaltimer ns when the band was taken, when its first step began, when it
- * ended, and SM id << 48 | import polls << 32 | export polls << 16 | cost
- * chunk polls.  *words receives the record size; dst may be NULL to query it. */
+ * globaltimer ns when the band's first row and its last row finished the
+ * middle pixel (u = width / 2), when the band ended, and SM id << 48 |
+ * import polls << 32 | export polls << 16 | row waits on the helpers.
+ * *words receives the record size; dst may be NULL to query it. */
 lumen_status lumen_sgbm_debug_trace(lumen_sgbm* h, int enable);
 lumen_status lumen_sgbm_debug_trace_copy(lumen_sgbm* h, unsigned long long* dst,
                                          size_t dst_words, size_t* words);

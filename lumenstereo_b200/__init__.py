@@ -281,9 +281,10 @@ class StereoSGBM:
         _check(_lib.lib().lumen_sgbm_debug_trace(self._h, int(enable)))
 
     def trace(self) -> np.ndarray:
-        """Band timeline of the last schedule-4 launch: one row per band ticket
-        (2*band + sweep): [taken_ns, first_step_ns, end_ns, sm << 48 | import
-        polls << 32 | export polls << 16 | cost-chunk polls]."""
+        """Band timeline of the last schedule-4/5 launch: one row per band
+        ticket (2*band + sweep): [first row at the middle pixel ns, last row at
+        the middle pixel ns, end ns, sm << 48 | import polls << 32 | export
+        polls << 16 | row waits]."""
         lib = _lib.lib()
         n = C.c_size_t(0)
         _check(lib.lumen_sgbm_debug_trace_copy(self._h, None, 0, C.byref(n)))

@@ -96,10 +96,12 @@ struct WaveArgs {
     unsigned long long* trace;  // optional [nTickets][4] band timeline
 };
 
-// Band timeline record (diagnostics, lumen_sgbm_debug_trace): per ticket t,
-// [0] globaltimer ns when the band was taken, [1] when its rows began,
-// [2] when it ended, [3] SM id << 48 | import polls << 32 | export polls << 16
-// | row waits on the helpers (saturating 16-bit counts).
+// Band timeline record (diagnostics, lumen_sgbm_debug_trace): per band ticket
+// 2 * band + sweep, [0] globaltimer ns when the band's first row finished the
+// middle pixel (u = W / 2), [1] when its last row did, [2] when the band
+// ended, [3] SM id << 48 | import polls << 32 | export polls << 16 | row waits
+// on the helpers (saturating 16-bit counts).  Consecutive bands' [0] give the
+// stagger, [0] of band b+1 minus [1] of band b the hand-off.
 __device__ __forceinline__ unsigned long long wave_now() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
@@ -458,8 +460,6 @@ wave_kernel(WaveArgs a) {
         }
         const int t = sflag[0];
         if (t >= a.nTickets) break;
-        unsigned long long tTaken = 0;
-        if (a.trace && threadIdx.x == 0) tTaken = wave_now();
         int sw, b;
         WaveJob J;
         if (a.jobs) {
@@ -513,8 +513,8 @@ wave_kernel(WaveArgs a) {
         const unsigned stallPix = (a.stallTest && tb == (CL > 1 ? 2 * CL : 2)) ? (unsigned)W + 1u : 0u;
         bool ok = true;
         __syncthreads();
-        unsigned long long tStart = 0;
-        if (a.trace && threadIdx.x == 0) tStart = wave_now();
+        // [24..27]: globaltimer of the middle pixel in the first and the last row
+        unsigned long long* tMid = reinterpret_cast<unsigned long long*>(sm + L.misc) + 12;
 
         if (!active) {
             // no band for this rank in this ticket
@@ -628,6 +628,10 @@ wave_kernel(WaveArgs a) {
 #pragma unroll
                     for (int pth = 0; pth < NP; ++pth) sum = WRAP ? __vadd2(sum, Ln[pth][w]) : sum + Ln[pth][w];
                     S[w] = sum;
+                }
+                if (a.trace && lane == 0 && on && u == (W >> 1)) {
+                    if (r == 0) tMid[0] = wave_now();
+                    if (r == lastActive) tMid[1] = wave_now();
                 }
                 if (on && ok) {
                     store_words<KW>(pout, S);
@@ -750,8 +754,8 @@ wave_kernel(WaveArgs a) {
             unsigned smid;
             asm volatile("mov.u32 %0, %%smid;\n" : "=r"(smid));
             unsigned long long* rec = a.trace + 4 * (size_t)tb;
-            rec[0] = tTaken;
-            rec[1] = tStart;
+            rec[0] = tMid[0];
+            rec[1] = tMid[1];
             rec[2] = wave_now();
             auto sat = [](int x) { return (unsigned long long)min(x, 0xFFFF); };
             rec[3] = ((unsigned long long)smid << 48) | (sat(sflag[2]) << 32) | (sat(sflag[3]) << 16) |
