@@ -463,23 +463,12 @@ def run_batch(args):
     plain_loop()
     torch.cuda.synchronize()
     plain_ms = timed(plain_loop, max(1, args.steps // 2))
-    # autotuned batch: rows per band, then graph replay
-    tune = {}
-    best_rows, best_ms = 8, None
-    for rows in (4, 8, 16):
-        with StereoBatch(rows_per_band=rows) as b:
-            for (p, dl, dr, w, h), o in zip(pairs, out):
-                b.add(p, dl.data_ptr(), dr.data_ptr(), w, h, o.data_ptr())
-            b.run(sptr)
-            b.sync(sptr)
-            ms = min(timed(lambda: b.run(sptr), 2))
-            b.sync(sptr)
-        tune[rows] = ms
-        if best_ms is None or ms < best_ms:
-            best_rows, best_ms = rows, ms
-    batch = StereoBatch(rows_per_band=best_rows, use_graph=True)
+    # the library's batch autotuner (rows per band), then graph replay
+    batch = StereoBatch(use_graph=True)
     for (p, dl, dr, w, h), o in zip(pairs, out):
         batch.add(p, dl.data_ptr(), dr.data_ptr(), w, h, o.data_ptr())
+    best_rows, best_ms = batch.autotune(sptr, repeats=2)
+    tune = {"rows_per_band": best_rows, "ms": best_ms}
     for _ in range(max(args.warmup, 2)):
         batch.run(sptr)
     batch.sync(sptr)

@@ -241,6 +241,11 @@ lumen_status lumen_sgbm_batch_clear(lumen_sgbm_batch* b);
 lumen_status lumen_sgbm_batch_set_options(lumen_sgbm_batch* b, int rows_per_band, int use_graph,
                                           size_t device_budget_bytes);
 lumen_status lumen_sgbm_batch_run(lumen_sgbm_batch* b, void* stream);
+/* Autotuner of the batched launch (no counterpart in the reference): runs the
+ * batch with 4, 8 and 16 rows per band (`repeats` timed runs each, on
+ * `stream`, writing the outputs) and keeps the fastest for later runs. */
+lumen_status lumen_sgbm_batch_autotune(lumen_sgbm_batch* b, void* stream, int repeats, int* best_rows,
+                                       float* best_ms);
 lumen_status lumen_sgbm_batch_sync(lumen_sgbm_batch* b, void* stream);
 /* Pooled device bytes, number of launch groups, kernels per run. */
 lumen_status lumen_sgbm_batch_info(const lumen_sgbm_batch* b, size_t* device_bytes, int* groups,

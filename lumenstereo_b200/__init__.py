@@ -342,6 +342,13 @@ class StereoBatch:
     def sync(self, stream: int = 0) -> None:
         _check(_lib.lib().lumen_sgbm_batch_sync(self._h, stream))
 
+    def autotune(self, stream: int = 0, repeats: int = 2):
+        """Times the batch at 4, 8 and 16 rows per band and keeps the fastest:
+        (rows, ms per run)."""
+        r, ms = C.c_int(0), C.c_float(0)
+        _check(_lib.lib().lumen_sgbm_batch_autotune(self._h, stream, repeats, C.byref(r), C.byref(ms)))
+        return r.value, ms.value
+
     def info(self):
         nb, ng, nl = C.c_size_t(0), C.c_int(0), C.c_ulonglong(0)
         _check(_lib.lib().lumen_sgbm_batch_info(self._h, C.byref(nb), C.byref(ng), C.byref(nl)))

@@ -95,6 +95,7 @@ def _declare(lib):
         "lumen_sgbm_batch_set_options": (i, [vp, i, i, sz]),
         "lumen_sgbm_batch_run": (i, [vp, vp]),
         "lumen_sgbm_batch_sync": (i, [vp, vp]),
+        "lumen_sgbm_batch_autotune": (i, [vp, vp, i, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
         "lumen_sgbm_batch_info": (i, [vp, C.POINTER(sz), C.POINTER(C.c_int), C.POINTER(C.c_ulonglong)]),
         "lumen_server_options_default": (None, [C.POINTER(CServerOptions)]),
         "lumen_server_create": (i, [C.POINTER(CServerOptions), C.POINTER(vp)]),

@@ -592,6 +592,56 @@ extern "C" lumen_status lumen_sgbm_batch_sync(lumen_sgbm_batch* b, void* stream)
     return LUMEN_OK;
 }
 
+extern "C" lumen_status lumen_sgbm_batch_autotune(lumen_sgbm_batch* b, void* stream, int repeats,
+                                                  int* best_rows, float* best_ms) {
+    if (!b) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "NULL batch");
+    if (b->pairs.empty()) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "empty batch");
+    if (repeats < 1) repeats = 1;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    BCU(cudaEventCreate(&e0));
+    cudaError_t ce = cudaEventCreate(&e1);
+    if (ce != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return bfail(LUMEN_ERR_CUDA, "batch autotune: event creation failed");
+    }
+    const int savedGraph = b->useGraph;
+    int bestR = 0;
+    float bestMs = 0.f;
+    lumen_status st = LUMEN_OK;
+    for (int R : {4, 8, 16}) {
+        cudaStreamSynchronize(s);
+        batch_release(b);
+        b->rows = R;
+        b->useGraph = 0;
+        st = lumen_sgbm_batch_run(b, stream);  // plans, warms up
+        if (st == LUMEN_OK) st = lumen_sgbm_batch_sync(b, stream);
+        if (st != LUMEN_OK) break;
+        cudaEventRecord(e0, s);
+        for (int i = 0; i < repeats && st == LUMEN_OK; ++i) st = lumen_sgbm_batch_run(b, stream);
+        cudaEventRecord(e1, s);
+        if (st == LUMEN_OK) st = lumen_sgbm_batch_sync(b, stream);
+        if (st != LUMEN_OK) break;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= (float)repeats;
+        if (!bestR || ms < bestMs) {
+            bestR = R;
+            bestMs = ms;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamSynchronize(s);
+    batch_release(b);
+    b->useGraph = savedGraph;
+    if (st != LUMEN_OK) return st;
+    b->rows = bestR;  // the next run plans (and captures) with it
+    if (best_rows) *best_rows = bestR;
+    if (best_ms) *best_ms = bestMs;
+    return LUMEN_OK;
+}
+
 extern "C" lumen_status lumen_sgbm_batch_info(const lumen_sgbm_batch* b, size_t* device_bytes,
                                               int* groups, unsigned long long* launches) {
     if (!b) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "NULL batch");

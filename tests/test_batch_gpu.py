@@ -87,3 +87,23 @@ def test_batch_many_wide_pairs(rows):
         for i, (o, ref) in enumerate(zip(outs, refs)):
             assert np.array_equal(o.cpu().numpy(), ref), i
         assert b.info()["groups"] == 1
+
+
+
+def test_batch_autotune_keeps_outputs():
+    """The batch autotuner picks a band height and the outputs stay exact."""
+    torch = pytest.importorskip("torch")
+    pairs = _pairs(torch)
+    refs = _plain(torch, pairs)
+    outs = [torch.zeros((h, w), dtype=torch.int16, device="cuda") for _, _, _, w, h in pairs]
+    with StereoBatch(use_graph=True) as b:
+        for (p, dl, dr, w, h), o in zip(pairs, outs):
+            b.add(p, dl.data_ptr(), dr.data_ptr(), w, h, o.data_ptr())
+        rows, ms = b.autotune()
+        assert rows in (4, 8, 16) and ms > 0
+        for o in outs:
+            o.fill_(0)
+        b.run()
+        b.sync()
+    for o, ref in zip(outs, refs):
+        assert np.array_equal(o.cpu().numpy(), ref)
