@@ -65,8 +65,6 @@ struct Sweep2Plan {
     int M;                 // exchange rows per sweep
     int grid;              // CTAs launched (persistent, ticket-scheduled)
     int smem;              // dynamic shared memory per CTA
-    int CL = 1;            // CTAs per thread-block cluster (1: none)
-    int nTickets = 0;      // tickets of a single-pair launch
     size_t ringBytes;      // exchange rows, both sweeps
     size_t counterWords;   // prod + cons + ticket
 };
@@ -85,6 +83,7 @@ struct WavePlan {
     int grid;              // CTAs launched (persistent, ticket-scheduled)
     int smem;              // dynamic shared memory per CTA
     int CL = 1;            // CTAs per thread-block cluster (1: none)
+    int T = 32;            // lanes per row (batched launches: 8 or 16)
     int nTickets = 0;      // tickets of a single-pair launch
     size_t ringBytes;      // exchange rings, both sweeps
     size_t counterWords;   // prod + cons + ticket

@@ -19,9 +19,30 @@ LUMEN_WAVE_DECL(5)
 LUMEN_WAVE_DECL(6)
 LUMEN_WAVE_DECL(7)
 LUMEN_WAVE_DECL(8)
+#define LUMEN_WAVE_TEAM_DECL(KP)                                                               \
+    cudaError_t wave_dispatch_team_##KP(const WaveArgs& a, int R, int NP, bool wrap, bool full, \
+                                        int smem, int grid, cudaStream_t s, int* perSM);
+LUMEN_WAVE_TEAM_DECL(1)
+LUMEN_WAVE_TEAM_DECL(2)
+LUMEN_WAVE_TEAM_DECL(3)
+LUMEN_WAVE_TEAM_DECL(4)
+
+// lanes per row of the batched launches: the narrowest team that fits the
+// padded disparities in a lane's registers
+int wave_team_lanes(int Dp) { return Dp <= 128 ? 8 : Dp <= 256 ? 16 : 32; }
 
 static cudaError_t dispatch_wave(const WaveArgs& a, int R, int NP, bool wrap, bool full, int smem,
-                                 int grid, cudaStream_t s, int* perSM) {
+                                 int grid, cudaStream_t s, int* perSM, int T = 32) {
+    if (T != 32) {
+        if (T != wave_team_lanes(a.Dp) || (R != 8 && R != 16)) return cudaErrorInvalidValue;
+        switch (a.Dp / 64) {
+        case 1: return wave_dispatch_team_1(a, R, NP, wrap, full, smem, grid, s, perSM);
+        case 2: return wave_dispatch_team_2(a, R, NP, wrap, full, smem, grid, s, perSM);
+        case 3: return wave_dispatch_team_3(a, R, NP, wrap, full, smem, grid, s, perSM);
+        case 4: return wave_dispatch_team_4(a, R, NP, wrap, full, smem, grid, s, perSM);
+        default: return cudaErrorInvalidValue;
+        }
+    }
     switch (a.Dp / 64) {
     case 1: return wave_dispatch_1(a, R, NP, wrap, full, smem, grid, s, perSM);
     case 2: return wave_dispatch_2(a, R, NP, wrap, full, smem, grid, s, perSM);
@@ -47,7 +68,7 @@ int wave_rows_options(int Dp, int* out, int max) {
 // Shared-memory fit (largest helper rings) and occupancy of one kernel class
 // at a widest image Wmax.
 static cudaError_t plan_class(int Wmax, int Dp, int R, bool wrap, bool full, bool diag, int numSMs,
-                              WavePlan* plan, int CL = 1) {
+                              WavePlan* plan, int CL = 1, int T = 32) {
     if (R != 4 && R != 8 && R != 16) return cudaErrorInvalidValue;
     const int NP = diag ? 3 : 1;
     int dev = 0, maxSmem = 0;
@@ -69,9 +90,10 @@ static cudaError_t plan_class(int Wmax, int Dp, int R, bool wrap, bool full, boo
     a.QI = a.QX = Q;
     a.CL = CL;
     int perSM = 0;
-    cudaError_t e = dispatch_wave(a, R, NP, wrap, full, L.total, 0, nullptr, &perSM);
+    cudaError_t e = dispatch_wave(a, R, NP, wrap, full, L.total, 0, nullptr, &perSM, T);
     if (e != cudaSuccess) return e;
     if (perSM < 1) return cudaErrorInvalidConfiguration;
+    plan->T = T;
     plan->R = R;
     plan->Q = Q;
     plan->smem = L.total;
@@ -158,6 +180,11 @@ int wave_lookahead_bands(int W) {
 
 cudaError_t wave_batch_plan(int Wmax, int Dp, int R, bool wrap, bool full, bool diag, int numSMs,
                             WavePlan* plan) {
+    // teams where they exist (8 or 16 rows per band), full warps otherwise
+    const int T = wave_team_lanes(Dp);
+    if (T != 32 && (R == 8 || R == 16) &&
+        plan_class(Wmax, Dp, R, wrap, full, diag, numSMs, plan, 1, T) == cudaSuccess)
+        return cudaSuccess;
     return plan_class(Wmax, Dp, R, wrap, full, diag, numSMs, plan);
 }
 
@@ -184,7 +211,7 @@ cudaError_t launch_aggregate_wave_batch(const WaveJob* d_jobs, const uint32_t* d
     a.stallTest = 0;
     a.trace = nullptr;
     int dummy = 0;
-    return dispatch_wave(a, plan.R, diag ? 3 : 1, wrap, full, plan.smem, grid, s, &dummy);
+    return dispatch_wave(a, plan.R, diag ? 3 : 1, wrap, full, plan.smem, grid, s, &dummy, plan.T);
 }
 
 }  // namespace lumen

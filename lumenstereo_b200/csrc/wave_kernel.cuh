@@ -394,16 +394,42 @@ __device__ __forceinline__ uint32_t wave_min(const uint32_t (&L)[KW], unsigned g
     return __reduce_min_sync(gmask, m);
 }
 
-// Warp layout: warps [0, R) carry one row each, warp R imports, warp R+1 exports.
-template <int KW, bool WRAP, bool FULL, int NP, int R>
-__global__ void __launch_bounds__((R + 2) * 32)
+// min over a team of T lanes' disparities, replicated in both halves
+template <int KW, int T>
+__device__ __forceinline__ uint32_t wave_min_t(const uint32_t (&L)[KW]) {
+    if constexpr (T == 32) {
+        return wave_min<KW>(L, kFullMask);
+    } else {
+        uint32_t a[KW];
+#pragma unroll
+        for (int i = 0; i < KW; ++i) a[i] = L[i];
+#pragma unroll
+        for (int s = 1; s < KW; s *= 2)
+#pragma unroll
+            for (int i = 0; i + s < KW; i += 2 * s) a[i] = __vminu2(a[i], a[i + s]);
+        uint32_t m = __vminu2(a[0], __byte_perm(a[0], a[0], 0x1032));
+#pragma unroll
+        for (int o = T / 2; o > 0; o >>= 1) m = __vminu2(m, __shfl_xor_sync(kFullMask, m, o));
+        return m;
+    }
+}
+
+// Warp layout: each row is a team of T lanes (32 / T rows per warp), row
+// warps [0, RW), then one import and one export warp.  T = 32 (one row per
+// warp) gives the shortest step; narrower teams spread a step's fixed costs
+// (prefetch, penalties, addressing, reductions) over several rows and suit
+// the throughput-bound batched launches.
+template <int KW, bool WRAP, bool FULL, int NP, int R, int T = 32>
+__global__ void __launch_bounds__((R / (32 / T) + 2) * 32)
 wave_kernel(WaveArgs a) {
     constexpr int LAG = NP == 3 ? 2 : 1;
-    constexpr int DP = 64 * KW;          // padded disparities
+    constexpr int DP = 2 * KW * T;       // padded disparities
     constexpr int SB = wave_slot_bytes(DP, NP);
-    constexpr int RW = R;                // row warps, one row each
+    constexpr int RPW = 32 / T;          // rows per warp
+    static_assert(R % RPW == 0, "whole warps of rows");
+    constexpr int RW = R / RPW;          // row warps
     constexpr int CPV = DP / 16;         // 16-byte cost chunks per pixel
-    static_assert(CPV <= 32, "one cost chunk per lane");
+    static_assert(CPV <= T, "one cost chunk per team lane");
     extern __shared__ __align__(128) uint8_t sm[];
     const WaveSmem L = wave_smem(a.Wmax, DP, R, NP, a.QI, a.QX);
     const int QI = a.QI, QX = a.QX;
@@ -416,7 +442,8 @@ wave_kernel(WaveArgs a) {
     unsigned* sctr = reinterpret_cast<unsigned*>(sm + L.misc) + 8;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int off = lane * 2 * KW;  // first disparity of this lane
+    const int tl = lane & (T - 1);  // lane within the row's team
+    const int off = tl * 2 * KW;    // first disparity of this lane
 
     // cluster mode: this CTA's rank; [16 + rank] of rank 0's sflag: the rank's stop request
     const int CL = a.CL;
@@ -488,7 +515,7 @@ wave_kernel(WaveArgs a) {
             lutP2 = J.P2;
         }
         if (J.D != maskD) {
-            make_lane_masks<KW>(lane, J.D, mk);
+            make_lane_masks<KW>(tl, J.D, mk);
             maskD = J.D;
         }
         const int v0 = b * R;
@@ -520,7 +547,7 @@ wave_kernel(WaveArgs a) {
             // no band for this rank in this ticket
         } else if (warp < RW) {
             // ===================== row warps, lockstep =====================
-            const int r = warp;                            // one row per warp
+            const int r = warp * RPW + lane / T;           // this team's row
             const bool rowOn = r <= lastActive;
             const int v = v0 + min(r, lastActive);
             const int y = sw ? H - 1 - v : v;
@@ -549,14 +576,17 @@ wave_kernel(WaveArgs a) {
                     const int x = sw ? W - 1 - p : p;
                     const uint8_t* src = cgrow + (size_t)x * DP;
                     const uint32_t dst = w_smem_addr(costRing + (p % kWPF) * DP);
-                    if (OWN) {
+                    if constexpr (OWN && (2 * KW) % 16 == 0) {
+#pragma unroll
+                        for (int q = 0; q < (2 * KW) / 16; ++q) w_cp_async16(dst + off + 16 * q, src + off + 16 * q);
+                    } else if (OWN) {
 #pragma unroll
                         for (int q = 0; q < KW / 2; ++q)
                             asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst + off + 4 * q),
                                          "l"(src + off + 4 * q)
                                          : "memory");
-                    } else if (lane < CPV) {
-                        w_cp_async16(dst + 16 * lane, src + 16 * lane);
+                    } else if (tl < CPV) {
+                        w_cp_async16(dst + 16 * tl, src + 16 * tl);
                     }
                 }
                 w_cp_commit();
@@ -569,20 +599,23 @@ wave_kernel(WaveArgs a) {
             for (int w = 0; w < KW; ++w) LH[w] = 0;
             uint32_t minH = 0;
             unsigned impSeen = 0, expSeen = 0;
-            const bool warpImports = importer0;
-            const bool warpExports = exporter;  // waits on the export warp for ring space
+            // the helper waits take whole warps: the one holding row 0 (imports)
+            // and the one holding the exporting row (export ring space)
+            const bool warpImports = hasPrev && warp == 0;
+            const bool warpExports = hasNext && warp == lastActive / RPW;
             for (int step = 0; step < nSteps; ++step) {
                 const int u = step - LAG * r;
                 const bool on = rowOn && u >= 0 && u < W;
                 const int uc = min(max(u, 0), W - 1);
                 // ---- helper hand-offs (row 0 / the exporting row) ----
-                if (warpImports && ok && on)
-                    ok = prevLocal ? w_wait_cl(&sctr[0], (unsigned)min(W, u + 2), impSeen, sflag + 1, a.status,
+                const int u0 = step, uE = step - LAG * lastActive;  // row 0's and the exporting row's pixel
+                if (warpImports && ok && u0 < W)
+                    ok = prevLocal ? w_wait_cl(&sctr[0], (unsigned)min(W, u0 + 2), impSeen, sflag + 1, a.status,
                                                a.spinMax, a.trace ? sflag + 4 : nullptr)
-                                   : w_wait_cta(&sctr[0], (unsigned)min(W, u + 2), impSeen, sflag + 1, a.status,
+                                   : w_wait_cta(&sctr[0], (unsigned)min(W, u0 + 2), impSeen, sflag + 1, a.status,
                                                 a.spinMax, a.trace ? sflag + 4 : nullptr);
-                if (warpExports && ok && on && u >= QX)
-                    ok = w_wait_cta(&sctr[3], (unsigned)(u - QX + 1), expSeen, sflag + 1, a.status,
+                if (warpExports && ok && uE >= QX && uE < W)
+                    ok = w_wait_cta(&sctr[3], (unsigned)(uE - QX + 1), expSeen, sflag + 1, a.status,
                                     a.spinMax, a.trace ? sflag + 4 : nullptr);
                 // ---- cost of this step's pixel ----
                 prefetch(step);
@@ -601,7 +634,7 @@ wave_kernel(WaveArgs a) {
                                          p2lut[abs(cur - iprev[min(uc + 1, W - 1)])]};
                 // ---- horizontal path ----
                 uint32_t LnH[KW];
-                wave_step<KW, 32, WRAP, FULL>(LH, Cw, minH, p2h, J.p1x2, J.bsub, mk, LnH);
+                wave_step<KW, T, WRAP, FULL>(LH, Cw, minH, p2h, J.p1x2, J.bsub, mk, LnH);
                 // ---- vertical / diagonal paths from the previous row ----
                 uint32_t Ln[NP][KW], mn[NP];
 #pragma unroll
@@ -612,14 +645,14 @@ wave_kernel(WaveArgs a) {
                     uint32_t Lp[KW];
                     load_words<KW>(reinterpret_cast<const uint16_t*>(slot + pth * 2 * DP) + off, Lp);
                     const uint32_t mp = reinterpret_cast<const uint32_t*>(slot + NP * 2 * DP)[pth];
-                    wave_step<KW, 32, WRAP, FULL>(Lp, Cw, mp, p2v[pth], J.p1x2, J.bsub, mk, Ln[pth]);
+                    wave_step<KW, T, WRAP, FULL>(Lp, Cw, mp, p2v[pth], J.p1x2, J.bsub, mk, Ln[pth]);
                 }
                 // a row that has not reached its first pixel ran on dummy data: its
                 // horizontal-path state must stay at its start value (0)
-                const uint32_t minHn = wave_min<KW>(LnH, kFullMask);
+                const uint32_t minHn = wave_min_t<KW, T>(LnH);
                 minH = on ? minHn : minH;
 #pragma unroll
-                for (int pth = 0; pth < NP; ++pth) mn[pth] = wave_min<KW>(Ln[pth], kFullMask);
+                for (int pth = 0; pth < NP; ++pth) mn[pth] = wave_min_t<KW, T>(Ln[pth]);
                 uint32_t S[KW];
 #pragma unroll
                 for (int w = 0; w < KW; ++w) {
@@ -629,7 +662,7 @@ wave_kernel(WaveArgs a) {
                     for (int pth = 0; pth < NP; ++pth) sum = WRAP ? __vadd2(sum, Ln[pth][w]) : sum + Ln[pth][w];
                     S[w] = sum;
                 }
-                if (a.trace && lane == 0 && on && u == (W >> 1)) {
+                if (a.trace && tl == 0 && on && u == (W >> 1)) {
                     if (r == 0) tMid[0] = wave_now();
                     if (r == lastActive) tMid[1] = wave_now();
                 }
@@ -642,21 +675,23 @@ wave_kernel(WaveArgs a) {
 #pragma unroll
                         for (int pth = 0; pth < NP; ++pth)
                             store_words<KW>(reinterpret_cast<uint16_t*>(slot + pth * 2 * DP) + off, Ln[pth]);
-                        if (lane == 0) {
+                        if (tl == 0) {
                             if (NP == 3)
                                 *reinterpret_cast<uint4*>(slot + NP * 2 * DP) = make_uint4(mn[0], mn[NP > 1 ? 1 : 0], mn[NP > 2 ? 2 : 0], 0u);
                             else
                                 *reinterpret_cast<uint32_t*>(slot + NP * 2 * DP) = mn[0];
                         }
                     }
-                    if (exporter || importer0) {
-                        __syncwarp();
-                        if (lane == 0) {
-                            if (exporter) w_st_release_cta(&sctr[2], (unsigned)(u + 1));
-                            if (importer0) {
-                                if (prevLocal) w_st_release_cl(&sctr[1], (unsigned)u);
-                                else w_st_release_cta(&sctr[1], (unsigned)u);
-                            }
+                }
+                // publish the exporting row's slot and row 0's progress (every
+                // lane of the warp has stored its part of the slot)
+                if (warpImports || warpExports) {
+                    __syncwarp();
+                    if (tl == 0 && on && ok) {
+                        if (exporter) w_st_release_cta(&sctr[2], (unsigned)(u + 1));
+                        if (importer0) {
+                            if (prevLocal) w_st_release_cl(&sctr[1], (unsigned)u);
+                            else w_st_release_cta(&sctr[1], (unsigned)u);
                         }
                     }
                 }
