@@ -157,7 +157,10 @@ lumen_status batch_describe(const std::vector<BatchPair>& pairs, std::vector<Bat
                             int R, int numSMs, std::vector<uint8_t>& host) {
     size_t dOff = 0;
     for (BatchGroup& g : groups) {
-        cudaError_t e = wave_batch_plan(g.Wmax, g.Dp, R, g.wrap, g.full, g.diag, numSMs, &g.plan);
+        // a group of several pairs is throughput-bound: lane teams; a pair or
+        // two are bound by the wavefront's step latency: full-warp rows
+        const bool teams = g.pairs.size() >= 4;
+        cudaError_t e = wave_batch_plan(g.Wmax, g.Dp, R, g.wrap, g.full, g.diag, numSMs, &g.plan, teams);
         if (e != cudaSuccess)
             return bfail(LUMEN_ERR_INVALID_ARGUMENT,
                          std::string("batch: no sweep configuration for a group: ") + cudaGetErrorString(e));

@@ -102,8 +102,10 @@ size_t wave_ring_bytes(int nBands, int Dp, bool diag);
 int wave_lookahead_bands(int W);
 WaveJob wave_job(const PairView& pv, uint16_t* partB, const SgmConsts& k, int R, uint8_t* xring,
                  unsigned* counters);
+// teams: narrow lane teams per row (throughput over step latency: for groups
+// with enough pairs to keep the GPU busy)
 cudaError_t wave_batch_plan(int Wmax, int Dp, int R, bool wrap, bool full, bool diag, int numSMs,
-                            WavePlan* plan);
+                            WavePlan* plan, bool teams = false);
 cudaError_t launch_aggregate_wave_batch(const WaveJob* d_jobs, const uint32_t* d_table, int nTickets,
                                         int window, int Wmax, int Dp, bool wrap, bool full,
                                         bool diag, const WavePlan& plan, unsigned* ticket,

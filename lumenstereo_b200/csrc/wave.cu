@@ -179,9 +179,9 @@ int wave_lookahead_bands(int W) {
 }
 
 cudaError_t wave_batch_plan(int Wmax, int Dp, int R, bool wrap, bool full, bool diag, int numSMs,
-                            WavePlan* plan) {
-    // teams where they exist (8 or 16 rows per band), full warps otherwise
-    const int T = wave_team_lanes(Dp);
+                            WavePlan* plan, bool teams) {
+    // teams where they exist (8 or 16 rows per band) and were asked for, full warps otherwise
+    const int T = teams ? wave_team_lanes(Dp) : 32;
     if (T != 32 && (R == 8 || R == 16) &&
         plan_class(Wmax, Dp, R, wrap, full, diag, numSMs, plan, 1, T) == cudaSuccess)
         return cudaSuccess;

@@ -429,7 +429,7 @@ wave_kernel(WaveArgs a) {
     static_assert(R % RPW == 0, "whole warps of rows");
     constexpr int RW = R / RPW;          // row warps
     constexpr int CPV = DP / 16;         // 16-byte cost chunks per pixel
-    static_assert(CPV <= T, "one cost chunk per team lane");
+    static_assert(KW % 2 == 0 || CPV <= T, "one cost chunk per team lane");
     extern __shared__ __align__(128) uint8_t sm[];
     const WaveSmem L = wave_smem(a.Wmax, DP, R, NP, a.QI, a.QX);
     const int QI = a.QI, QX = a.QX;

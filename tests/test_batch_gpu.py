@@ -107,3 +107,34 @@ def test_batch_autotune_keeps_outputs():
         b.sync()
     for o, ref in zip(outs, refs):
         assert np.array_equal(o.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("rows", [8, 16])
+def test_batch_lane_team_classes(rows):
+    """Groups of four or more pairs run with narrow lane teams per row (8
+    lanes for 64/128 padded disparities, 16 for 192/256): every class of them
+    (both path sets, uint16 wrap, partial padding, odd sizes) against the
+    plain call, which keeps full-warp rows."""
+    torch = pytest.importorskip("torch")
+    classes = [
+        dict(maxDisparity=128, numDirections=8, matchingCostMode=MatchingCostMode.Census),
+        dict(maxDisparity=170, numDirections=4),                      # Dp 192, partial
+        dict(maxDisparity=256, numDirections=8),                      # Dp 256
+        dict(minDisparity=3, maxDisparity=40, numDirections=8, blockSize=19),  # wrap, Dp 64
+    ]
+    pairs = []
+    for c, kw in enumerate(classes):
+        for i in range(4):
+            w, h = 150 + 17 * i, 60 + 9 * i
+            left, right, _ = synth.make_pair(synth.PairSpec(w, h, 4, 1, 30, 2.0, 900 + 10 * c + i))
+            p = StereoParams(speckleWindowSize=0, P2=700 + 50 * i, **kw)
+            pairs.append((p, torch.from_numpy(left).cuda(), torch.from_numpy(right).cuda(), w, h))
+    refs = _plain(torch, pairs)
+    outs = [torch.full((h, w), 0x7ABC, dtype=torch.int16, device="cuda") for _, _, _, w, h in pairs]
+    with StereoBatch(rows_per_band=rows, use_graph=True) as b:
+        for (p, dl, dr, w, h), o in zip(pairs, outs):
+            b.add(p, dl.data_ptr(), dr.data_ptr(), w, h, o.data_ptr())
+        b.run()
+        b.sync()
+    for i, (o, ref) in enumerate(zip(outs, refs)):
+        assert np.array_equal(o.cpu().numpy(), ref), i
