@@ -448,11 +448,13 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
     const bool sweepable = (mask == 0xFFu || mask == 0x0Fu);
     int sched = h->schedule;
     SweepConfig cfg = h->forced.T ? h->forced : sweep_default_config(Dp, wrap);
+    bool cfgChosen = h->forced.T != 0;  // pinned or tuned, not a schedule's default
     if (!h->forced.T && sched == 0) {
         auto it = h->tuned.find(tune_key(W, H, p, mask, wrap));
         if (it != h->tuned.end()) {
             sched = it->second.first;
             cfg = it->second.second;
+            cfgChosen = true;
         }
     }
     if (sched == 0) sched = sweepable ? 4 : 1;
@@ -471,7 +473,15 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
         if (planned) cfg = SweepConfig{32, plan4.R};
         else sched = 4;
     }
-    if (sched == 4) {
+    bool teamPlanned = false;
+    if (sched == 4 && cfgChosen && cfg.T != 32 && cfg.T == wave_team_lanes(Dp) && (cfg.NW == 8 || cfg.NW == 16)) {
+        // rows as lane teams of cfg.T lanes (an autotuner candidate)
+        if (wave_plan(k, cfg.NW, wrap, mask == 0xFFu, h->numSMs, &plan4, 1, cfg.T) == cudaSuccess)
+            teamPlanned = true;
+        else
+            cfg = SweepConfig{32, cfg.NW};
+    }
+    if (sched == 4 && !teamPlanned) {
         const int R = (cfg.T == 32 && (cfg.NW == 4 || cfg.NW == 8 || cfg.NW == 16)) ? cfg.NW : 8;
         if (wave_plan(k, R, wrap, mask == 0xFFu, h->numSMs, &plan4) == cudaSuccess ||
             wave_plan(k, 8, wrap, mask == 0xFFu, h->numSMs, &plan4) == cudaSuccess ||
@@ -663,6 +673,11 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
         for (int i = 0; i < nr; ++i) cands.push_back({3, SweepConfig{32, rs[i]}});
         const int nw = wave_rows_options(Dp, rs, 4);
         for (int i = 0; i < nw; ++i) cands.push_back({4, SweepConfig{32, rs[i]}});
+        const int tl = wave_team_lanes(Dp);
+        if (tl != 32) {
+            cands.push_back({4, SweepConfig{tl, 8}});
+            cands.push_back({4, SweepConfig{tl, 16}});
+        }
         for (int i = 0; i < nw; ++i) cands.push_back({5, SweepConfig{32, rs[i]}});
     }
     const SweepConfig savedForced = h->forced;

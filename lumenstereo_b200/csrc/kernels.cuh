@@ -91,8 +91,11 @@ struct WavePlan {
 int wave_rows_options(int Dp, int* out, int max);
 // CL > 1: consecutive bands of a sweep run in thread-block clusters of CL CTAs
 // (hand-offs inside a cluster through distributed shared memory).
+// T < 32: rows as teams of T lanes (wave_team_lanes(Dp) only, no clusters).
 cudaError_t wave_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSMs, WavePlan* plan,
-                      int CL = 1);
+                      int CL = 1, int T = 32);
+// the team width of the team kernels for a padded disparity count (32: none)
+int wave_team_lanes(int Dp);
 // Batched form: one launch over the bands of several pairs of one kernel
 // class (padded disparity count, path set, arithmetic mode).  d_jobs / d_table
 // live in device memory (see wave_kernel.cuh for their layout).

@@ -108,9 +108,10 @@ size_t wave_ring_bytes(int nBands, int Dp, bool diag) {
 }
 
 cudaError_t wave_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSMs, WavePlan* plan,
-                      int CL) {
+                      int CL, int T) {
     if (CL != 1 && CL != 2 && CL != 4 && CL != 8) return cudaErrorInvalidValue;
-    cudaError_t e = plan_class(k.W, k.Dp, R, wrap, k.D == k.Dp, diag, numSMs, plan, CL);
+    if (T != 32 && (CL != 1 || T != wave_team_lanes(k.Dp))) return cudaErrorInvalidValue;
+    cudaError_t e = plan_class(k.W, k.Dp, R, wrap, k.D == k.Dp, diag, numSMs, plan, CL, T);
     if (e != cudaSuccess) return e;
     plan->nBands = (k.H + R - 1) / R;
     // tickets alternate the two sweeps; with clusters a ticket holds CL
@@ -166,7 +167,7 @@ cudaError_t launch_aggregate_wave(const PairView& pv, uint16_t* partB, const Sgm
     cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned) * plan.counterWords, s);
     if (e != cudaSuccess) return e;
     int dummy = 0;
-    return dispatch_wave(a, plan.R, diag ? 3 : 1, wrap, k.D == k.Dp, plan.smem, plan.grid, s, &dummy);
+    return dispatch_wave(a, plan.R, diag ? 3 : 1, wrap, k.D == k.Dp, plan.smem, plan.grid, s, &dummy, plan.T);
 }
 
 int wave_lookahead_bands(int W) {

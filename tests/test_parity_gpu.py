@@ -190,6 +190,30 @@ def test_parity_schedule4_rows(D, rows, oracle_mod):
         assert_subpix_close(disp, ref_disp)
 
 
+@pytest.mark.parametrize("rows", [8, 16])
+@pytest.mark.parametrize("D", [40, 128, 150, 200, 256])
+def test_parity_schedule4_lane_teams(D, rows, oracle_mod):
+    """Rows as lane teams (8 lanes for 64/128 padded disparities, 16 for
+    192/256; the batched launches' form) in the plain call, pinned through
+    set_tuning: bit for bit equal to the oracle, partial last bands included."""
+    team = 8 if D <= 128 else 16
+    left, right, _ = synth.make_pair(synth.PairSpec(131, 75, 4, 1, min(D - 1, 40), 2.0, 280 + D))
+    for mode, nd in ((0, 8), (1, 4)):
+        pd = params_dict(maxDisparity=D, numDirections=nd, matchingCostMode=mode,
+                         speckleWindowSize=0)
+        with StereoSGBM(to_params(pd)) as s:
+            s.set_schedule(4)
+            s.set_tuning(team, rows)
+            s.retain_intermediates(True)
+            disp = s.compute(left, right)
+            agg = s.intermediate("agg", (75, 131, D), np.uint16)
+            used = s.get_tuning()
+        assert tuple(used) == (4, team, rows), used
+        ref_disp, ref = oracle_mod.sgbm(pd, left, right, intermediates=True)
+        assert np.array_equal(agg, ref["agg"]), (mode, nd)
+        assert_subpix_close(disp, ref_disp)
+
+
 def test_parity_schedule4_wide_image(oracle_mod):
     """A row longer than the exchange ring (kWK = 64 pixels) exercises the
     exporter's back-pressure waits between bands."""
