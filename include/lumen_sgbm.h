@@ -121,9 +121,11 @@ lumen_status lumen_sgbm_debug_set_paths(lumen_sgbm* h, uint32_t path_mask);
  * distributed shared memory.  Outputs are identical for every schedule. */
 lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule);
 /* Pin the fused-sweep configuration: lanes per pixel (8, 16 or 32) and warps
- * per thread block (2, 4, 8 or 16; rows per band = warps * 32 / lanes).
- * Schedules 3 and 4 use 32 lanes and take `warps` as their rows per band
- * (schedule 3: 4 or 8; schedules 4 and 5: 4, 8 or 16).  0, 0 restores the automatic
+ * per thread block (schedule 2: 2, 4, 8 or 16; rows per band = warps * 32 /
+ * lanes).  Schedules 3-5 take `warps` as their rows per band: schedule 3 with
+ * 32 lanes, 4 or 8 rows; schedules 4 and 5 with 32 lanes, 4, 8 or 16 rows;
+ * schedule 4 with 8 lanes (padded disparities up to 128) or 16 lanes (up to
+ * 256), rows as lane teams, 8, 16 or 32 rows.  0, 0 restores the automatic
  * choice.  Values are identical for every setting. */
 lumen_status lumen_sgbm_set_tuning(lumen_sgbm* h, int lanes_per_pixel, int warps_per_block);
 /* The schedule and configuration the last compute used: {schedule, lanes, warps}. */

@@ -293,8 +293,9 @@ extern "C" lumen_status lumen_sgbm_set_tuning(lumen_sgbm* h, int lanes, int warp
         h->forced = SweepConfig{0, 0};
         return LUMEN_OK;
     }
-    if (!(lanes == 8 || lanes == 16 || lanes == 32) || !(warps == 2 || warps == 4 || warps == 8 || warps == 16))
-        return fail(LUMEN_ERR_INVALID_ARGUMENT, "lanes must be 8/16/32 and warps 2/4/8/16");
+    if (!(lanes == 8 || lanes == 16 || lanes == 32) ||
+        !(warps == 2 || warps == 4 || warps == 8 || warps == 16 || warps == 32))
+        return fail(LUMEN_ERR_INVALID_ARGUMENT, "lanes must be 8/16/32 and warps 2/4/8/16/32");
     h->forced = SweepConfig{lanes, warps};
     return LUMEN_OK;
 }
@@ -474,7 +475,8 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
         else sched = 4;
     }
     bool teamPlanned = false;
-    if (sched == 4 && cfgChosen && cfg.T != 32 && cfg.T == wave_team_lanes(Dp) && (cfg.NW == 8 || cfg.NW == 16)) {
+    if (sched == 4 && cfgChosen && cfg.T != 32 && cfg.T == wave_team_lanes(Dp) &&
+        (cfg.NW == 8 || cfg.NW == 16 || cfg.NW == 32)) {
         // rows as lane teams of cfg.T lanes (an autotuner candidate)
         if (wave_plan(k, cfg.NW, wrap, mask == 0xFFu, h->numSMs, &plan4, 1, cfg.T) == cudaSuccess)
             teamPlanned = true;
@@ -677,6 +679,7 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
         if (tl != 32) {
             cands.push_back({4, SweepConfig{tl, 8}});
             cands.push_back({4, SweepConfig{tl, 16}});
+            cands.push_back({4, SweepConfig{tl, 32}});
         }
         for (int i = 0; i < nw; ++i) cands.push_back({5, SweepConfig{32, rs[i]}});
     }

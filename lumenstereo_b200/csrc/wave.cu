@@ -34,7 +34,7 @@ int wave_team_lanes(int Dp) { return Dp <= 128 ? 8 : Dp <= 256 ? 16 : 32; }
 static cudaError_t dispatch_wave(const WaveArgs& a, int R, int NP, bool wrap, bool full, int smem,
                                  int grid, cudaStream_t s, int* perSM, int T = 32) {
     if (T != 32) {
-        if (T != wave_team_lanes(a.Dp) || (R != 8 && R != 16)) return cudaErrorInvalidValue;
+        if (T != wave_team_lanes(a.Dp) || (R != 8 && R != 16 && R != 32)) return cudaErrorInvalidValue;
         switch (a.Dp / 64) {
         case 1: return wave_dispatch_team_1(a, R, NP, wrap, full, smem, grid, s, perSM);
         case 2: return wave_dispatch_team_2(a, R, NP, wrap, full, smem, grid, s, perSM);
@@ -69,7 +69,8 @@ int wave_rows_options(int Dp, int* out, int max) {
 // at a widest image Wmax.
 static cudaError_t plan_class(int Wmax, int Dp, int R, bool wrap, bool full, bool diag, int numSMs,
                               WavePlan* plan, int CL = 1, int T = 32) {
-    if (R != 4 && R != 8 && R != 16) return cudaErrorInvalidValue;
+    // 32-row bands only as lane teams (at most 8 row warps)
+    if (R != 4 && R != 8 && R != 16 && !(R == 32 && T != 32)) return cudaErrorInvalidValue;
     const int NP = diag ? 3 : 1;
     int dev = 0, maxSmem = 0;
     cudaGetDevice(&dev);

@@ -54,6 +54,8 @@ cudaError_t wave_dispatch_team_kp(const WaveArgs& a, int R, int NP, bool wrap, b
                                : wave_launch_np<KW, 1, 8, T>(a, wrap, full, smem, grid, s, perSM);
     if (R == 16) return NP == 3 ? wave_launch_np<KW, 3, 16, T>(a, wrap, full, smem, grid, s, perSM)
                                 : wave_launch_np<KW, 1, 16, T>(a, wrap, full, smem, grid, s, perSM);
+    if (R == 32) return NP == 3 ? wave_launch_np<KW, 3, 32, T>(a, wrap, full, smem, grid, s, perSM)
+                                : wave_launch_np<KW, 1, 32, T>(a, wrap, full, smem, grid, s, perSM);
     return cudaErrorInvalidValue;
 }
 

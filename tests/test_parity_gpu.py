@@ -190,7 +190,7 @@ def test_parity_schedule4_rows(D, rows, oracle_mod):
         assert_subpix_close(disp, ref_disp)
 
 
-@pytest.mark.parametrize("rows", [8, 16])
+@pytest.mark.parametrize("rows", [8, 16, 32])
 @pytest.mark.parametrize("D", [40, 128, 150, 200, 256])
 def test_parity_schedule4_lane_teams(D, rows, oracle_mod):
     """Rows as lane teams (8 lanes for 64/128 padded disparities, 16 for
@@ -208,7 +208,8 @@ def test_parity_schedule4_lane_teams(D, rows, oracle_mod):
             disp = s.compute(left, right)
             agg = s.intermediate("agg", (75, 131, D), np.uint16)
             used = s.get_tuning()
-        assert tuple(used) == (4, team, rows), used
+        # 32 rows of 256 disparities exceed the shared memory: 16-row bands then
+        assert tuple(used) == (4, team, rows) or (rows == 32 and used[0] == 4), used
         ref_disp, ref = oracle_mod.sgbm(pd, left, right, intermediates=True)
         assert np.array_equal(agg, ref["agg"]), (mode, nd)
         assert_subpix_close(disp, ref_disp)
