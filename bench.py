@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--schedule", type=int, default=0, help="aggregation schedule (0 = auto)")
     ap.add_argument("--rows", type=int, default=0,
                     help="rows per band of the fused sweeps with --schedule 3/4 (0 = default)")
+    ap.add_argument("--lanes", type=int, default=32,
+                    help="lanes per row with --schedule 4 --rows (8/16: lane teams)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve", "epilogue"],
                     help="plain: one pair per call (default); batch: the 64-pair mixed stream; "
@@ -230,7 +232,7 @@ def run_ours(args):
     if args.schedule:
         sgbm.set_schedule(args.schedule)
         if args.rows:
-            sgbm.set_tuning(32, args.rows)
+            sgbm.set_tuning(args.lanes, args.rows)
     stream = torch.cuda.current_stream(dev)
     sptr = stream.cuda_stream
     dl = torch.from_numpy(left).to(dev)
