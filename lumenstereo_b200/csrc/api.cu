@@ -475,7 +475,7 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
         else sched = 4;
     }
     bool teamPlanned = false;
-    if (sched == 4 && cfgChosen && cfg.T != 32 && cfg.T == wave_team_lanes(Dp) &&
+    if (sched == 4 && cfgChosen && cfg.T != 32 && wave_team_exists(Dp, cfg.T) &&
         (cfg.NW == 8 || cfg.NW == 16 || cfg.NW == 32)) {
         // rows as lane teams of cfg.T lanes (an autotuner candidate)
         if (wave_plan(k, cfg.NW, wrap, mask == 0xFFu, h->numSMs, &plan4, 1, cfg.T) == cudaSuccess)
@@ -675,8 +675,8 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
         for (int i = 0; i < nr; ++i) cands.push_back({3, SweepConfig{32, rs[i]}});
         const int nw = wave_rows_options(Dp, rs, 4);
         for (int i = 0; i < nw; ++i) cands.push_back({4, SweepConfig{32, rs[i]}});
-        const int tl = wave_team_lanes(Dp);
-        if (tl != 32) {
+        for (int tl : {8, 16}) {
+            if (!wave_team_exists(Dp, tl)) continue;
             cands.push_back({4, SweepConfig{tl, 8}});
             cands.push_back({4, SweepConfig{tl, 16}});
             cands.push_back({4, SweepConfig{tl, 32}});

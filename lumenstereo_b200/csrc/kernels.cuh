@@ -94,8 +94,10 @@ int wave_rows_options(int Dp, int* out, int max);
 // T < 32: rows as teams of T lanes (wave_team_lanes(Dp) only, no clusters).
 cudaError_t wave_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSMs, WavePlan* plan,
                       int CL = 1, int T = 32);
-// the team width of the team kernels for a padded disparity count (32: none)
+// the team width of the batched launches for a padded disparity count (32:
+// none), and whether a team kernel of T lanes exists for it
 int wave_team_lanes(int Dp);
+bool wave_team_exists(int Dp, int T);
 // Batched form: one launch over the bands of several pairs of one kernel
 // class (padded disparity count, path set, arithmetic mode).  d_jobs / d_table
 // live in device memory (see wave_kernel.cuh for their layout).

@@ -19,27 +19,33 @@ LUMEN_WAVE_DECL(5)
 LUMEN_WAVE_DECL(6)
 LUMEN_WAVE_DECL(7)
 LUMEN_WAVE_DECL(8)
-#define LUMEN_WAVE_TEAM_DECL(KP)                                                               \
-    cudaError_t wave_dispatch_team_##KP(const WaveArgs& a, int R, int NP, bool wrap, bool full, \
-                                        int smem, int grid, cudaStream_t s, int* perSM);
-LUMEN_WAVE_TEAM_DECL(1)
-LUMEN_WAVE_TEAM_DECL(2)
-LUMEN_WAVE_TEAM_DECL(3)
-LUMEN_WAVE_TEAM_DECL(4)
+#define LUMEN_WAVE_TEAM_DECL(KP, T)                                                            \
+    cudaError_t wave_dispatch_team_##KP##_##T(const WaveArgs& a, int R, int NP, bool wrap,     \
+                                              bool full, int smem, int grid, cudaStream_t s,   \
+                                              int* perSM);
+LUMEN_WAVE_TEAM_DECL(1, 8)
+LUMEN_WAVE_TEAM_DECL(2, 8)
+LUMEN_WAVE_TEAM_DECL(1, 16)
+LUMEN_WAVE_TEAM_DECL(2, 16)
+LUMEN_WAVE_TEAM_DECL(3, 16)
+LUMEN_WAVE_TEAM_DECL(4, 16)
 
 // lanes per row of the batched launches: the narrowest team that fits the
 // padded disparities in a lane's registers
 int wave_team_lanes(int Dp) { return Dp <= 128 ? 8 : Dp <= 256 ? 16 : 32; }
+bool wave_team_exists(int Dp, int T) { return T == wave_team_lanes(Dp) || (T == 16 && Dp <= 128); }
 
 static cudaError_t dispatch_wave(const WaveArgs& a, int R, int NP, bool wrap, bool full, int smem,
                                  int grid, cudaStream_t s, int* perSM, int T = 32) {
     if (T != 32) {
-        if (T != wave_team_lanes(a.Dp) || (R != 8 && R != 16 && R != 32)) return cudaErrorInvalidValue;
-        switch (a.Dp / 64) {
-        case 1: return wave_dispatch_team_1(a, R, NP, wrap, full, smem, grid, s, perSM);
-        case 2: return wave_dispatch_team_2(a, R, NP, wrap, full, smem, grid, s, perSM);
-        case 3: return wave_dispatch_team_3(a, R, NP, wrap, full, smem, grid, s, perSM);
-        case 4: return wave_dispatch_team_4(a, R, NP, wrap, full, smem, grid, s, perSM);
+        if (!wave_team_exists(a.Dp, T) || (R != 8 && R != 16 && R != 32)) return cudaErrorInvalidValue;
+        switch (a.Dp / 64 * 100 + T) {
+        case 108: return wave_dispatch_team_1_8(a, R, NP, wrap, full, smem, grid, s, perSM);
+        case 208: return wave_dispatch_team_2_8(a, R, NP, wrap, full, smem, grid, s, perSM);
+        case 116: return wave_dispatch_team_1_16(a, R, NP, wrap, full, smem, grid, s, perSM);
+        case 216: return wave_dispatch_team_2_16(a, R, NP, wrap, full, smem, grid, s, perSM);
+        case 316: return wave_dispatch_team_3_16(a, R, NP, wrap, full, smem, grid, s, perSM);
+        case 416: return wave_dispatch_team_4_16(a, R, NP, wrap, full, smem, grid, s, perSM);
         default: return cudaErrorInvalidValue;
         }
     }
@@ -111,7 +117,7 @@ size_t wave_ring_bytes(int nBands, int Dp, bool diag) {
 cudaError_t wave_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSMs, WavePlan* plan,
                       int CL, int T) {
     if (CL != 1 && CL != 2 && CL != 4 && CL != 8) return cudaErrorInvalidValue;
-    if (T != 32 && (CL != 1 || T != wave_team_lanes(k.Dp))) return cudaErrorInvalidValue;
+    if (T != 32 && (CL != 1 || !wave_team_exists(k.Dp, T))) return cudaErrorInvalidValue;
     cudaError_t e = plan_class(k.W, k.Dp, R, wrap, k.D == k.Dp, diag, numSMs, plan, CL, T);
     if (e != cudaSuccess) return e;
     plan->nBands = (k.H + R - 1) / R;

@@ -82,11 +82,12 @@ cudaError_t wave_dispatch_kp(const WaveArgs& a, int R, int NP, bool wrap, bool f
     }                                                                                          \
     }
 
-// team instances: 8 lanes for 64 and 128 padded disparities, 16 for 192 and 256
+// team instances: 8 or 16 lanes for 64 and 128 padded disparities, 16 for 192 and 256
 #define LUMEN_WAVE_TEAM_INSTANCE(KP, T)                                                        \
     namespace lumen {                                                                          \
-    cudaError_t wave_dispatch_team_##KP(const WaveArgs& a, int R, int NP, bool wrap, bool full, \
-                                        int smem, int grid, cudaStream_t s, int* perSM) {      \
+    cudaError_t wave_dispatch_team_##KP##_##T(const WaveArgs& a, int R, int NP, bool wrap,     \
+                                              bool full, int smem, int grid, cudaStream_t s,   \
+                                              int* perSM) {                                    \
         return wave_dispatch_team_kp<KP, T>(a, R, NP, wrap, full, smem, grid, s, perSM);       \
     }                                                                                          \
     }

@@ -4,3 +4,4 @@
 
 LUMEN_WAVE_INSTANCE(1)
 LUMEN_WAVE_TEAM_INSTANCE(1, 8)
+LUMEN_WAVE_TEAM_INSTANCE(1, 16)

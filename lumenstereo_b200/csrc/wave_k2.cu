@@ -4,3 +4,4 @@
 
 LUMEN_WAVE_INSTANCE(2)
 LUMEN_WAVE_TEAM_INSTANCE(2, 8)
+LUMEN_WAVE_TEAM_INSTANCE(2, 16)

@@ -191,12 +191,11 @@ def test_parity_schedule4_rows(D, rows, oracle_mod):
 
 
 @pytest.mark.parametrize("rows", [8, 16, 32])
-@pytest.mark.parametrize("D", [40, 128, 150, 200, 256])
-def test_parity_schedule4_lane_teams(D, rows, oracle_mod):
-    """Rows as lane teams (8 lanes for 64/128 padded disparities, 16 for
+@pytest.mark.parametrize("D,team", [(40, 8), (128, 8), (40, 16), (128, 16), (150, 16), (200, 16), (256, 16)])
+def test_parity_schedule4_lane_teams(D, team, rows, oracle_mod):
+    """Rows as lane teams (8 or 16 lanes for 64/128 padded disparities, 16 for
     192/256; the batched launches' form) in the plain call, pinned through
     set_tuning: bit for bit equal to the oracle, partial last bands included."""
-    team = 8 if D <= 128 else 16
     left, right, _ = synth.make_pair(synth.PairSpec(131, 75, 4, 1, min(D - 1, 40), 2.0, 280 + D))
     for mode, nd in ((0, 8), (1, 4)):
         pd = params_dict(maxDisparity=D, numDirections=nd, matchingCostMode=mode,
