@@ -29,10 +29,11 @@ LUMEN_WAVE_TEAM_DECL(1, 16)
 LUMEN_WAVE_TEAM_DECL(2, 16)
 LUMEN_WAVE_TEAM_DECL(3, 16)
 LUMEN_WAVE_TEAM_DECL(4, 16)
+LUMEN_WAVE_TEAM_DECL(5, 16)
 
 // lanes per row of the batched launches: the narrowest team that fits the
 // padded disparities in a lane's registers
-int wave_team_lanes(int Dp) { return Dp <= 128 ? 8 : Dp <= 256 ? 16 : 32; }
+int wave_team_lanes(int Dp) { return Dp <= 128 ? 8 : Dp <= 320 ? 16 : 32; }
 bool wave_team_exists(int Dp, int T) { return T == wave_team_lanes(Dp) || (T == 16 && Dp <= 128); }
 
 static cudaError_t dispatch_wave(const WaveArgs& a, int R, int NP, bool wrap, bool full, int smem,
@@ -46,6 +47,7 @@ static cudaError_t dispatch_wave(const WaveArgs& a, int R, int NP, bool wrap, bo
         case 216: return wave_dispatch_team_2_16(a, R, NP, wrap, full, smem, grid, s, perSM);
         case 316: return wave_dispatch_team_3_16(a, R, NP, wrap, full, smem, grid, s, perSM);
         case 416: return wave_dispatch_team_4_16(a, R, NP, wrap, full, smem, grid, s, perSM);
+        case 516: return wave_dispatch_team_5_16(a, R, NP, wrap, full, smem, grid, s, perSM);
         default: return cudaErrorInvalidValue;
         }
     }

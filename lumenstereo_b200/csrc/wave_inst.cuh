@@ -82,7 +82,7 @@ cudaError_t wave_dispatch_kp(const WaveArgs& a, int R, int NP, bool wrap, bool f
     }                                                                                          \
     }
 
-// team instances: 8 or 16 lanes for 64 and 128 padded disparities, 16 for 192 and 256
+// team instances: 8 or 16 lanes for 64 and 128 padded disparities, 16 for 192 to 320
 #define LUMEN_WAVE_TEAM_INSTANCE(KP, T)                                                        \
     namespace lumen {                                                                          \
     cudaError_t wave_dispatch_team_##KP##_##T(const WaveArgs& a, int R, int NP, bool wrap,     \

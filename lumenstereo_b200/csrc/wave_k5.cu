@@ -3,3 +3,4 @@
 #include "wave_inst.cuh"
 
 LUMEN_WAVE_INSTANCE(5)
+LUMEN_WAVE_TEAM_INSTANCE(5, 16)

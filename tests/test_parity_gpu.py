@@ -191,7 +191,8 @@ def test_parity_schedule4_rows(D, rows, oracle_mod):
 
 
 @pytest.mark.parametrize("rows", [8, 16, 32])
-@pytest.mark.parametrize("D,team", [(40, 8), (128, 8), (40, 16), (128, 16), (150, 16), (200, 16), (256, 16)])
+@pytest.mark.parametrize("D,team", [(40, 8), (128, 8), (40, 16), (128, 16), (150, 16), (200, 16), (256, 16),
+                                    (290, 16)])
 def test_parity_schedule4_lane_teams(D, team, rows, oracle_mod):
     """Rows as lane teams (8 or 16 lanes for 64/128 padded disparities, 16 for
     192/256; the batched launches' form) in the plain call, pinned through
@@ -207,7 +208,7 @@ def test_parity_schedule4_lane_teams(D, team, rows, oracle_mod):
             disp = s.compute(left, right)
             agg = s.intermediate("agg", (75, 131, D), np.uint16)
             used = s.get_tuning()
-        # 32 rows of 256 disparities exceed the shared memory: 16-row bands then
+        # 32 rows of 256+ disparities exceed the shared memory: 16-row bands then
         assert tuple(used) == (4, team, rows) or (rows == 32 and used[0] == 4), used
         ref_disp, ref = oracle_mod.sgbm(pd, left, right, intermediates=True)
         assert np.array_equal(agg, ref["agg"]), (mode, nd)
