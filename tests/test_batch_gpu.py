@@ -112,7 +112,7 @@ def test_batch_autotune_keeps_outputs():
 @pytest.mark.parametrize("rows", [8, 16])
 def test_batch_lane_team_classes(rows):
     """Groups of four or more pairs run with narrow lane teams per row (8
-    lanes for 64/128 padded disparities, 16 for 192/256): every class of them
+    lanes for 64/128 padded disparities, 16 for 192-320): every class of them
     (both path sets, uint16 wrap, partial padding, odd sizes) against the
     plain call, which keeps full-warp rows."""
     torch = pytest.importorskip("torch")
@@ -121,6 +121,7 @@ def test_batch_lane_team_classes(rows):
         dict(maxDisparity=170, numDirections=4),                      # Dp 192, partial
         dict(maxDisparity=256, numDirections=8),                      # Dp 256
         dict(minDisparity=3, maxDisparity=40, numDirections=8, blockSize=19),  # wrap, Dp 64
+        dict(maxDisparity=290, numDirections=8, matchingCostMode=MatchingCostMode.Census),  # Dp 320
     ]
     pairs = []
     for c, kw in enumerate(classes):
