@@ -474,8 +474,12 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
         if (planned) cfg = SweepConfig{32, plan4.R};
         else sched = 4;
     }
+    // untuned default of the row-band sweeps: 16-row bands, rows as 8-lane
+    // teams where the disparity range allows (the best plain configuration
+    // measured on 1920x1080 D128; the autotuner refines it per workload)
+    if (sched == 4 && !cfgChosen) cfg = SweepConfig{wave_team_exists(Dp, 8) ? 8 : 32, 16};
     bool teamPlanned = false;
-    if (sched == 4 && cfgChosen && cfg.T != 32 && wave_team_exists(Dp, cfg.T) &&
+    if (sched == 4 && cfg.T != 32 && wave_team_exists(Dp, cfg.T) &&
         (cfg.NW == 8 || cfg.NW == 16 || cfg.NW == 32)) {
         // rows as lane teams of cfg.T lanes (an autotuner candidate)
         if (wave_plan(k, cfg.NW, wrap, mask == 0xFFu, h->numSMs, &plan4, 1, cfg.T) == cudaSuccess)
