@@ -29,6 +29,7 @@
 
 #include "../../include/lumen_sgbm.h"
 #include "batch_core.cuh"
+#include "batch_tickets.h"
 #include "common.cuh"
 #include "kernels.cuh"
 #include "wave_kernel.cuh"
@@ -182,38 +183,13 @@ lumen_status batch_describe(const std::vector<BatchPair>& pairs, std::vector<Bat
             jobs[j] = wave_job(pv, reinterpret_cast<uint16_t*>(q.base + q.oPartB), q.k, R, q.base + q.oRing,
                                reinterpret_cast<unsigned*>(q.base + q.oCtr));
         }
-        // Chunks of pairs, tickets band-major within a chunk (the chunk's
-        // wavefronts overlap), chunk after chunk.  A band may need the next
-        // wave_lookahead_bands(W) bands of its pair and sweep running, which
-        // band-major order puts up to 2 * n * lookahead tickets later in a
-        // chunk of n pairs: chunks stay small enough for that window to fit
-        // in the resident CTAs.
-        int t = 0;
-        g.window = 0;
-        for (int j0 = 0; j0 < (int)g.pairs.size();) {
-            int j1 = j0, Wc = 0, nb = 0;
-            while (j1 < (int)g.pairs.size()) {
-                const BatchPair& q = pairs[g.pairs[j1]];
-                const int w2 = std::max(Wc, q.W);
-                if (j1 > j0 && 2 * (j1 - j0 + 1) * wave_lookahead_bands(w2) + 1 > g.plan.grid) break;
-                Wc = w2;
-                nb = std::max(nb, q.nBands);
-                ++j1;
-            }
-            int chunkTickets = 0;
-            for (int j = j0; j < j1; ++j) chunkTickets += 2 * pairs[g.pairs[j]].nBands;
-            // needs stay inside the chunk
-            const int win = std::min(2 * (j1 - j0) * wave_lookahead_bands(Wc), chunkTickets);
-            if (win + 1 > g.plan.grid)
-                return bfail(LUMEN_ERR_INVALID_ARGUMENT, "batch: a pair is too wide for the resident sweep CTAs");
-            g.window = std::max(g.window, win);
-            for (int band = 0; band < nb; ++band)
-                for (int j = j0; j < j1; ++j)
-                    if (band < pairs[g.pairs[j]].nBands)
-                        for (int sw = 0; sw < 2; ++sw)
-                            table[t++] = ((uint32_t)j << 20) | ((uint32_t)sw << 19) | (uint32_t)band;
-            j0 = j1;
-        }
+        std::vector<TicketPair> tp(g.pairs.size());
+        for (int j = 0; j < (int)g.pairs.size(); ++j) tp[j] = TicketPair{pairs[g.pairs[j]].W, pairs[g.pairs[j]].nBands};
+        std::vector<uint32_t> tickets;
+        g.window = build_ticket_table(tp, g.plan.grid, kWK, tickets);
+        if (g.window < 0)
+            return bfail(LUMEN_ERR_INVALID_ARGUMENT, "batch: a pair is too wide for the resident sweep CTAs");
+        std::copy(tickets.begin(), tickets.end(), table);
     }
     return LUMEN_OK;
 }

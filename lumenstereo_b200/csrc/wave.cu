@@ -5,6 +5,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "wave_kernel.cuh"
+#include "batch_tickets.h"
 
 namespace lumen {
 
@@ -179,14 +180,7 @@ cudaError_t launch_aggregate_wave(const PairView& pv, uint16_t* partB, const Sgm
     return dispatch_wave(a, plan.R, diag ? 3 : 1, wrap, k.D == k.Dp, plan.smem, plan.grid, s, &dummy, plan.T);
 }
 
-int wave_lookahead_bands(int W) {
-    // A band's export waits for the next band to consume its ring (kWK
-    // pixels), so a band that has no CTA stalls the band above it after
-    // kWK pixels, that one after about 2 * kWK, and so on: a band can finish
-    // a row of W pixels once the ceil(W / kWK) bands below it run too (one
-    // more for the in-band row lag and the import queue).
-    return (W + kWK - 1) / kWK + 1;
-}
+int wave_lookahead_bands(int W) { return lookahead_bands(W, kWK); }
 
 cudaError_t wave_batch_plan(int Wmax, int Dp, int R, bool wrap, bool full, bool diag, int numSMs,
                             WavePlan* plan, bool teams) {

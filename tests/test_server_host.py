@@ -1,7 +1,8 @@
-"""Host logic of the served form that needs no GPU: the device-arena
-bookkeeping (lumenstereo_b200/csrc/host_arena.h) under a randomised
-allocate/free sequence, and the C ABI's server entry points exported by the
-library."""
+"""Host logic of the batched and served forms that needs no GPU: the
+device-arena bookkeeping (lumenstereo_b200/csrc/host_arena.h) under a
+randomised allocate/free sequence, the batched sweep launch's ticket table
+(lumenstereo_b200/csrc/batch_tickets.h) against the ordering and window
+properties its progress rests on, and the server's option defaults."""
 import os
 import shutil
 import subprocess
@@ -17,6 +18,15 @@ def test_arena_first_fit_and_coalescing(tmp_path):
     subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "lumenstereo_b200", "csrc"),
                     os.path.join(ROOT, "tests", "cpp", "arena_test.cpp"), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0 and out.stdout.strip() == "ok", out.stdout + out.stderr
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_ticket_table_order_and_window(tmp_path):
+    exe = tmp_path / "tickets_test"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "lumenstereo_b200", "csrc"),
+                    os.path.join(ROOT, "tests", "cpp", "tickets_test.cpp"), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
     assert out.returncode == 0 and out.stdout.strip() == "ok", out.stdout + out.stderr
 
 
