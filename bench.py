@@ -70,6 +70,20 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
+def replica_rate(local_time: float, units_per_rank: float, world: int, device="cpu"):
+    """Whole-job time and rate of `world` independent replicas: every rank
+    processed `units_per_rank`; the job's time is the slowest rank's (a MAX
+    all-reduce over the process group when world > 1)."""
+    t = float(local_time)
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        tt = torch.tensor([t], device=device, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    return t, units_per_rank * world / t
+
+
 def workload_params(wl) -> StereoParams:
     # StereoParams{} defaults except the configuration's fields and the speckle
     # filter (off: not one of the measured stages, and racy in the reference).
@@ -280,13 +294,8 @@ def run_ours(args):
         barrier()
     launches = sgbm.launch_count() - launches0
     step_ms = [a.elapsed_time(b) for a, b in ev]
-    total_ms = float(sum(step_ms))
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
-    value = pd_per_step * args.steps * world / (total_ms / 1e3)
+    total_s, value = replica_rate(sum(step_ms) / 1e3, pd_per_step * args.steps, world, dev)
+    total_ms = total_s * 1e3
 
     # e2e: host buffers through the C-ABI call (H2D + compute + D2H per step)
     lh = torch.from_numpy(left).pin_memory()
@@ -309,12 +318,7 @@ def run_ours(args):
         t0 = time.perf_counter()
         e2e_step()     # synchronous: H2D, pipeline, D2H
         e2e_time += time.perf_counter() - t0
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([e2e_time], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_time = float(tt.item())
-    e2e_value = pd_per_step * args.steps * world / e2e_time
+    e2e_time, e2e_value = replica_rate(e2e_time, pd_per_step * args.steps, world, dev)
 
     hbm, peak_kind = measured_peaks()
     P = wl.num_directions
