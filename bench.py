@@ -648,45 +648,80 @@ def run_serve(args):
 # (depth: 2 B read + 4 B written per pixel; maps: 8 B written per pixel).
 # ---------------------------------------------------------------------------
 def run_epilogue(args):
+    """The kernels either side of the disparity map, each timed as a CUDA
+    graph of 20 launches (one launch is a few microseconds: a loop of host
+    calls would time the host)."""
     import torch
-    from lumenstereo_b200 import disparity_to_depth_device, rectify_maps_device
+    from lumenstereo_b200 import (depth_colorize_device, depth_to_points_device, disparity_to_depth_color_device,
+                                  disparity_to_depth_device, rectify_maps_device)
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     peak, kind = measured_peaks()
-    stream = torch.cuda.current_stream()
-    res = {"metric": "GB/s of the depth and map-generation kernels", "unit": "GB/s", "n_gpus": world,
-           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "data": "synthetic",
-           "dtype": "f32", "vs_baseline": None, "peak_gbs": peak, "peak_kind": kind}
+    res = {"metric": "GB/s of the depth, colour, point-cloud and map-generation kernels", "unit": "GB/s",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+           "data": "synthetic", "dtype": "f32", "vs_baseline": None, "peak_gbs": peak, "peak_kind": kind}
+    reps = 20
 
     def timed(fn):
-        for _ in range(max(3, args.warmup)):
-            fn()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        for _ in range(args.steps):
-            fn()
-        b.record(stream)
+        side = torch.cuda.Stream()
+        with torch.cuda.stream(side):
+            for _ in range(max(3, args.warmup)):
+                fn(side.cuda_stream)
         torch.cuda.synchronize()
-        return a.elapsed_time(b) / args.steps
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=side):
+            for _ in range(reps):
+                fn(side.cuda_stream)
+        g.replay()
+        torch.cuda.synchronize()
+        cur = torch.cuda.current_stream()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(cur)
+        for _ in range(args.steps):
+            g.replay()
+        b.record(cur)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / (args.steps * reps)
 
-    W, H = 1920, 1080
-    disp = torch.randint(-16, 128 * 16, (H, W), dtype=torch.int16, device="cuda")
-    depth = torch.empty((H, W), dtype=torch.float32, device="cuda")
-    ms = timed(lambda: disparity_to_depth_device(disp.data_ptr(), W, H, 1400.0, 0.12, depth.data_ptr(),
-                                                 0.0, stream.cuda_stream))
-    res["depth"] = {"workload": f"{W}x{H}", "ms": ms, "gbs": W * H * 6 / ms / 1e6,
-                    "frac": W * H * 6 / ms / 1e6 / peak}
+    def entry(name, W, H, ms, bytes_):
+        res[name] = {"workload": f"{W}x{H}", "ms": ms, "gbs": bytes_ / ms / 1e6, "frac": bytes_ / ms / 1e6 / peak}
+
+    lut = np.stack([np.arange(256), 255 - np.arange(256), np.arange(256) // 2], axis=1).astype(np.uint8)
+    for W, H in ((1920, 1080), (2880, 1988)):
+        disp = torch.randint(-16, 128 * 16, (H, W), dtype=torch.int16, device="cuda")
+        depth = torch.empty((H, W), dtype=torch.float32, device="cuda")
+        rgb = torch.empty((H, W, 3), dtype=torch.uint8, device="cuda")
+        tag = f"_{H}p" if H == 1080 else ""
+        entry("depth" + tag, W, H, timed(lambda s: disparity_to_depth_device(
+            disp.data_ptr(), W, H, 1400.0, 0.12, depth.data_ptr(), 0.0, s)), W * H * 6)
+        # depth + colour: fused (2 B in, 4 + 3 B out) against the two passes
+        entry("depth_color_fused" + tag, W, H, timed(lambda s: disparity_to_depth_color_device(
+            disp.data_ptr(), W, H, 1400.0, 0.12, depth.data_ptr(), rgb.data_ptr(), lut, 0.5, 10.0, 0.0, s)),
+            W * H * 9)
+
+        def two(s):
+            disparity_to_depth_device(disp.data_ptr(), W, H, 1400.0, 0.12, depth.data_ptr(), 0.0, s)
+            depth_colorize_device(depth.data_ptr(), W, H, rgb.data_ptr(), lut, 0.5, 10.0, s)
+        entry("depth_color_two_pass" + tag, W, H, timed(two), W * H * 9)
+        # point cloud: depth read twice (count, write), colours read, 16 B a point written
+        bgr = torch.randint(0, 256, (H, W, 3), dtype=torch.uint8, device="cuda")
+        pts = torch.empty((H * W * 16,), dtype=torch.uint8, device="cuda")
+        offs = torch.empty((H + 1,), dtype=torch.int32, device="cuda")
+        ms = timed(lambda s: depth_to_points_device(depth.data_ptr(), W, H, 1733.7, 1731.5, W / 2, H / 2,
+                                                    pts.data_ptr(), offs.data_ptr(), bgr.data_ptr(), s))
+        torch.cuda.synchronize()
+        n = int(offs[H].item())
+        entry("points" + tag, W, H, ms, W * H * (4 + 3) + n * 16)
+        res["points" + tag]["points"] = n
     W, H = 2880, 1988
     K = np.array([[1500.0, 0, 1440], [0, 1500.0, 994], [0, 0, 1]])
     R = np.eye(3)
     P = np.hstack([K, np.zeros((3, 1))])
     mx = torch.empty((H, W), dtype=torch.float32, device="cuda")
     my = torch.empty((H, W), dtype=torch.float32, device="cuda")
-    ms = timed(lambda: rectify_maps_device(K, [0.05, -0.01, 1e-4, -1e-4, 0.0], R, P, W, H, mx.data_ptr(),
-                                           my.data_ptr(), stream.cuda_stream))
-    res["maps"] = {"workload": f"{W}x{H}", "ms": ms, "gbs": W * H * 8 / ms / 1e6,
-                   "frac": W * H * 8 / ms / 1e6 / peak}
-    res["value"] = res["depth"]["gbs"]
+    entry("maps", W, H, timed(lambda s: rectify_maps_device(K, [0.05, -0.01, 1e-4, -1e-4, 0.0], R, P, W, H,
+                                                           mx.data_ptr(), my.data_ptr(), s)), W * H * 8)
+    res["value"] = res["depth_color_fused"]["gbs"]
     if rank == 0:
         print(json.dumps(res), flush=True)
 

@@ -207,6 +207,48 @@ lumen_status lumen_disparity_to_depth_device(const int16_t* d_disp, int width, i
                                              size_t disp_stride, float focal_px, float baseline,
                                              float disparity_offset_px, float* d_depth,
                                              size_t depth_stride, void* stream);
+/* The same conversion with a colour output in one pass (the reference runs
+ * disparityToDepthKernel, then colorizeDepthKernel on the stored depth,
+ * src/depth_map.cu:74-142): d_depth may be NULL when only the colours are
+ * wanted; d_rgb (3 bytes a pixel, NULL: none) gets the colours of
+ * lumen_depth_colorize_device.  `lut` is a HOST table of 256 channel triplets
+ * in output order (768 bytes). */
+lumen_status lumen_disparity_to_depth_color_device(const int16_t* d_disp, int width, int height,
+                                                   size_t disp_stride, float focal_px, float baseline,
+                                                   float disparity_offset_px, float* d_depth,
+                                                   size_t depth_stride, float min_depth,
+                                                   float max_depth, const uint8_t* lut, uint8_t* d_rgb,
+                                                   size_t rgb_stride, void* stream);
+/* colorizeDepthKernel (src/depth_map.cu:104-142): colour index 0 where
+ * z <= 0 or z > 2 max_depth, else (int)((1 - clamp((z - min) / (max - min),
+ * 0, 1)) * 255); each pixel gets lut[3 i .. 3 i + 2] (HOST table of 256
+ * triplets; the reference's is a Turbo-like ramp in RGB order). */
+lumen_status lumen_depth_colorize_device(const float* d_depth, int width, int height,
+                                         size_t depth_stride, float min_depth, float max_depth,
+                                         const uint8_t* lut, uint8_t* d_rgb, size_t rgb_stride,
+                                         void* stream);
+/* Point3D (include/stereo/point_cloud.h:17-25): 16 bytes, pad = 0. */
+typedef struct lumen_point3d {
+    float x, y, z;
+    uint8_t r, g, b, pad;
+} lumen_point3d;
+/* depthToPointCloud (src/point_cloud.cpp:11-55) on the device: every pixel
+ * with 0 < Z <= 100 (NaN kept, as in the reference) becomes the point
+ * ((float)((u - cx) Z / fx), (float)((v - cy) Z / fy), Z), computed in double,
+ * with the colour of d_bgr (BGR, 3 bytes a pixel, NULL: white), in raster
+ * order.  d_points: device room for width*height points, 16-byte aligned;
+ * d_row_offsets: device room for height + 1 ints, which receive row y's first
+ * point index at [y] and the number of points at [height].  Asynchronous. */
+lumen_status lumen_depth_to_points_device(const float* d_depth, int width, int height,
+                                          size_t depth_stride, const uint8_t* d_bgr, size_t bgr_stride,
+                                          double fx, double fy, double cx, double cy,
+                                          lumen_point3d* d_points, int* d_row_offsets, void* stream);
+/* depthToPointCloud (src/point_cloud.cpp:11-55) with HOST buffers: the same
+ * points as lumen_depth_to_points_device, `count` of them written to
+ * `points` (room for width*height).  Synchronous. */
+lumen_status lumen_depth_to_points(const float* depth, int width, int height, size_t depth_stride,
+                                   const uint8_t* bgr, size_t bgr_stride, double fx, double fy, double cx,
+                                   double cy, lumen_point3d* points, int* count);
 /* The CV_32FC1 maps cv::initUndistortRectifyMap produces for one camera
  * (src/calibration.cpp:253-266), generated on the device: K row-major 3x3,
  * dist = (k1, k2, p1, p2, k3) or NULL, R the rectifying rotation (3x3), P the

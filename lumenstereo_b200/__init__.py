@@ -544,6 +544,82 @@ def disparity_to_depth_device(disp_ptr: int, width: int, height: int, focal_px: 
                                                       disparity_offset_px, depth_ptr, 0, stream))
 
 
+def turbo_lut() -> np.ndarray:
+    """A 256 x 3 RGB colour table: OpenCV's COLORMAP_TURBO (the map the
+    reference's host colorizeDepth applies, src/depth_map.cu:189-203), taken
+    from cv2 at run time."""
+    import cv2
+    ramp = np.arange(256, dtype=np.uint8).reshape(256, 1)
+    return np.ascontiguousarray(cv2.applyColorMap(ramp, cv2.COLORMAP_TURBO).reshape(256, 3)[:, ::-1])
+
+
+def _lut_bytes(lut) -> np.ndarray:
+    t = np.ascontiguousarray(turbo_lut() if lut is None else lut, dtype=np.uint8)
+    if t.size != 768:
+        raise StereoException("colour table must hold 256 triplets")
+    return t.reshape(768)
+
+
+def disparity_to_depth_color_device(disp_ptr: int, width: int, height: int, focal_px: float, baseline: float,
+                                    depth_ptr: int, rgb_ptr: int, lut=None, min_depth: float = 0.5,
+                                    max_depth: float = 10.0, disparity_offset_px: float = 0.0,
+                                    stream: int = 0) -> None:
+    """disparityToDepthKernel + colorizeDepthKernel (src/depth_map.cu:74-142)
+    fused: packed device int16 disparity -> packed float32 depth (depth_ptr 0:
+    not stored) and packed 3-byte colours (rgb_ptr 0: none).  `lut`: 256 x 3
+    uint8 table (default turbo_lut())."""
+    t = _lut_bytes(lut) if rgb_ptr else None
+    _check(_lib.lib().lumen_disparity_to_depth_color_device(
+        disp_ptr, width, height, 0, focal_px, baseline, disparity_offset_px, depth_ptr or None, 0,
+        min_depth, max_depth, None if t is None else t.ctypes.data, rgb_ptr or None, 0, stream))
+
+
+def depth_colorize_device(depth_ptr: int, width: int, height: int, rgb_ptr: int, lut=None,
+                          min_depth: float = 0.5, max_depth: float = 10.0, stream: int = 0) -> None:
+    """colorizeDepthGPU (include/stereo/depth_map.h:53-56): packed device
+    float32 depth -> packed 3-byte colours through a 256 x 3 table."""
+    t = _lut_bytes(lut)
+    _check(_lib.lib().lumen_depth_colorize_device(depth_ptr, width, height, 0, min_depth, max_depth,
+                                                  t.ctypes.data, rgb_ptr, 0, stream))
+
+
+POINT_DTYPE = np.dtype([("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("r", "u1"), ("g", "u1"), ("b", "u1"),
+                        ("pad", "u1")])
+
+
+def depth_to_points_device(depth_ptr: int, width: int, height: int, fx: float, fy: float, cx: float,
+                           cy: float, points_ptr: int, row_offsets_ptr: int, bgr_ptr: int = 0,
+                           stream: int = 0) -> None:
+    """depthToPointCloud (src/point_cloud.cpp:11-55) on the device: packed
+    float32 depth (and packed BGR colours, 0: white) -> POINT_DTYPE records in
+    raster order at points_ptr (room for width*height, 16-byte aligned);
+    row_offsets_ptr receives height + 1 int32 offsets, the last one the
+    number of points."""
+    _check(_lib.lib().lumen_depth_to_points_device(depth_ptr, width, height, 0, bgr_ptr or None, 0, fx, fy,
+                                                   cx, cy, points_ptr, row_offsets_ptr, stream))
+
+
+def depth_to_point_cloud(depth: np.ndarray, K, color: np.ndarray = None) -> np.ndarray:
+    """depthToPointCloud(depth, color, params) (include/stereo/point_cloud.h:
+    39-43) with host arrays: float32 depth, K the 3x3 intrinsics (params.K0),
+    an optional BGR image used when its size matches.  Returns POINT_DTYPE
+    records in raster order (the reference's std::vector<Point3D>)."""
+    z = np.ascontiguousarray(depth, dtype=np.float32)
+    if z.ndim != 2:
+        raise StereoException("depth must be a one-channel image")
+    k = np.asarray(K, np.float64).reshape(3, 3)
+    h, w = z.shape
+    bgr = None
+    if color is not None and color.shape[:2] == z.shape and color.ndim == 3 and color.shape[2] == 3:
+        bgr = np.ascontiguousarray(color, dtype=np.uint8)
+    out = np.empty(h * w, POINT_DTYPE)
+    n = C.c_int(0)
+    _check(_lib.lib().lumen_depth_to_points(z.ctypes.data, w, h, 0, None if bgr is None else bgr.ctypes.data, 0,
+                                            k[0, 0], k[1, 1], k[0, 2], k[1, 2], out.ctypes.data,
+                                            C.byref(n)))
+    return out[:n.value].copy()
+
+
 def rectify_maps_device(K, dist, R, P, width: int, height: int, map_x_ptr: int, map_y_ptr: int,
                         stream: int = 0) -> None:
     """cv::initUndistortRectifyMap (CV_32FC1) for one camera, on the device."""

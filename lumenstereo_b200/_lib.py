@@ -107,6 +107,13 @@ def _declare(lib):
         "lumen_server_get_stats": (i, [vp, C.POINTER(CServerStats)]),
         "lumen_disparity_to_depth_device": (i, [vp, i, i, sz, C.c_float, C.c_float, C.c_float, vp, sz, vp]),
         "lumen_rectify_maps_device": (i, [vp, vp, vp, vp, i, i, vp, vp, vp]),
+        "lumen_disparity_to_depth_color_device": (i, [vp, i, i, sz, C.c_float, C.c_float, C.c_float, vp, sz,
+                                                      C.c_float, C.c_float, vp, vp, sz, vp]),
+        "lumen_depth_colorize_device": (i, [vp, i, i, sz, C.c_float, C.c_float, vp, vp, sz, vp]),
+        "lumen_depth_to_points_device": (i, [vp, i, i, sz, vp, sz, C.c_double, C.c_double, C.c_double,
+                                             C.c_double, vp, vp, vp]),
+        "lumen_depth_to_points": (i, [vp, i, i, sz, vp, sz, C.c_double, C.c_double, C.c_double, C.c_double, vp,
+                                      C.POINTER(C.c_int)]),
         "lumen_census_cost_noalloc": (i, [vp, vp, i, i, i, i, vp, i, vp]),
         "lumen_census_cost_noalloc_max_pixels": (sz, []),
     }

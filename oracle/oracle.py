@@ -217,6 +217,48 @@ def disparity_to_depth(disp: np.ndarray, focal: float, baseline: float, doffs: f
     return np.where((disp > 0) & (denom > 0), z, np.float32(0.0)).astype(np.float32)
 
 
+def depth_color_index(depth: np.ndarray, min_depth: float, max_depth: float) -> np.ndarray:
+    """colorizeDepthKernel's index (src/depth_map.cu:121-133) in IEEE float32:
+    0 for z <= 0 or z > 2 max, else int((1 - clamp((z - min)/(max - min))) * 255)
+    with C's fminf/fmaxf NaN rules."""
+    z = depth.astype(np.float32)
+    lo, hi = np.float32(min_depth), np.float32(max_depth)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        n = (z - lo) / (hi - lo)
+    n = np.fmax(np.float32(0), np.fmin(np.float32(1), n))
+    n = np.float32(1) - n
+    idx = (n * np.float32(255)).astype(np.int32)
+    bad = (z <= 0) | (z > hi * np.float32(2))
+    return np.where(bad, 0, idx).astype(np.int32)
+
+
+def depth_color_ramp(depth: np.ndarray, min_depth: float, max_depth: float) -> np.ndarray:
+    """The pre-truncation value (1 - clamp(...)) * 255 of depth_color_index,
+    float64, for locating pixels that sit on an index boundary."""
+    z = depth.astype(np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        n = (z - min_depth) / (max_depth - min_depth)
+    return (1.0 - np.fmax(0.0, np.fmin(1.0, n))) * 255.0
+
+
+def depth_to_point_cloud(depth: np.ndarray, bgr, fx: float, fy: float, cx: float, cy: float):
+    """depthToPointCloud (src/point_cloud.cpp:11-55): pixels with 0 < Z <= 100
+    (NaN kept) in raster order, X = (float)((u - cx) Z / fx), Y likewise in v,
+    both in float64; colour (r, g, b) from a BGR image of the same size, else
+    white.  Returns (xyz float32 [n, 3], rgb uint8 [n, 3])."""
+    z = depth.astype(np.float32)
+    keep = ~((z <= 0) | (z > np.float32(100)))
+    v, u = np.nonzero(keep)                  # raster order
+    Z = z[v, u]
+    X = ((u.astype(np.float64) - cx) * Z.astype(np.float64) / fx).astype(np.float32)
+    Y = ((v.astype(np.float64) - cy) * Z.astype(np.float64) / fy).astype(np.float32)
+    if bgr is not None and bgr.shape[:2] == depth.shape:
+        rgb = bgr[v, u][:, ::-1].astype(np.uint8)
+    else:
+        rgb = np.full((len(Z), 3), 255, np.uint8)
+    return np.stack([X, Y, Z], axis=1), np.ascontiguousarray(rgb)
+
+
 def rectify_maps(K, dist, R, P, width: int, height: int):
     """The maps of cv::initUndistortRectifyMap (CV_32FC1), restated in float64
     numpy from the published pinhole + Brown-Conrady model: the ray
