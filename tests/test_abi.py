@@ -63,3 +63,33 @@ def test_null_arguments_are_invalid():
     assert lib.lumen_sgbm_set_params(None, None) == _lib.ERR_INVALID_ARGUMENT
     assert lib.lumen_sgbm_destroy(None) == _lib.OK
     assert "NULL" in _lib.last_error() or _lib.last_error() == ""
+
+
+def test_depth_entry_points_check_arguments_before_the_device():
+    """Argument errors of the depth / colour / point-cloud entry points are
+    reported before any CUDA call (so they hold without a device too)."""
+    lib = _lib.lib()
+    bad = _lib.ERR_INVALID_ARGUMENT
+    fake = 1 << 20                       # never dereferenced: the checks fail first
+    lut = (C.c_uint8 * 768)()
+    # no output at all / NULL input / empty size
+    assert lib.lumen_disparity_to_depth_color_device(fake, 4, 4, 0, 1.0, 1.0, 0.0, None, 0, 0.5, 10.0, lut,
+                                                     None, 0, None) == bad
+    assert lib.lumen_disparity_to_depth_device(None, 4, 4, 0, 1.0, 1.0, 0.0, fake, 0, None) == bad
+    assert lib.lumen_disparity_to_depth_device(fake, 0, 4, 0, 1.0, 1.0, 0.0, fake, 0, None) == bad
+    # colours without a table; strides below the packed row or not a multiple of the element
+    assert lib.lumen_disparity_to_depth_color_device(fake, 4, 4, 0, 1.0, 1.0, 0.0, None, 0, 0.5, 10.0, None,
+                                                     fake, 0, None) == bad
+    assert lib.lumen_disparity_to_depth_device(fake, 4, 4, 6, 1.0, 1.0, 0.0, fake, 0, None) == bad
+    assert lib.lumen_disparity_to_depth_device(fake, 4, 4, 9, 1.0, 1.0, 0.0, fake, 0, None) == bad
+    assert lib.lumen_depth_colorize_device(fake, 4, 4, 0, 0.5, 10.0, lut, fake, 11, None) == bad
+    assert lib.lumen_depth_colorize_device(fake, 4, 4, 0, 0.5, 10.0, None, fake, 0, None) == bad
+    # points: unaligned record buffer, missing offsets, bad colour stride
+    pts = fake + 8
+    assert lib.lumen_depth_to_points_device(fake, 4, 4, 0, None, 0, 1.0, 1.0, 0.0, 0.0, pts, fake, None) == bad
+    assert lib.lumen_depth_to_points_device(fake, 4, 4, 0, None, 0, 1.0, 1.0, 0.0, 0.0, fake, None, None) == bad
+    assert lib.lumen_depth_to_points_device(fake, 4, 4, 0, fake, 5, 1.0, 1.0, 0.0, 0.0, fake, fake, None) == bad
+    n = C.c_int(-1)
+    assert lib.lumen_depth_to_points(None, 4, 4, 0, None, 0, 1.0, 1.0, 0.0, 0.0, fake, C.byref(n)) == bad
+    assert n.value == -1
+    assert "stride" in _lib.last_error() or "NULL" in _lib.last_error()
