@@ -105,13 +105,14 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(workload: str):
-    """DRAM bytes per pixel-disparity of the aggregation stage from the ncu
-    summary committed under profiles/ (None when absent)."""
+def profiled_traffic(workload: str, schedule: int):
+    """DRAM bytes per pixel-disparity of the aggregation stage of `schedule` on
+    `workload` from the ncu summary committed under profiles/ (None when that
+    kernel has no capture)."""
     path = os.path.join(ROOT, "profiles", "dram_traffic.json")
     try:
         with open(path) as f:
-            return json.load(f).get(workload)
+            return json.load(f).get(f"{workload}/schedule{schedule}")
     except Exception:
         return None
 
@@ -325,7 +326,7 @@ def run_ours(args):
     agg_mean = statistics.mean(agg_ms)
     agg_bytes = (P + 2) * pd_per_step          # cost read once per path + agg written once
     achieved = agg_bytes / (agg_mean / 1e3) / 1e9
-    traffic_per_pd = profiled_traffic(args.workload)
+    traffic_per_pd = profiled_traffic(args.workload, tuning[0])
     pipe_ms = statistics.mean(step_ms)
     pipe_bytes = (P + 5) * pd_per_step         # SGM core model: cost w + P reads, agg w + r
     result = {

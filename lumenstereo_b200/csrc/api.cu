@@ -72,6 +72,7 @@ struct lumen_sgbm {
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     DevBuf inL, inR, gray[2], pref[2], census[2], cost, agg, dispL, dispR, out, dbgLR, magic;
     DevBuf partB, xring, counters, status;  // sweep schedule: backward partial, exchange rings
+    DevBuf partC, partD;                    // schedule 6: the column sweeps' partials
     DevBuf trace;                           // lumen_sgbm_debug_trace: band timeline of schedule 4
     int traceOn = 0;
     size_t traceWords = 0;
@@ -173,8 +174,8 @@ extern "C" lumen_status lumen_sgbm_destroy(lumen_sgbm* h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (DevBuf* b : {&h->inL, &h->inR, &h->gray[0], &h->gray[1], &h->pref[0], &h->pref[1],
                       &h->census[0], &h->census[1], &h->cost, &h->agg, &h->dispL, &h->dispR,
-                      &h->out, &h->dbgLR, &h->magic, &h->partB, &h->xring, &h->counters,
-                      &h->status, &h->trace})
+                      &h->out, &h->dbgLR, &h->magic, &h->partB, &h->partC, &h->partD, &h->xring,
+                      &h->counters, &h->status, &h->trace})
         b->release();
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
@@ -281,8 +282,8 @@ extern "C" lumen_status lumen_sgbm_debug_set_paths(lumen_sgbm* h, uint32_t mask)
 
 extern "C" lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule) {
     if (!h) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL handle");
-    if (schedule < 0 || schedule > 5)
-        return fail(LUMEN_ERR_INVALID_ARGUMENT, "schedule must be 0, 1, 2, 3, 4 or 5");
+    if (schedule < 0 || schedule > 6)
+        return fail(LUMEN_ERR_INVALID_ARGUMENT, "schedule must be 0, 1, 2, 3, 4, 5 or 6");
     h->schedule = schedule;
     return LUMEN_OK;
 }
@@ -458,8 +459,15 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
             cfgChosen = true;
         }
     }
-    if (sched == 0) sched = sweepable ? 4 : 1;
+    // untuned default: the four lag-free sweeps for 8 paths (schedule 6, which
+    // falls back to schedule 4 where it has no instance), schedule 4 for 4 paths
+    if (sched == 0) sched = mask == 0xFFu ? 6 : (sweepable ? 4 : 1);
     if (sched >= 2 && !sweepable) sched = 1;          // single-path debug masks: per-direction kernels
+    PairPlan plan6{};
+    if (sched == 6 && (mask != 0xFFu || pair_plan(k, wrap, h->numSMs, &plan6) != cudaSuccess)) {
+        sched = 4;                                     // 4 paths, or no instance for this range
+        if (!h->forced.T) cfgChosen = false;
+    }
     WavePlan plan4{};
     if (sched == 5) {
         // row bands in thread-block clusters: the largest cluster that plans
@@ -510,7 +518,31 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
     }
     if (sched == 2 && !sweep_fits(W, Dp, cfg)) sched = 1;  // very wide images: per-direction kernels
     const uint16_t* aggB = nullptr;
-    if (sched == 4 || sched == 5) {
+    const uint16_t* aggC = nullptr;
+    const uint16_t* aggD = nullptr;
+    if (sched == 6) {
+        LCU(h->partB.ensure(ND * 2));
+        LCU(h->partC.ensure(ND * 2));
+        LCU(h->partD.ensure(ND * 2));
+        LCU(h->xring.ensure(plan6.xbufBytes));
+        LCU(h->counters.ensure(sizeof(unsigned) * plan6.counterWords));
+        uint16_t* const parts[4] = {h->agg.as<uint16_t>(), h->partB.as<uint16_t>(), h->partC.as<uint16_t>(),
+                                    h->partD.as<uint16_t>()};
+        LCU(launch_aggregate_pair(pv, parts, k, wrap, plan6, h->xring.as<uint8_t>(), h->counters.as<unsigned>(),
+                                  h->status.as<int>(), h->spinMax, s, h->stallTest));
+        h->statusPending = true;
+        nl += 1;
+        cfg = SweepConfig{plan6.T, plan6.R};
+        aggB = parts[1];
+        aggC = parts[2];
+        aggD = parts[3];
+        if (h->retain || select_needs_summed_volume(D, Dp)) {
+            for (int i = 1; i < 4; ++i) launch_sum_volumes(parts[0], parts[i], parts[0], ND, s);
+            LCU(cudaGetLastError());
+            nl += 3;
+            aggB = aggC = aggD = nullptr;
+        }
+    } else if (sched == 4 || sched == 5) {
         LCU(h->partB.ensure(ND * 2));
         LCU(h->xring.ensure(plan4.ringBytes));
         LCU(h->counters.ensure(sizeof(unsigned) * plan4.counterWords));
@@ -580,7 +612,7 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
     if (timed) LCU(cudaEventRecord(h->ev[3], s));
     // selection + post-processing
     LCU(launch_select(h->agg.as<uint16_t>(), aggB, wrap, W, H, D, Dp, p.minDisparity,
-                      p.uniquenessRatio, h->dispL.as<int16_t>(), h->dispR.as<int16_t>(), s));
+                      p.uniquenessRatio, h->dispL.as<int16_t>(), h->dispR.as<int16_t>(), s, aggC, aggD));
     const int lr = p.disp12MaxDiff >= 0 ? p.disp12MaxDiff * 16 : -1;
     const int spk = p.speckleWindowSize > 0 ? std::min(p.speckleWindowSize, 25) : 0;
     LCU(launch_post(h->dispL.as<int16_t>(), h->dispR.as<int16_t>(), W, H, lr, spk,
@@ -686,6 +718,7 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
             cands.push_back({4, SweepConfig{tl, 32}});
         }
         for (int i = 0; i < nw; ++i) cands.push_back({5, SweepConfig{32, rs[i]}});
+        if (mask == 0xFFu) cands.push_back({6, SweepConfig{0, 0}});
     }
     const SweepConfig savedForced = h->forced;
     const int savedSched = h->schedule;

@@ -121,10 +121,28 @@ cudaError_t launch_aggregate_wave(const PairView& pv, uint16_t* partB, const Sgm
                                   cudaStream_t s, int stallTest = 0,
                                   unsigned long long* trace = nullptr);
 
-// aggB (nullable): second partial volume summed with agg (mod 2^16 when wrap).
+// ---- schedule 6: four lag-free two-path sweeps (pair.cu, pair_kernel.cuh) ----
+struct PairPlan {
+    int R, T;              // rows per band, lanes per row
+    int nb0, nb1;          // bands of the row sweeps, of the column sweeps
+    int nTickets;          // 2 * nb0 + 2 * nb1
+    int grid;              // CTAs launched (persistent, ticket-scheduled)
+    int smem;              // dynamic shared memory per CTA
+    size_t xbufBytes;      // band-boundary row buffers, all sweeps
+    size_t counterWords;   // progress per band + ticket
+};
+// cudaErrorInvalidValue: no instance for these disparities / sizes
+cudaError_t pair_plan(const SgmConsts& k, bool wrap, int numSMs, PairPlan* plan);
+// part[0..3]: the four sweeps' partial volumes (part[0] may be pv.agg)
+cudaError_t launch_aggregate_pair(const PairView& pv, uint16_t* const part[4], const SgmConsts& k, bool wrap,
+                                  const PairPlan& plan, uint8_t* xbuf, unsigned* counters, int* status,
+                                  long long spinMax, cudaStream_t s, int stallTest = 0);
+
+// aggB (nullable): second partial volume summed with agg (mod 2^16 when wrap);
+// aggC, aggD (nullable, both or neither): two more (schedule 6).
 cudaError_t launch_select(const uint16_t* agg, const uint16_t* aggB, bool wrap, int W, int H,
                           int D, int Dp, int minD, int UR, int16_t* dispL, int16_t* dispR,
-                          cudaStream_t s);
+                          cudaStream_t s, const uint16_t* aggC = nullptr, const uint16_t* aggD = nullptr);
 bool select_needs_summed_volume(int D, int Dp);
 // dst = a + b (mod 2^16 per element), n uint16 elements (n even).
 void launch_sum_volumes(const uint16_t* a, const uint16_t* b, uint16_t* dst, size_t n,

@@ -1,0 +1,89 @@
+// pair.cu -- host side of schedule 6 (four lag-free two-path sweeps,
+// pair_kernel.cuh): instance choice, shared-memory fit, buffers, launch.
+#include <algorithm>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "pair_kernel.cuh"
+
+namespace lumen {
+
+extern template cudaError_t pair_launch_t<4, 8>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
+extern template cudaError_t pair_launch_t<8, 8>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
+extern template cudaError_t pair_launch_t<6, 16>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
+extern template cudaError_t pair_launch_t<8, 16>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
+extern template cudaError_t pair_launch_t<10, 16>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
+
+constexpr int kPairRows = 16;
+
+// lanes per row for a padded disparity count (0: no instance)
+static int pair_lanes(int Dp) { return Dp <= 128 ? 8 : Dp <= 320 ? 16 : 0; }
+
+static cudaError_t pair_dispatch(const PairArgs& a, int Dp, bool wrap, bool full, int smem, int grid,
+                                 cudaStream_t s, int* perSM) {
+    switch (Dp) {
+    case 64: return pair_launch_t<4, 8>(a, wrap, full, smem, grid, s, perSM);
+    case 128: return pair_launch_t<8, 8>(a, wrap, full, smem, grid, s, perSM);
+    case 192: return pair_launch_t<6, 16>(a, wrap, full, smem, grid, s, perSM);
+    case 256: return pair_launch_t<8, 16>(a, wrap, full, smem, grid, s, perSM);
+    case 320: return pair_launch_t<10, 16>(a, wrap, full, smem, grid, s, perSM);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t pair_plan(const SgmConsts& k, bool wrap, int numSMs, PairPlan* plan) {
+    if (!pair_lanes(k.Dp)) return cudaErrorInvalidValue;
+    const int R = kPairRows;
+    PairPlan p{};
+    p.R = R;
+    p.T = pair_lanes(k.Dp);
+    p.nb0 = (k.H + R - 1) / R;
+    p.nb1 = (k.W + R - 1) / R;
+    p.nTickets = 2 * p.nb0 + 2 * p.nb1;
+    p.smem = pair_smem(std::max(k.W, k.H), k.Dp, R).total;
+    if (p.smem > 227 * 1024) return cudaErrorInvalidValue;
+    PairArgs dummy{};
+    int perSM = 0;
+    cudaError_t e = pair_dispatch(dummy, k.Dp, wrap, k.D == k.Dp, p.smem, 0, nullptr, &perSM);
+    if (e != cudaSuccess) return e;
+    if (perSM < 1) return cudaErrorInvalidConfiguration;
+    p.grid = std::min(p.nTickets, perSM * numSMs);
+    p.xbufBytes = pair_xbase(3, p.nb1, k.W, k.H, p.nb0, p.nb1) * (size_t)pair_slot_bytes(k.Dp);
+    p.counterWords = (size_t)pair_poff(3, p.nb0, p.nb1) + p.nb1 + 1;   // progress per band + ticket
+    *plan = p;
+    return cudaSuccess;
+}
+
+cudaError_t launch_aggregate_pair(const PairView& pv, uint16_t* const part[4], const SgmConsts& k, bool wrap,
+                                  const PairPlan& plan, uint8_t* xbuf, unsigned* counters, int* status,
+                                  long long spinMax, cudaStream_t s, int stallTest) {
+    PairArgs a{};
+    PairJob& J = a.job;
+    J.cost = pv.cost;
+    J.img = pv.img;
+    for (int i = 0; i < 4; ++i) J.part[i] = part[i];
+    J.xbuf = xbuf;
+    J.prod = counters;
+    J.W = k.W;
+    J.H = k.H;
+    J.D = k.D;
+    J.nb[0] = plan.nb0;
+    J.nb[1] = plan.nb1;
+    J.P1 = k.P1;
+    J.P2 = k.P2;
+    J.costScale = k.costScale;
+    J.p1x2 = k.p1x2;
+    J.bsub = k.bsub;
+    a.nTickets = plan.nTickets;
+    a.Lmax = std::max(k.W, k.H);
+    a.ticket = counters + plan.counterWords - 1;
+    a.status = status;
+    a.spinMax = spinMax;
+    a.stallTest = stallTest;
+    cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned) * plan.counterWords, s);
+    if (e != cudaSuccess) return e;
+    int perSM = 0;
+    return pair_dispatch(a, k.Dp, wrap, k.D == k.Dp, plan.smem, plan.grid, s, &perSM);
+}
+
+}  // namespace lumen

@@ -1,0 +1,380 @@
+// pair_kernel.cuh -- SGM aggregation as four lag-free sweeps (schedule 6).
+//
+// The eight path kernels of the reference (src/sgbm_kernels.cu:315-742) regroup
+// into four sweeps of two paths each: one horizontal path of the sweep and the
+// one diagonal that runs the same way.  In sweep coordinates (u along a sweep
+// row, v across rows) both paths of a pixel (u, v) come from pixel u-1:
+//   sweep 0  rows top-down,     pixels left-to-right   LR   (u-1, v)  TLBR (u-1, v-1)
+//   sweep 1  rows bottom-up,    pixels right-to-left   RL              BRTL
+//   sweep 2  columns right-to-left, pixels top-down    TB              TRBL
+//   sweep 3  columns left-to-right, pixels bottom-up   BT              BLTR
+// with (x, y) = (u, v), (W-1-u, H-1-v), (W-1-v, u), (v, H-1-u).  Sweeps 2 and
+// 3 run over the columns of the image: their "rows" are image columns.
+//
+// Because row v needs only pixel u-1 of row v-1, all rows of a band handle
+// the same pixel at the same step (no lag between rows): a band of R rows
+// spans its row length in steps, and the next band trails it by one
+// hand-off, so a sweep spans about len + bands * hand-off steps instead of
+// the W + 2H of a sweep that also carries TRBL.
+//
+// Work decomposition:
+//  * a CTA owns a band of R consecutive sweep rows, each row a team of T
+//    lanes (a lane holds 2*KW disparities as KW packed uint16x2 words); all
+//    rows advance in lockstep, one barrier per step;
+//  * row r reads row r-1's diagonal vector of pixel u-1 from a two-slot
+//    shared-memory ring written one step earlier;
+//  * the band's first row reads the band above's last row from a per-boundary
+//    row buffer in global memory: the producing row stores every pixel's
+//    vector there and publishes its progress every kPE pixels (release at
+//    GPU scope); the consuming row waits for pixel u (acquire, every lane)
+//    and loads it during step u for use at step u+1, so the load overlaps a
+//    step.  The row buffers hold whole rows, so a band never waits on the
+//    band below it: bands only depend on earlier tickets and any number of
+//    resident CTAs makes progress;
+//  * matching costs are prefetched kPPF-1 pixels ahead with cp.async;
+//    adaptive P2 is looked up from staged image rows;
+//  * bands are handed out by a ticket counter, the four sweeps interleaved,
+//    each sweep's bands in order.
+// Every wait is bounded: on timeout the CTA records LUMEN_ERR_TIMEOUT in
+// *status and stops; CTAs that see a non-zero status stop taking bands.
+#pragma once
+
+#include "wave_kernel.cuh"
+
+namespace lumen {
+
+constexpr int kPPF = 8;    // per-row cost ring (pixels); kPPF-1 prefetched ahead
+constexpr int kPE = 4;     // a band's last row publishes its progress every kPE pixels
+
+struct PairJob {
+    const uint8_t* cost;     // [H][W][Dp]
+    const uint8_t* img;      // [H][W] left gray image (adaptive P2)
+    uint16_t* part[4];       // per-sweep partial sums, [H][W][Dp]
+    uint8_t* xbuf;           // band-boundary rows (pair_xbase), kPairSlot(Dp) bytes a pixel
+    unsigned* prod;          // [pair_poff(4)] pixels of band b's last row published
+    int W, H, D;
+    int nb[2];               // bands of the row sweeps (0, 1) and of the column sweeps (2, 3)
+    int P1, P2, costScale;
+    uint32_t p1x2, bsub;
+};
+
+struct PairArgs {
+    PairJob job;
+    int nTickets;            // 2 * nb[0] + 2 * nb[1]
+    int Lmax;                // max(W, H): staged image row length
+    unsigned* ticket;
+    int* status;
+    long long spinMax;
+    int stallTest;           // 1: ticket 4 (band 1 of sweep 0) waits on a pixel never published
+};
+
+__host__ __device__ constexpr int pair_slot_bytes(int Dp) { return 2 * Dp + 16; }
+
+struct PairSmem {
+    int img, cost, slots, zero, lut, misc, total, Lp;
+};
+__host__ __device__ inline PairSmem pair_smem(int Lmax, int Dp, int R) {
+    PairSmem s;
+    s.Lp = (Lmax + 15) & ~15;
+    const int SB = pair_slot_bytes(Dp);
+    int o = 0;
+    s.img = o;
+    o += (R + 1) * s.Lp;
+    o = (o + 127) & ~127;
+    s.cost = o;
+    o += R * kPPF * Dp;
+    s.slots = o;
+    o += R * 2 * SB;
+    s.zero = o;   // all-zero slot: a path that starts reads it (L' = 0, min L' = 0 gives L = C)
+    o += SB;
+    s.lut = o;
+    o += 256 * 4;
+    s.misc = o;
+    o += 32 * 4;
+    s.total = o;
+    return s;
+}
+
+// sweep s, sweep coordinates (u, v) -> image (x, y)
+__host__ __device__ __forceinline__ void pair_xy(int s, int u, int v, int W, int H, int& x, int& y) {
+    if (s == 0) { x = u; y = v; }
+    else if (s == 1) { x = W - 1 - u; y = H - 1 - v; }
+    else if (s == 2) { x = W - 1 - v; y = u; }
+    else { x = v; y = H - 1 - u; }
+}
+
+// ticket -> (sweep, band): the four sweeps round-robin while all have bands
+// left, then the two sweeps with more bands alternate; every band comes
+// after the band before it in its own sweep.
+__host__ __device__ __forceinline__ void pair_ticket(int t, int nb0, int nb1, int& s, int& b) {
+    const int m = nb0 < nb1 ? nb0 : nb1;
+    if (t < 4 * m) {
+        s = t & 3;
+        b = t >> 2;
+        return;
+    }
+    const int t2 = t - 4 * m;
+    s = (nb0 > nb1 ? 0 : 2) + (t2 & 1);
+    b = m + (t2 >> 1);
+}
+
+// first pixel (in slots) of the row buffer of sweep s, boundary b (the last row of band b)
+__host__ __device__ __forceinline__ size_t pair_xbase(int s, int b, int W, int H, int nb0, int nb1) {
+    const size_t rows = (size_t)nb0 * W;
+    if (s == 0) return (size_t)b * W;
+    if (s == 1) return rows + (size_t)b * W;
+    if (s == 2) return 2 * rows + (size_t)b * H;
+    return 2 * rows + (size_t)nb1 * H + (size_t)b * H;
+}
+__host__ __device__ __forceinline__ int pair_poff(int s, int nb0, int nb1) {
+    return s < 2 ? s * nb0 : 2 * nb0 + (s - 2) * nb1;
+}
+
+// Bounded wait (whole warp) until the global counter *p >= need; every lane
+// acquires its own sufficient value, so each lane's later loads of the data
+// the counter publishes are ordered after it.
+__device__ __forceinline__ bool p_wait_gpu(const unsigned* p, unsigned need, unsigned& cache,
+                                           volatile int* abortFlag, int* status, long long spinMax) {
+    if (cache >= need) return true;
+    long long k = 0;
+    for (;;) {
+        const unsigned v = w_ld_acquire_gpu(p);
+        if (__all_sync(kFullMask, v >= need)) {
+            cache = __shfl_sync(kFullMask, v, 0);
+            return true;
+        }
+        if (__shfl_sync(kFullMask, *abortFlag, 0)) return false;
+        if ((k & 63) == 63 && __shfl_sync(kFullMask, *(volatile int*)status, 0) != 0) {
+            *abortFlag = 1;
+            return false;
+        }
+        if (++k >= spinMax) {
+            if ((threadIdx.x & 31) == 0) atomicExch(status, (int)LUMEN_ERR_TIMEOUT);
+            *abortFlag = 1;
+            return false;
+        }
+        __nanosleep(32);
+    }
+}
+
+template <int KW, bool WRAP, bool FULL, int R, int T>
+__global__ void __launch_bounds__(R / (32 / T) * 32)
+pair_kernel(PairArgs a) {
+    constexpr int DP = 2 * KW * T;       // padded disparities
+    constexpr int SB = pair_slot_bytes(DP);
+    constexpr int RPW = 32 / T;          // rows per warp
+    static_assert(R % RPW == 0, "whole warps of rows");
+    constexpr int RW = R / RPW;          // warps
+    static_assert(KW % 2 == 0, "a lane's cost bytes are whole 4-byte words");
+    extern __shared__ __align__(128) uint8_t sm[];
+    const PairSmem L = pair_smem(a.Lmax, DP, R);
+    uint8_t* simg = sm + L.img;
+    const uint32_t* p2lut = reinterpret_cast<const uint32_t*>(sm + L.lut);
+    // [0] ticket, [1] abort
+    volatile int* sflag = reinterpret_cast<volatile int*>(sm + L.misc);
+    const uint8_t* const zeroSlot = sm + L.zero;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tl = lane & (T - 1);      // lane within the row's team
+    const int off = tl * 2 * KW;        // first disparity of this lane
+    const int r = warp * RPW + lane / T;
+    const PairJob& J = a.job;
+    const int W = J.W, H = J.H;
+
+    for (int i = threadIdx.x; i < SB / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(sm + L.zero)[i] = 0u;
+    // adaptive P2 (src/sgbm_kernels.cu:301-310) as a table of |dI|, replicated in both halves
+    for (int g = threadIdx.x; g < 256; g += blockDim.x)
+        reinterpret_cast<uint32_t*>(sm + L.lut)[g] =
+            ((uint32_t)max(J.P1 + 1, J.P2 * 8 / max(8, g)) & 0xFFFFu) * 0x10001u;
+    LaneMasks<KW> mk;
+    make_lane_masks<KW>(tl, J.D, mk);
+    __syncthreads();
+
+    for (;;) {
+        if (threadIdx.x == 0) {
+            int t = (int)atomicAdd(a.ticket, 1u);
+            if (*(volatile int*)a.status != 0) t = a.nTickets;
+            sflag[0] = t;
+            sflag[1] = 0;
+        }
+        __syncthreads();
+        const int t = sflag[0];
+        if (t >= a.nTickets) break;
+        int s, b;
+        pair_ticket(t, J.nb[0], J.nb[1], s, b);
+        const bool tr = s >= 2;
+        const int Ws = tr ? H : W, Hs = tr ? W : H;
+        const int nbS = tr ? J.nb[1] : J.nb[0];
+        const int v0 = b * R;
+        const int lastActive = min(R - 1, Hs - 1 - v0);
+        const bool hasPrev = b > 0, hasNext = b + 1 < nbS;
+        // ---- stage sweep rows v0-1 .. v0+R-1 of the image (column sweeps: row index fastest) ----
+        for (int i = threadIdx.x; i < (R + 1) * Ws; i += blockDim.x) {
+            int rr, u;
+            if (tr) { rr = i % (R + 1); u = i / (R + 1); }
+            else { rr = i / Ws; u = i - rr * Ws; }
+            const int vv = v0 - 1 + rr;
+            uint8_t val = 0;
+            if (vv >= 0 && vv < Hs) {
+                int x, y;
+                pair_xy(s, u, vv, W, H, x, y);
+                val = J.img[(size_t)y * W + x];
+            }
+            simg[rr * L.Lp + u] = val;
+        }
+        __syncthreads();
+
+        const bool rowOn = r <= lastActive;
+        const int v = v0 + min(r, lastActive);
+        int x0, y0;
+        pair_xy(s, 0, v, W, H, x0, y0);
+        const ptrdiff_t du = s == 0 ? 1 : s == 1 ? -1 : s == 2 ? (ptrdiff_t)W : -(ptrdiff_t)W;
+        const ptrdiff_t pix0 = (ptrdiff_t)y0 * W + x0;
+        uint16_t* const part = s == 0 ? J.part[0] : s == 1 ? J.part[1] : s == 2 ? J.part[2] : J.part[3];
+        uint16_t* pout = part + pix0 * DP + off;
+        const ptrdiff_t pstep = du * DP;
+        uint8_t* const costRing = sm + L.cost + r * kPPF * DP;
+        const uint8_t* irow = simg + (r + 1) * L.Lp;
+        const uint8_t* iprev = simg + r * L.Lp;
+        uint8_t* const mySlots = sm + L.slots + r * 2 * SB;
+        const uint8_t* const upSlots = sm + L.slots + (r > 0 ? r - 1 : 0) * 2 * SB;
+        const bool exporter = rowOn && r == lastActive && hasNext;
+        const bool warpExports = hasNext && warp == lastActive / RPW;
+        const bool warpImports = hasPrev && warp == 0;   // row 0 is in warp 0
+        uint8_t* const xout = hasNext ? J.xbuf + pair_xbase(s, b, W, H, J.nb[0], J.nb[1]) * SB : nullptr;
+        const uint8_t* const xin = hasPrev ? J.xbuf + pair_xbase(s, b - 1, W, H, J.nb[0], J.nb[1]) * SB : nullptr;
+        unsigned* const prodOut = J.prod + pair_poff(s, J.nb[0], J.nb[1]) + b;
+        const unsigned* const prodIn = J.prod + pair_poff(s, J.nb[0], J.nb[1]) + (b > 0 ? b - 1 : 0);
+        const unsigned stallNeed = (a.stallTest && t == 4) ? (unsigned)Ws + 1u : 0u;
+
+        auto prefetch = [&](int step) {
+            const int p = step + kPPF - 1;
+            if (rowOn && p >= 0 && p < Ws) {
+                const uint8_t* src = J.cost + (pix0 + (ptrdiff_t)p * du) * DP + off;
+                const uint32_t dst = w_smem_addr(costRing + (p % kPPF) * DP + off);
+                if constexpr ((2 * KW) % 16 == 0) {
+#pragma unroll
+                    for (int q = 0; q < (2 * KW) / 16; ++q) w_cp_async16(dst + 16 * q, src + 16 * q);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < KW / 2; ++q)
+                        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst + 4 * q),
+                                     "l"(src + 4 * q)
+                                     : "memory");
+                }
+            }
+            w_cp_commit();
+        };
+        for (int st = -(kPPF - 1); st < 0; ++st) prefetch(st);
+
+        uint32_t LH[KW], imp[KW];
+#pragma unroll
+        for (int w = 0; w < KW; ++w) { LH[w] = 0; imp[w] = 0; }
+        uint32_t minH = 0, impMin = 0;
+        unsigned seen = 0;
+        bool ok = true;
+        for (int u = 0; u < Ws; ++u) {
+            // ---- the band above's pixel u-1 (loaded last step); load pixel u for the next step ----
+            uint32_t pred[KW];
+#pragma unroll
+            for (int w = 0; w < KW; ++w) pred[w] = imp[w];
+            const uint32_t predMin = impMin;
+            if (warpImports && u + 1 < Ws) {
+                ok = ok && p_wait_gpu(prodIn, stallNeed ? stallNeed : (unsigned)(u + 1), seen, sflag + 1,
+                                      a.status, a.spinMax);
+                if (ok && r == 0) {
+                    const uint8_t* src = xin + (size_t)u * SB;
+                    load_words<KW>(reinterpret_cast<const uint16_t*>(src) + off, imp);
+                    impMin = *reinterpret_cast<const uint32_t*>(src + 2 * DP);
+                }
+            }
+            // ---- cost of this step's pixel ----
+            prefetch(u);
+            w_cp_wait<kPPF - 1>();
+            uint32_t Cw[KW];
+            load_cost_words<KW>(costRing + (u % kPPF) * DP + off, Cw);
+            if (WRAP || J.costScale != 1) {
+#pragma unroll
+                for (int w = 0; w < KW; ++w) Cw[w] = scale_cost<WRAP>(Cw[w], J.costScale);
+            }
+            // ---- adaptive P2: horizontal predecessor (u-1, v), diagonal (u-1, v-1) ----
+            const int um = max(u - 1, 0);
+            const int cur = irow[u];
+            const uint32_t p2h = p2lut[abs(cur - irow[um])];
+            const uint32_t p2d = p2lut[abs(cur - iprev[um])];
+            // ---- horizontal path (its state starts at 0: L = C at u = 0) ----
+            uint32_t LnH[KW];
+            wave_step<KW, T, WRAP, FULL>(LH, Cw, minH, p2h, J.p1x2, J.bsub, mk, LnH);
+            // ---- diagonal path from the row above, pixel u-1 ----
+            uint32_t Lp[KW], mp;
+            if (u == 0 || v == 0) {
+                load_words<KW>(reinterpret_cast<const uint16_t*>(zeroSlot) + off, Lp);
+                mp = 0u;
+            } else if (r == 0) {
+#pragma unroll
+                for (int w = 0; w < KW; ++w) Lp[w] = pred[w];
+                mp = predMin;
+            } else {
+                const uint8_t* slot = upSlots + ((u - 1) & 1) * SB;
+                load_words<KW>(reinterpret_cast<const uint16_t*>(slot) + off, Lp);
+                mp = *reinterpret_cast<const uint32_t*>(slot + 2 * DP);
+            }
+            uint32_t LnD[KW];
+            wave_step<KW, T, WRAP, FULL>(Lp, Cw, mp, p2d, J.p1x2, J.bsub, mk, LnD);
+            minH = wave_min_t<KW, T>(LnH);
+            const uint32_t minD = wave_min_t<KW, T>(LnD);
+            uint32_t S[KW];
+#pragma unroll
+            for (int w = 0; w < KW; ++w) {
+                LH[w] = LnH[w];
+                S[w] = WRAP ? __vadd2(LnH[w], LnD[w]) : LnH[w] + LnD[w];
+            }
+            // ---- hand the diagonal vector to the row below / the band below ----
+            {
+                uint8_t* slot = mySlots + (u & 1) * SB;
+                store_words<KW>(reinterpret_cast<uint16_t*>(slot) + off, LnD);
+                if (tl == 0) *reinterpret_cast<uint32_t*>(slot + 2 * DP) = minD;
+            }
+            if (rowOn) {
+                store_words<KW>(pout, S);
+                pout += pstep;
+                if (exporter) {
+                    uint8_t* dst = xout + (size_t)u * SB;
+                    store_words<KW>(reinterpret_cast<uint16_t*>(dst) + off, LnD);
+                    if (tl == 0) *reinterpret_cast<uint32_t*>(dst + 2 * DP) = minD;
+                }
+            }
+            if (warpExports && ((u % kPE) == kPE - 1 || u == Ws - 1)) {
+                __syncwarp();
+                if (exporter && tl == 0) w_st_release_gpu(prodOut, (unsigned)(u + 1));
+            }
+            w_rows_barrier(RW * 32);
+            if (sflag[1]) break;
+        }
+        w_cp_wait<0>();
+        __syncthreads();
+    }
+}
+
+}  // namespace lumen
+
+namespace lumen {
+
+// Launch of one instance (the host picks KW and T from the padded disparity count).
+template <int KW, int T>
+cudaError_t pair_launch_t(const PairArgs& a, bool wrap, bool full, int smem, int grid, cudaStream_t s,
+                          int* perSM) {
+    constexpr int R = 16;
+    constexpr int threads = R / (32 / T) * 32;
+    void (*k)(PairArgs) = wrap ? (full ? pair_kernel<KW, true, true, R, T> : pair_kernel<KW, true, false, R, T>)
+                               : (full ? pair_kernel<KW, false, true, R, T> : pair_kernel<KW, false, false, R, T>);
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, k, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (grid <= 0) return cudaSuccess;   // occupancy query only
+    k<<<grid, threads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace lumen

@@ -54,17 +54,26 @@ __device__ __forceinline__ int16_t subpixel_disp(float c0, float c1, float c2, i
 // Subpixel neighbours are re-read from the (L1/L2-resident) volumes.  The
 // 1/16-px outputs equal the reference's bit for bit.
 // ---------------------------------------------------------------------------
-template <int KS>
+// w = a + b (+ c + d when NV == 4) over a lane's KS words (mod 2^16 per half when wrap)
+__device__ __forceinline__ uint32_t vsum(uint32_t x, uint32_t y, bool wrap) { return wrap ? __vadd2(x, y) : x + y; }
+
+template <int KS, int NV>
 __device__ __forceinline__ void slide_load(const uint16_t* __restrict__ a, const uint16_t* __restrict__ b,
+                                           const uint16_t* __restrict__ c, const uint16_t* __restrict__ d,
                                            bool wrap, uint32_t (&w)[KS]) {
     if constexpr (KS % 4 == 0) {
 #pragma unroll
         for (int i = 0; i < KS / 4; ++i) {
             uint4 v = __ldg(reinterpret_cast<const uint4*>(a) + i);
-            if (b) {
+            if (NV == 4 || b) {
                 const uint4 u = __ldg(reinterpret_cast<const uint4*>(b) + i);
-                v = wrap ? make_uint4(__vadd2(v.x, u.x), __vadd2(v.y, u.y), __vadd2(v.z, u.z), __vadd2(v.w, u.w))
-                         : make_uint4(v.x + u.x, v.y + u.y, v.z + u.z, v.w + u.w);
+                v = make_uint4(vsum(v.x, u.x, wrap), vsum(v.y, u.y, wrap), vsum(v.z, u.z, wrap), vsum(v.w, u.w, wrap));
+            }
+            if (NV == 4) {
+                const uint4 u = __ldg(reinterpret_cast<const uint4*>(c) + i);
+                const uint4 q = __ldg(reinterpret_cast<const uint4*>(d) + i);
+                v = make_uint4(vsum(v.x, vsum(u.x, q.x, wrap), wrap), vsum(v.y, vsum(u.y, q.y, wrap), wrap),
+                               vsum(v.z, vsum(u.z, q.z, wrap), wrap), vsum(v.w, vsum(u.w, q.w, wrap), wrap));
             }
             w[4 * i] = v.x; w[4 * i + 1] = v.y; w[4 * i + 2] = v.z; w[4 * i + 3] = v.w;
         }
@@ -73,25 +82,34 @@ __device__ __forceinline__ void slide_load(const uint16_t* __restrict__ a, const
 #pragma unroll
         for (int i = 0; i < KS / 2; ++i) {
             uint2 v = __ldg(reinterpret_cast<const uint2*>(a) + i);
-            if (b) {
+            if (NV == 4 || b) {
                 const uint2 u = __ldg(reinterpret_cast<const uint2*>(b) + i);
-                v = wrap ? make_uint2(__vadd2(v.x, u.x), __vadd2(v.y, u.y)) : make_uint2(v.x + u.x, v.y + u.y);
+                v = make_uint2(vsum(v.x, u.x, wrap), vsum(v.y, u.y, wrap));
+            }
+            if (NV == 4) {
+                const uint2 u = __ldg(reinterpret_cast<const uint2*>(c) + i);
+                const uint2 q = __ldg(reinterpret_cast<const uint2*>(d) + i);
+                v = make_uint2(vsum(v.x, vsum(u.x, q.x, wrap), wrap), vsum(v.y, vsum(u.y, q.y, wrap), wrap));
             }
             w[2 * i] = v.x; w[2 * i + 1] = v.y;
         }
     }
 }
 
+template <int NV>
 __device__ __forceinline__ uint32_t vol_cost(const uint16_t* __restrict__ a, const uint16_t* __restrict__ b,
+                                             const uint16_t* __restrict__ c, const uint16_t* __restrict__ d,
                                              size_t i) {
-    uint32_t c = __ldg(a + i);
-    if (b) c = (c + __ldg(b + i)) & 0xFFFFu;
-    return c;
+    uint32_t v = __ldg(a + i);
+    if (NV == 4 || b) v += __ldg(b + i);
+    if (NV == 4) v += (uint32_t)__ldg(c + i) + __ldg(d + i);
+    return v & 0xFFFFu;
 }
 
-template <int TL, int KS, bool FULL>
+template <int TL, int KS, bool FULL, int NV>
 __global__ void __launch_bounds__(256)
-select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict__ aggB, int wrap,
+select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict__ aggB,
+                    const uint16_t* __restrict__ aggC, const uint16_t* __restrict__ aggD, int wrap,
                     int W, int D, int Dp, int minD, int UR, int S, int16_t* __restrict__ dispL,
                     int16_t* __restrict__ dispR) {
     constexpr int M = 2 * KS;
@@ -108,11 +126,16 @@ select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict
     const size_t rowOff = (size_t)y * W * Dp;
     const uint16_t* rowA = agg + rowOff + d0;
     const uint16_t* rowB = aggB ? aggB + rowOff + d0 : nullptr;
+    const uint16_t* rowC = NV == 4 ? aggC + rowOff + d0 : nullptr;
+    const uint16_t* rowD = NV == 4 ? aggD + rowOff + d0 : nullptr;
     uint32_t R[M];
 #pragma unroll
     for (int j = 0; j < M; ++j) R[j] = INF;
     uint32_t wn[KS];
-    if (xs < W) slide_load<KS>(rowA + (size_t)xs * Dp, rowB ? rowB + (size_t)xs * Dp : nullptr, wrap, wn);
+    if (xs < W)
+        slide_load<KS, NV>(rowA + (size_t)xs * Dp, rowB ? rowB + (size_t)xs * Dp : nullptr,
+                           NV == 4 ? rowC + (size_t)xs * Dp : nullptr, NV == 4 ? rowD + (size_t)xs * Dp : nullptr,
+                           wrap, wn);
     for (int s = 0; s < S; s += M) {
 #pragma unroll
         for (int u = 0; u < M; ++u) {
@@ -122,7 +145,9 @@ select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict
 #pragma unroll
             for (int k = 0; k < KS; ++k) w[k] = wn[k];
             if (x + 1 < W && (s + u + 1) < S)
-                slide_load<KS>(rowA + (size_t)(x + 1) * Dp, rowB ? rowB + (size_t)(x + 1) * Dp : nullptr, wrap, wn);
+                slide_load<KS, NV>(rowA + (size_t)(x + 1) * Dp, rowB ? rowB + (size_t)(x + 1) * Dp : nullptr,
+                                   NV == 4 ? rowC + (size_t)(x + 1) * Dp : nullptr,
+                                   NV == 4 ? rowD + (size_t)(x + 1) * Dp : nullptr, wrap, wn);
             // slide by one: the slot leaving this lane (logical M-1, physical
             // (M-1-u) mod M) enters the next lane as its logical slot 0 and
             // this lane's logical 0 takes the previous lane's
@@ -163,8 +188,8 @@ select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict
                     out = -1;
                 } else if (bestD > 0 && bestD < D - 1) {
                     const size_t i0 = rowOff + (size_t)x * Dp + bestD;
-                    out = subpixel_disp((float)vol_cost(agg, aggB, i0 - 1), (float)best,
-                                        (float)vol_cost(agg, aggB, i0 + 1), bestD, D, minD);
+                    out = subpixel_disp((float)vol_cost<NV>(agg, aggB, aggC, aggD, i0 - 1), (float)best,
+                                        (float)vol_cost<NV>(agg, aggB, aggC, aggD, i0 + 1), bestD, D, minD);
                 } else {
                     out = subpixel_disp(0.f, 0.f, 0.f, bestD, D, minD);
                 }
@@ -189,8 +214,8 @@ select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict
         int16_t out;
         if (bestD > 0 && bestD < D - 1) {
             const size_t i0 = rowOff + (size_t)(xr + minD + bestD) * Dp + bestD;
-            out = subpixel_disp((float)vol_cost(agg, aggB, i0 - 1), (float)(k >> 16),
-                                (float)vol_cost(agg, aggB, i0 + 1), bestD, D, minD);
+            out = subpixel_disp((float)vol_cost<NV>(agg, aggB, aggC, aggD, i0 - 1), (float)(k >> 16),
+                                (float)vol_cost<NV>(agg, aggB, aggC, aggD, i0 + 1), bestD, D, minD);
         } else {
             out = subpixel_disp(0.f, 0.f, 0.f, bestD, D, minD);
         }
@@ -201,17 +226,20 @@ select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict
 template <int TL, int KS>
 static cudaError_t launch_select_slide(const uint16_t* agg, const uint16_t* aggB, bool wrap, int W, int H,
                                        int D, int Dp, int minD, int UR, int16_t* dispL, int16_t* dispR,
-                                       cudaStream_t s) {
+                                       cudaStream_t s, const uint16_t* aggC, const uint16_t* aggD) {
     constexpr int M = 2 * KS, kTeams = 256 / TL;
     const int seg = (W + kTeams - 1) / kTeams;
     const int S = (seg + M - 1) / M * M;
     const size_t smem = (size_t)W * 4;
-    auto kern = D == Dp ? select_slide_kernel<TL, KS, true> : select_slide_kernel<TL, KS, false>;
+    const bool four = aggB && aggC && aggD;
+    auto kern = four ? (D == Dp ? select_slide_kernel<TL, KS, true, 4> : select_slide_kernel<TL, KS, false, 4>)
+                     : (D == Dp ? select_slide_kernel<TL, KS, true, 2> : select_slide_kernel<TL, KS, false, 2>);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    kern<<<H, 256, smem, s>>>(agg, aggB, wrap ? 1 : 0, W, D, Dp, minD, UR, S, dispL, dispR);
+    kern<<<H, 256, smem, s>>>(agg, aggB, four ? aggC : nullptr, four ? aggD : nullptr, wrap ? 1 : 0, W, D, Dp,
+                              minD, UR, S, dispL, dispR);
     return cudaGetLastError();
 }
 
@@ -241,18 +269,18 @@ void launch_sum_volumes(const uint16_t* a, const uint16_t* b, uint16_t* dst, siz
 
 cudaError_t launch_select(const uint16_t* agg, const uint16_t* aggB, bool wrap, int W, int H,
                           int D, int Dp, int minD, int UR, int16_t* dispL, int16_t* dispR,
-                          cudaStream_t s) {
+                          cudaStream_t s, const uint16_t* aggC, const uint16_t* aggD) {
     if ((size_t)W * 4 > kSelectSmemMax) return cudaErrorInvalidValue;  // W > 58112: no row array
     switch (Dp / 64) {
-    case 1: return launch_select_slide<8, 4>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 2: return launch_select_slide<8, 8>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 3: return launch_select_slide<8, 12>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 1: return launch_select_slide<8, 4>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, aggC, aggD);
+    case 2: return launch_select_slide<8, 8>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, aggC, aggD);
+    case 3: return launch_select_slide<8, 12>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, aggC, aggD);
     // wider pixels spread over 16 lanes: 16-20 words per lane cost occupancy
-    case 4: return launch_select_slide<16, 8>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 5: return launch_select_slide<16, 10>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 6: return launch_select_slide<16, 12>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 7: return launch_select_slide<16, 14>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
-    case 8: return launch_select_slide<16, 16>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s);
+    case 4: return launch_select_slide<16, 8>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, aggC, aggD);
+    case 5: return launch_select_slide<16, 10>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, aggC, aggD);
+    case 6: return launch_select_slide<16, 12>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, aggC, aggD);
+    case 7: return launch_select_slide<16, 14>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, aggC, aggD);
+    case 8: return launch_select_slide<16, 16>(agg, aggB, wrap, W, H, D, Dp, minD, UR, dispL, dispR, s, aggC, aggD);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -104,7 +104,7 @@ CASES = {
 }
 
 
-@pytest.mark.parametrize("schedule", [1, 2, 3, 4])
+@pytest.mark.parametrize("schedule", [1, 2, 3, 4, 6])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_parity_small(name, schedule, oracle_mod):
     w, h, over = CASES[name]
@@ -275,7 +275,50 @@ def test_parity_schedule5_wide_image(oracle_mod):
         assert_subpix_close(disp, ref_disp)
 
 
-@pytest.mark.parametrize("schedule", [3, 4, 5])
+@pytest.mark.parametrize("D,size", [(40, (131, 53)), (64, (40, 200)), (128, (97, 150)), (150, (160, 70)),
+                                    (200, (230, 16)), (290, (330, 41))])
+@pytest.mark.parametrize("census", [False, True])
+def test_parity_schedule6_pair_sweeps(D, size, census, oracle_mod):
+    """Four lag-free sweeps (schedule 6: {LR, TLBR}, {RL, BRTL} over rows,
+    {TB, TRBL}, {BT, BLTR} over columns) reproduce the oracle's summed volume
+    bit for bit; without retained intermediates the selection sums the four
+    partial volumes itself and the maps still match.  Sizes cover wider and
+    taller images than bands (both ticket orders) and a single-band sweep."""
+    w, h = size
+    left, right, _ = synth.make_pair(synth.PairSpec(w, h, 4, 1, min(D - 1, 40), 2.0, 90 + D + w))
+    pd = params_dict(maxDisparity=D, numDirections=8, speckleWindowSize=0, matchingCostMode=int(census))
+    ref_disp, ref = oracle_mod.sgbm(pd, left, right, intermediates=True)
+    with StereoSGBM(to_params(pd)) as s:
+        s.set_schedule(6)
+        s.retain_intermediates(True)
+        disp = s.compute(left, right)
+        agg = s.intermediate("agg", (h, w, D), np.uint16)
+        assert s.get_tuning()[0] == 6
+    assert np.array_equal(agg, ref["agg"])
+    assert_subpix_close(disp, ref_disp)
+    with StereoSGBM(to_params(pd)) as s:
+        s.set_schedule(6)
+        assert np.array_equal(s.compute(left, right), disp)
+
+
+def test_schedule6_matches_schedule4_full_size():
+    """1920x1080 D128 SAD and Census, 8 paths: the four-partial selection of
+    schedule 6 gives schedule 4's maps (no intermediates retained)."""
+    for wl in ("1920x1080_d128_sad_8path", "1920x1080_d128_census_8path"):
+        w = synth.WORKLOADS[wl]
+        left, right, _ = synth.make_pair(w.pair)
+        p = StereoParams(maxDisparity=w.max_disparity, numDirections=8, speckleWindowSize=0,
+                         matchingCostMode=MatchingCostMode.Census if w.census else MatchingCostMode.SAD)
+        outs = []
+        for schedule in (4, 6):
+            with StereoSGBM(p) as s:
+                s.set_schedule(schedule)
+                outs.append(s.compute(left, right))
+                assert s.get_tuning()[0] == schedule
+        assert np.array_equal(outs[0], outs[1]), wl
+
+
+@pytest.mark.parametrize("schedule", [3, 4, 5, 6])
 def test_fused_sweep_timeout_reports_error(schedule):
     """A device-side wait that runs out ends the launch with a timeout status,
     not a hang: one wait of a band that imports through the global ring is
@@ -409,14 +452,14 @@ def test_schedules_agree_full_size(wl):
                      matchingCostMode=MatchingCostMode.Census if w.census else MatchingCostMode.SAD,
                      speckleWindowSize=0)
     outs = []
-    for schedule in (1, 2, 3, 4, 5):
+    for schedule in (1, 2, 3, 4, 5, 6):
         with StereoSGBM(p) as s:
             s.set_schedule(schedule)
             s.retain_intermediates(True)
             d = s.compute(left, right)
             agg = s.intermediate("agg", left.shape + (w.max_disparity,), np.uint16)
             outs.append((d, agg))
-    for k in (1, 2, 3, 4):
+    for k in (1, 2, 3, 4, 5):
         assert np.array_equal(outs[0][1], outs[k][1]), k
         assert np.array_equal(outs[0][0], outs[k][0]), k
 
