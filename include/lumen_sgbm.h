@@ -116,9 +116,12 @@ lumen_status lumen_sgbm_debug_set_paths(lumen_sgbm* h, uint32_t path_mask);
  * per direction, 2 = two fused wavefront sweeps (rows of a band in lockstep),
  * 3 = two fused wavefront sweeps with decoupled row warps and ticket-ordered
  * bands, 4 = two fused wavefront sweeps with lockstep row bands and helper
- * warps for the band hand-offs (the default), 5 = schedule 4 with consecutive
- * bands in thread-block clusters of up to 8 CTAs that hand rows over through
- * distributed shared memory.  Outputs are identical for every schedule. */
+ * warps for the band hand-offs (the 4-path default), 5 = schedule 4 with
+ * consecutive bands in thread-block clusters of up to 8 CTAs that hand rows
+ * over through distributed shared memory, 6 = four lag-free two-path sweeps,
+ * two over rows and two over columns (the 8-path default for padded
+ * disparities up to 320; 4 paths or wider ranges fall back to schedule 4).
+ * Outputs are identical for every schedule. */
 lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule);
 /* Pin the fused-sweep configuration: lanes per pixel (8, 16 or 32) and warps
  * per thread block (schedule 2: 2, 4, 8 or 16; rows per band = warps * 32 /
@@ -163,9 +166,10 @@ lumen_status lumen_sgbm_debug_trace_copy(lumen_sgbm* h, unsigned long long* dst,
 unsigned long long lumen_sgbm_debug_launch_count(const lumen_sgbm* h);
 /* Iteration limit of every device-side wait (0 restores the default, 2^22). */
 lumen_status lumen_sgbm_debug_set_wait_limit(lumen_sgbm* h, long long spins);
-/* Failure-path self test of schedule 3: while enabled, one wait of the first
- * band can never be satisfied, so it runs out after the wait limit and the
- * compute returns LUMEN_ERR_TIMEOUT (no fault, no hang; the handle stays usable). */
+/* Failure-path self test of schedules 3-6: while enabled, one wait of a band
+ * that imports from the band above can never be satisfied, so it runs out
+ * after the wait limit and the compute returns LUMEN_ERR_TIMEOUT (no fault, no
+ * hang; the handle stays usable). */
 lumen_status lumen_sgbm_debug_stall_test(lumen_sgbm* h, int enable);
 
 /* ---- rectification remap (replaces stereo::StereoRectifier,
