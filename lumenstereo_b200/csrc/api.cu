@@ -464,9 +464,19 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
     if (sched == 0) sched = mask == 0xFFu ? 6 : (sweepable ? 4 : 1);
     if (sched >= 2 && !sweepable) sched = 1;          // single-path debug masks: per-direction kernels
     PairPlan plan6{};
-    if (sched == 6 && (mask != 0xFFu || pair_plan(k, wrap, h->numSMs, &plan6) != cudaSuccess)) {
-        sched = 4;                                     // 4 paths, or no instance for this range
-        if (!h->forced.T) cfgChosen = false;
+    if (sched == 6) {
+        // 4 paths, no instance for this range, or short of device memory for
+        // the four partial volumes and the row buffers: schedule 4
+        bool ok6 = mask == 0xFFu && pair_plan(k, wrap, h->numSMs, &plan6) == cudaSuccess;
+        if (ok6)
+            ok6 = h->partB.ensure(ND * 2) == cudaSuccess && h->partC.ensure(ND * 2) == cudaSuccess &&
+                  h->partD.ensure(ND * 2) == cudaSuccess && h->xring.ensure(plan6.xbufBytes) == cudaSuccess &&
+                  h->counters.ensure(sizeof(unsigned) * plan6.counterWords) == cudaSuccess;
+        if (!ok6) {
+            (void)cudaGetLastError();                  // a failed allocation is not a sticky error
+            sched = 4;
+            if (!h->forced.T) cfgChosen = false;
+        }
     }
     WavePlan plan4{};
     if (sched == 5) {
