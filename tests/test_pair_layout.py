@@ -27,6 +27,21 @@ def test_pair_layout_host_checks(tmp_path):
     assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
 
 
+def test_pair_handoff_protocol_host_model(tmp_path):
+    """Worker threads standing for any number of resident CTAs run the bands
+    in ticket order with the kernel's publish / bounded-wait protocol: every
+    band finishes and consumes only published pixels."""
+    cxx = shutil.which("g++")
+    if not cxx:
+        pytest.skip("no C++ compiler")
+    exe = tmp_path / "pair_progress_test"
+    subprocess.run([cxx, "-std=c++17", "-O2", "-Wall", "-pthread", "-I",
+                    os.path.join(ROOT, "lumenstereo_b200", "csrc"),
+                    os.path.join(ROOT, "tests", "cpp", "pair_progress_test.cpp"), "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
+
+
 def _step(Lp, C, P1, p2):
     """src/sgbm_kernels.cu:338-360 on one pixel (uint16 wrap)."""
     a = Lp.astype(np.int64)
