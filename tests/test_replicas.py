@@ -48,3 +48,13 @@ def test_replica_rate_max_over_ranks():
 def test_replica_rate_single_rank():
     import bench
     assert bench.replica_rate(0.5, 10.0, 1) == (0.5, 20.0)
+
+
+def test_profiled_traffic_belongs_to_the_captured_schedule():
+    """The DRAM traffic bench.py reports comes from an ncu capture of the same
+    aggregation kernel: it is keyed by workload and schedule, and a schedule
+    without a capture reports none."""
+    import bench
+    assert bench.profiled_traffic("1920x1080_d128_sad_8path", 4) == 6.42
+    assert bench.profiled_traffic("1920x1080_d128_sad_8path", 6) is None
+    assert bench.profiled_traffic("640x480_d64_census_4path", 4) is None
