@@ -14,14 +14,7 @@
 #include "../lumen_sgbm.h"
 #include "common.h"
 #include "sgbm_limits.h"
-#include "stereo_params.h"
-
-#if defined(__has_include)
-#if __has_include(<opencv2/core.hpp>)
-#include <opencv2/core.hpp>
-#define LUMEN_HAVE_OPENCV 1
-#endif
-#endif
+#include "stereo_params.h"  // defines LUMEN_HAVE_OPENCV when OpenCV headers exist
 
 namespace stereo {
 

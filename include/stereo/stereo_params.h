@@ -5,6 +5,13 @@
  */
 #include "../lumen_sgbm.h"
 
+#if defined(__has_include)
+#if __has_include(<opencv2/core.hpp>)
+#include <opencv2/core.hpp>
+#define LUMEN_HAVE_OPENCV 1
+#endif
+#endif
+
 namespace stereo {
 
 enum class MatchingCostMode : int {
@@ -80,5 +87,34 @@ struct StereoParams {
         return p;
     }
 };
+
+#ifdef LUMEN_HAVE_OPENCV
+/** Calibration of a camera pair, field for field as the reference's
+ *  CameraParams (include/stereo/stereo_params.h:132-175).  The rectifier uses
+ *  width, height and the four CV_32FC1 maps; empty maps mean the pair is
+ *  already rectified. */
+struct CameraParams {
+    int width = 0;
+    int height = 0;
+    cv::Mat K0, D0;
+    cv::Mat K1, D1;
+    cv::Mat R, T;
+    double baseline = 0.0;
+    double focalLength = 0.0;
+    int disparityOffset = 0;
+    int numDisparities = 0;
+    cv::Mat R0, R1;
+    cv::Mat P0, P1;
+    cv::Mat Q;
+    cv::Mat map0x, map0y;
+    cv::Mat map1x, map1y;
+
+    /** baseline = |T|, focalLength = (fx + fy) / 2 of camera 0. */
+    void computeDerivedValues() {
+        if (!T.empty()) baseline = cv::norm(T);
+        if (!K0.empty()) focalLength = (K0.at<double>(0, 0) + K0.at<double>(1, 1)) / 2.0;
+    }
+};
+#endif
 
 }  // namespace stereo

@@ -11,13 +11,21 @@ SRC = os.path.join(ROOT, "tests", "cpp", "api_surface.cpp")
 LIBDIR = os.path.join(ROOT, "lumenstereo_b200")
 
 
-def build_binary(tmp_path):
+SRC_CV = os.path.join(ROOT, "tests", "cpp", "api_cvmat.cpp")
+FAKE_CV = os.path.join(ROOT, "tests", "cpp", "fake_opencv")
+
+
+def build_binary(tmp_path, src=SRC, extra_includes=()):
     cxx = shutil.which("g++")
     if not cxx:
         pytest.skip("no C++ compiler")
-    exe = str(tmp_path / "api_surface")
-    subprocess.run([cxx, "-std=c++17", "-O1", "-Wall", "-I", os.path.join(ROOT, "include"), SRC,
-                    "-L", LIBDIR, "-llumen_sgbm", f"-Wl,-rpath,{LIBDIR}", "-o", exe], check=True)
+    exe = str(tmp_path / os.path.splitext(os.path.basename(src))[0])
+    inc = []
+    for d in extra_includes:
+        inc += ["-I", d]
+    subprocess.run([cxx, "-std=c++17", "-O1", "-Wall", *inc, "-I", os.path.join(ROOT, "include"),
+                    src, "-L", LIBDIR, "-llumen_sgbm", f"-Wl,-rpath,{LIBDIR}", "-o", exe],
+                   check=True)
     return exe
 
 
@@ -36,5 +44,31 @@ def test_cpp_headers_cpu(tmp_path):
 @pytest.mark.gpu
 def test_cpp_headers_gpu(tmp_path):
     exe = build_binary(tmp_path)
+    r = subprocess.run([exe, "gpu"], capture_output=True, text=True)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
+
+
+def _no_gpu_visible():
+    try:
+        import torch
+        return not torch.cuda.is_available()
+    except ImportError:
+        return True
+
+
+def test_cpp_cvmat_forms_cpu(tmp_path):
+    """The reference's cv::Mat / CameraParams signatures compile (against a
+    stand-in cv::Mat) and reject bad maps before touching the device."""
+    if not _no_gpu_visible():
+        pytest.skip("CPU variant: runs where no GPU is visible")
+    exe = build_binary(tmp_path, SRC_CV, (FAKE_CV,))
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
+
+
+@pytest.mark.gpu
+def test_cpp_cvmat_forms_gpu(tmp_path):
+    """Every cv::Mat form equals the raw-pointer form of the same call."""
+    exe = build_binary(tmp_path, SRC_CV, (FAKE_CV,))
     r = subprocess.run([exe, "gpu"], capture_output=True, text=True)
     assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr
