@@ -367,12 +367,13 @@ lumen_status lumen_server_get_stats(lumen_server* s, lumen_server_stats* out);
 /* ---- Census cost volume without device allocation.  No counterpart in the
  * reference: it serves callers that cannot call cudaMalloc (a real-time loop
  * that must not take cudaMalloc's implicit device synchronisation, a plugin host
- * whose pool owns all device memory, work built inside a stream capture). ----
+ * whose pool owns all device memory). ----
  *
  * Census 5x5 descriptors of both DEVICE images (gray, width*height bytes, pitch
  * width) and the uint8 cost volume d_cost[(y*width + x)*cost_stride + d], the
  * values of the Census stage of lumen_sgbm_compute (entries d >= maxDisparity -
- * minDisparity are 0).  cost_stride: a multiple of 16, >= the disparity range.
+ * minDisparity are 0).  cost_stride: a multiple of 16, >= the disparity range;
+ * d_cost: 16-byte aligned (LUMEN_ERR_INVALID_ARGUMENT otherwise).
  * Asynchronous on `stream` (NULL = the default stream).  The descriptors live
  * in a fixed 16 MiB array inside the library (held by every GPU that loads it
  * until exit): images above lumen_census_cost_noalloc_max_pixels() pixels

@@ -3,12 +3,11 @@
 // lumen_census_cost_noalloc runs the two Census stages of the pipeline
 // (census_kernel, census_cost_kernel in cost.cu) for callers that must not
 // allocate device memory: code that enqueues work from a real-time loop where
-// cudaMalloc's implicit device synchronisation would stall other streams,
-// plugin hosts that own every byte of device memory through their own pool,
-// and callers that build their work inside a stream capture, where cudaMalloc
-// is not permitted.  The caller passes the two gray images and the output
-// volume; the only intermediate, the two Census descriptor images, lives in
-// the file-scope array below.
+// cudaMalloc's implicit device synchronisation would stall other streams, and
+// plugin hosts that own every byte of device memory through their own pool.
+// The caller passes the two gray images and the output volume; the only
+// intermediate, the two Census descriptor images, lives in the file-scope
+// array below.
 //
 // The array is part of the library's device image: every GPU that loads the
 // library holds its 16 MiB until the process exits.  Every call shares it, so
@@ -17,6 +16,7 @@
 // every descriptor it reads (border pixels get 0), so nothing has to be
 // cleared between calls.
 #include <cuda_runtime.h>
+#include <cstdint>
 #include <mutex>
 #include <string>
 
@@ -84,6 +84,15 @@ extern "C" lumen_status lumen_census_cost_noalloc(const uint8_t* d_left, const u
     if (D > LUMEN_MAX_DISPARITY_RANGE)
         return set_error(LUMEN_ERR_RANGE_EXCEEDS_LIMIT,
                          "lumen_census_cost_noalloc: disparity range exceeds 512");
+    // the same bound as the other entry points: keeps every index of the cost
+    // kernel (x - minDisparity - d) inside int range
+    if ((long long)max_disparity * 16 > 32767)
+        return set_error(LUMEN_ERR_INVALID_ARGUMENT,
+                         "lumen_census_cost_noalloc: maxDisparity * 16 exceeds the int16 output range");
+    // the cost kernel writes 16 disparities per 16-byte store
+    if ((reinterpret_cast<uintptr_t>(d_cost) & 15u) != 0)
+        return set_error(LUMEN_ERR_INVALID_ARGUMENT,
+                         "lumen_census_cost_noalloc: d_cost must be 16-byte aligned");
     if (cost_stride < D || cost_stride % 16 != 0 || cost_stride > 4096)
         return set_error(LUMEN_ERR_INVALID_ARGUMENT,
                          "lumen_census_cost_noalloc: cost_stride must be a multiple of 16, "

@@ -132,6 +132,23 @@ def sgbm(params, left: np.ndarray, right: np.ndarray, intermediates: bool = Fals
     return (out, arrs) if intermediates else out
 
 
+def census_cost(left: np.ndarray, right: np.ndarray, min_disparity: int, max_disparity: int):
+    """Census stage alone: descriptors of both gray images
+    (src/sgbm_kernels.cu:217-245) and the uint8 cost volume [H][W][D]
+    (src/sgbm_kernels.cu:250-286)."""
+    left = np.ascontiguousarray(left, np.uint8)
+    right = np.ascontiguousarray(right, np.uint8)
+    h, w = left.shape
+    D = max_disparity - min_disparity
+    cl = np.zeros((h, w), np.uint32)
+    cr = np.zeros((h, w), np.uint32)
+    lib().oracle_census5x5(_ptr(left), _ptr(cl), w, h)
+    lib().oracle_census5x5(_ptr(right), _ptr(cr), w, h)
+    cost = np.zeros((h, w, D), np.uint8)
+    lib().oracle_cost_census(_ptr(cl), _ptr(cr), _ptr(cost), w, h, D, min_disparity)
+    return cost
+
+
 def remap(src: np.ndarray, mapx: np.ndarray, mapy: np.ndarray) -> np.ndarray:
     src = np.ascontiguousarray(src)
     h, w = mapx.shape
