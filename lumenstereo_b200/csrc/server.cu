@@ -314,6 +314,27 @@ void slot_retire(lumen_server* S, Slot& sl) {
     S->cvWork.notify_all();
 }
 
+// A fatal CUDA error: every request still in a busy slot completes with
+// LUMEN_ERR_CUDA and leaves its slot; the device memory is not reused (the
+// server stops).  Caller holds S->mu.
+void fail_all_inflight(lumen_server* S) {
+    for (Slot& o : S->slots) {
+        if (!o.busy) continue;
+        for (Request* r : o.reqs) {
+            r->inFlight = false;
+            if (!r->done) {
+                complete(S, r, LUMEN_ERR_CUDA, S->fatal);
+            } else if (r->user == nullptr) {  // abandoned by its caller after the watchdog
+                S->reqs.erase(r->id);
+                delete r;
+            }
+        }
+        o.reqs.clear();
+        o.busy = false;
+        S->st.inflight_batches--;
+    }
+}
+
 void server_loop(lumen_server* S) {
     cudaSetDevice(S->device);
     for (;;) {
@@ -325,11 +346,11 @@ void server_loop(lumen_server* S) {
                 slot_retire(S, sl);
                 progressed = true;
             } else if (q != cudaErrorNotReady) {
-                // the context is unusable: fail everything and stop serving
+                // the context is unusable: fail every request of every busy
+                // slot and of the queue, and stop serving
                 std::lock_guard<std::mutex> g(S->mu);
                 S->fatal = std::string("server: CUDA error: ") + cudaGetErrorString(q);
-                for (Request* r : sl.reqs)
-                    if (!r->done) complete(S, r, LUMEN_ERR_CUDA, S->fatal);
+                fail_all_inflight(S);
                 for (Request* r : S->queue) complete(S, r, LUMEN_ERR_CUDA, S->fatal);
                 S->queue.clear();
                 S->stop = true;
