@@ -92,6 +92,17 @@ def workload_params(wl) -> StereoParams:
                         speckleWindowSize=0)
 
 
+def workload_config(name: str, world: int) -> dict:
+    """The `config` object of the JSON line; both arms print the same one."""
+    wl = synth.WORKLOADS[name]
+    return {"workload": name, "width": wl.pair.width, "height": wl.pair.height,
+            "max_disparity": wl.max_disparity,
+            "cost": "census" if wl.census else "sad+sobel-x prefilter",
+            "paths": wl.num_directions, "params": "StereoParams defaults, speckleWindowSize=0",
+            "l2": "256 MiB buffer written before every timed step, outside its events",
+            "parallelism": f"replicas x{world}"}
+
+
 def params_dict(p: StereoParams):
     return {k: int(v) for k, v in p.__dict__.items()}
 
@@ -333,13 +344,9 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
-        "config": {"workload": args.workload, "width": W, "height": H, "max_disparity": D,
-                   "cost": "census" if wl.census else "sad+sobel-x prefilter",
-                   "paths": P, "params": "StereoParams defaults, speckleWindowSize=0",
-                   "l2": "256 MiB buffer written before every timed step, outside its events",
-                   "parallelism": f"replicas x{world}",
-                   "schedule": {"requested": args.schedule or "auto", "used": tuning[0],
-                                "lanes_per_pixel": tuning[1], "warps_per_block": tuning[2]}},
+        "config": workload_config(args.workload, world),
+        "schedule": {"requested": args.schedule or "auto", "used": tuning[0],
+                     "lanes_per_pixel": tuning[1], "warps_per_block": tuning[2]},
         "roofline": {"bound": "hbm", "kernel": "sgm aggregation stage",
                      "achieved": achieved, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / hbm,
@@ -405,8 +412,7 @@ def run_reference(args):
            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "u16", "data": "synthetic",
-           "config": {"workload": args.workload, "width": W, "height": H, "max_disparity": D,
-                      "paths": wl.num_directions, "cost": "census" if wl.census else "sad"},
+           "config": workload_config(args.workload, world),
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": oracle.max_threads(),
                             "kind": "port", "sample": sample},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

@@ -529,7 +529,9 @@ def test_parity_vs_reference_kernels_full_size(wl, oracle_mod):
     p = params_dict(maxDisparity=w.max_disparity, matchingCostMode=int(w.census),
                     numDirections=w.num_directions, speckleWindowSize=0)
     ref_disp, ref, _ = oracle_mod.ref_sgbm(p, left, right, intermediates=False)
-    for schedule in (1, 2, 3):
+    # 0: the untuned default the bench runs; 4 and 6: the fused sweeps it picks
+    # (4 paths: schedule 4; 8 paths: schedule 6); 1: the per-direction fallback
+    for schedule in (0, 1, 4, 6):
         ours, inter = run_ours_light(p, left, right, schedule)
         assert np.array_equal(ours, ref_disp), schedule
     # sanity: the scene's disparities are recovered
@@ -555,11 +557,29 @@ def test_parity_vs_reference_kernels_intermediates(oracle_mod):
         p = params_dict(maxDisparity=64, matchingCostMode=mode, numDirections=nd,
                         uniquenessRatio=ur, speckleWindowSize=0)
         ref_disp, ref, _ = oracle_mod.ref_sgbm(p, left, right, intermediates=True)
-        for schedule in (1, 2, 3):
+        for schedule in (0, 1, 4, 6):
             disp, ours = run_ours(p, left, right, schedule=schedule)
             for key in ("cost", "agg", "disp_wta", "disp_right", "disp_lr"):
                 assert np.array_equal(ours[key], ref[key]), (mode, nd, key, schedule)
             assert np.array_equal(disp, ref_disp)
+
+
+@pytest.mark.parametrize("wl", ["1920x1080_d128_sad_8path", "1920x1080_d128_census_8path"])
+def test_parity_vs_reference_kernels_volume_full_size(wl, oracle_mod):
+    """The summed aggregated volume of the default 8-path schedule (four
+    partial volumes summed mod 2^16 in the selection) and every map after it
+    against the reference kernels' agg volume and maps at 1920x1080 D128."""
+    _ref_or_skip(oracle_mod)
+    w = synth.WORKLOADS[wl]
+    left, right, _ = synth.make_pair(w.pair)
+    p = params_dict(maxDisparity=w.max_disparity, matchingCostMode=int(w.census),
+                    numDirections=w.num_directions, speckleWindowSize=0)
+    ref_disp, ref, _ = oracle_mod.ref_sgbm(p, left, right, intermediates=True)
+    for schedule in (0, 6):
+        disp, ours = run_ours(p, left, right, schedule=schedule)
+        for key in ("cost", "agg", "disp_wta", "disp_right", "disp_lr"):
+            assert np.array_equal(ours[key], ref[key]), (wl, key, schedule)
+        assert np.array_equal(disp, ref_disp), schedule
 
 
 def test_remap_vs_reference_kernel(oracle_mod):
