@@ -211,6 +211,40 @@ def ref_sgbm(params, left: np.ndarray, right: np.ndarray, intermediates: bool = 
     return out, arrs, ms.value
 
 
+def ref_depth(disp: np.ndarray, focal: float, baseline: float, doffs: float = 0.0) -> np.ndarray:
+    """The reference's disparityToDepthKernel (src/depth_map.cu:74-102) on the GPU."""
+    disp = np.ascontiguousarray(disp, np.int16)
+    h, w = disp.shape
+    out = np.zeros((h, w), np.float32)
+    rc = ref().ref_depth_run(_ptr(disp), _ptr(out), w, h, C.c_float(focal), C.c_float(baseline),
+                             C.c_float(doffs))
+    if rc != 0:
+        raise RuntimeError(f"ref_depth_run failed ({rc}): {ref().ref_last_error()!r}")
+    return out
+
+
+def ref_colorize(depth: np.ndarray, min_depth: float, max_depth: float) -> np.ndarray:
+    """The reference's colorizeDepthKernel (src/depth_map.cu:104-142) on the
+    GPU: H x W x 3 bytes in R, G, B order."""
+    depth = np.ascontiguousarray(depth, np.float32)
+    h, w = depth.shape
+    out = np.zeros((h, w, 3), np.uint8)
+    rc = ref().ref_colorize_run(_ptr(depth), _ptr(out), w, h, C.c_float(min_depth),
+                                C.c_float(max_depth))
+    if rc != 0:
+        raise RuntimeError(f"ref_colorize_run failed ({rc}): {ref().ref_last_error()!r}")
+    return out
+
+
+def ref_turbo_table() -> np.ndarray:
+    """The reference's colour table (src/depth_map.cu:18-64) as 256 x 3 (R, G, B)."""
+    out = np.zeros((256, 3), np.uint8)
+    rc = ref().ref_turbo_table(_ptr(out))
+    if rc != 0:
+        raise RuntimeError(f"ref_turbo_table failed ({rc}): {ref().ref_last_error()!r}")
+    return out
+
+
 def ref_remap(src: np.ndarray, mapx: np.ndarray, mapy: np.ndarray) -> np.ndarray:
     src = np.ascontiguousarray(src)
     h, w = mapx.shape

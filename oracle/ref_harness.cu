@@ -35,6 +35,11 @@ __global__ void consistencyCheck(int16_t*, const int16_t*, int, int, int);
 __global__ void medianFilter3x3(const int16_t*, int16_t*, int, int);
 __global__ void speckleFilter(int16_t*, int, int, int, int);
 __global__ void remapKernelSimple(const unsigned char*, const float*, const float*, unsigned char*, int, int, int);
+__global__ void disparityToDepthKernel(const int16_t*, float*, int, int, float, float, float);
+__global__ void colorizeDepthKernel(const float*, unsigned char*, int, int, float, float);
+extern __constant__ unsigned char turboR[256];
+extern __constant__ unsigned char turboG[256];
+extern __constant__ unsigned char turboB[256];
 }  // namespace stereo
 
 // Field order of oracle_params / lumen_stereo_params; external linkage so the
@@ -288,5 +293,66 @@ extern "C" int ref_remap_run(const uint8_t* hsrc, const float* hmx, const float*
     RCHECK(cudaMemcpy(hdst, dd, n, cudaMemcpyDeviceToHost));
 cleanup:
     cudaFree(ds); cudaFree(dd); cudaFree(dx); cudaFree(dy);
+    return rc;
+}
+
+// disparityToDepthGPU's launch (src/depth_map.cu:169-187): 16x16 blocks.
+extern "C" int ref_depth_run(const int16_t* hdisp, float* hdepth, int W, int H, float focal,
+                             float baseline, float doffs) {
+    int rc = 0;
+    const size_t n = (size_t)W * H;
+    int16_t* dd = nullptr;
+    float* dz = nullptr;
+    RCHECK(cudaMalloc(&dd, n * 2));
+    RCHECK(cudaMalloc(&dz, n * 4));
+    RCHECK(cudaMemcpy(dd, hdisp, n * 2, cudaMemcpyHostToDevice));
+    {
+        dim3 b(16, 16), g(divUp(W, 16), divUp(H, 16));
+        stereo::disparityToDepthKernel<<<g, b>>>(dd, dz, W, H, focal, baseline, doffs);
+    }
+    RCHECK(cudaGetLastError());
+    RCHECK(cudaDeviceSynchronize());
+    RCHECK(cudaMemcpy(hdepth, dz, n * 4, cudaMemcpyDeviceToHost));
+cleanup:
+    cudaFree(dd); cudaFree(dz);
+    return rc;
+}
+
+// colorizeDepthGPU's launch (src/depth_map.cu:205-222): 16x16 blocks, RGB out.
+extern "C" int ref_colorize_run(const float* hdepth, uint8_t* hrgb, int W, int H, float minDepth,
+                                float maxDepth) {
+    int rc = 0;
+    const size_t n = (size_t)W * H;
+    float* dz = nullptr;
+    unsigned char* dc = nullptr;
+    RCHECK(cudaMalloc(&dz, n * 4));
+    RCHECK(cudaMalloc(&dc, n * 3));
+    RCHECK(cudaMemcpy(dz, hdepth, n * 4, cudaMemcpyHostToDevice));
+    {
+        dim3 b(16, 16), g(divUp(W, 16), divUp(H, 16));
+        stereo::colorizeDepthKernel<<<g, b>>>(dz, dc, W, H, minDepth, maxDepth);
+    }
+    RCHECK(cudaGetLastError());
+    RCHECK(cudaDeviceSynchronize());
+    RCHECK(cudaMemcpy(hrgb, dc, n * 3, cudaMemcpyDeviceToHost));
+cleanup:
+    cudaFree(dz); cudaFree(dc);
+    return rc;
+}
+
+// The reference's colour table as 256 (R, G, B) triplets, read back from the
+// device, for callers that pass it to the engine's caller-given table.
+extern "C" int ref_turbo_table(uint8_t* out768) {
+    int rc = 0;
+    uint8_t r[256], g[256], b[256];
+    RCHECK(cudaMemcpyFromSymbol(r, stereo::turboR, 256));
+    RCHECK(cudaMemcpyFromSymbol(g, stereo::turboG, 256));
+    RCHECK(cudaMemcpyFromSymbol(b, stereo::turboB, 256));
+    for (int i = 0; i < 256; ++i) {
+        out768[3 * i] = r[i];
+        out768[3 * i + 1] = g[i];
+        out768[3 * i + 2] = b[i];
+    }
+cleanup:
     return rc;
 }

@@ -182,3 +182,57 @@ def test_host_point_cloud_matches_oracle():
         assert np.array_equal(np.isnan(got), nan)
         assert np.array_equal(got[~nan].view(np.int32), xyz[~nan].view(np.int32))
         assert np.array_equal(np.stack([rec["r"], rec["g"], rec["b"]], axis=1), rgb)
+
+
+# ---------------------------------------------------------------------------
+# The reference's own depth and colour kernels (oracle/_ref).
+# ---------------------------------------------------------------------------
+def _ref_or_skip():
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref not built (needs the reference tree at build time)")
+
+
+@pytest.mark.gpu
+def test_depth_and_colour_vs_reference_kernels():
+    """disparityToDepthKernel and colorizeDepthKernel (src/depth_map.cu:74-142)
+    against the depth-only pass, the colour-only pass and the fused pass, with
+    the reference's own colour table passed as the caller's table: depth bit
+    for bit, colours byte for byte.  Depth fields hold no NaN (a disparity map
+    never gives one; the reference's clamp of NaN under fast math is not part
+    of the comparison)."""
+    _ref_or_skip()
+    torch = pytest.importorskip("torch")
+    from lumenstereo_b200 import (depth_colorize_device, disparity_to_depth_color_device,
+                                  disparity_to_depth_device)
+    lut = oracle.ref_turbo_table()
+    rng = np.random.Generator(np.random.PCG64(21))
+    H, W = 257, 611
+    disp = rng.integers(-40, 300 * 16, (H, W)).astype(np.int16)
+    disp[0, :6] = [-1, 0, 1, 16, 32767, -32768]
+    dd = torch.from_numpy(disp).cuda()
+    for f, b, doffs, lo, hi in ((1400.0, 0.12, 0.0, 0.5, 10.0), (3997.684, 0.19395, 131.111, 1.0, 6.0),
+                                (2000.0, 0.3, -3.5, 0.2, 3.0)):
+        ref_z = oracle.ref_depth(disp, f, b, doffs)
+        ref_rgb = oracle.ref_colorize(ref_z, lo, hi)
+        z = torch.empty((H, W), dtype=torch.float32, device="cuda")
+        disparity_to_depth_device(dd.data_ptr(), W, H, f, b, z.data_ptr(), doffs)
+        z2 = torch.empty((H, W), dtype=torch.float32, device="cuda")
+        rgb = torch.empty((H, W, 3), dtype=torch.uint8, device="cuda")
+        disparity_to_depth_color_device(dd.data_ptr(), W, H, f, b, z2.data_ptr(), rgb.data_ptr(), lut, lo, hi,
+                                        doffs)
+        rgb2 = torch.empty((H, W, 3), dtype=torch.uint8, device="cuda")
+        depth_colorize_device(torch.from_numpy(ref_z).cuda().data_ptr(), W, H, rgb2.data_ptr(), lut, lo, hi)
+        torch.cuda.synchronize()
+        assert np.array_equal(z.cpu().numpy().view(np.int32), ref_z.view(np.int32)), (f, b, doffs)
+        assert np.array_equal(z2.cpu().numpy().view(np.int32), ref_z.view(np.int32)), (f, b, doffs)
+        assert np.array_equal(rgb.cpu().numpy(), ref_rgb), (f, b, doffs, lo, hi)
+        assert np.array_equal(rgb2.cpu().numpy(), ref_rgb), (f, b, doffs, lo, hi)
+    # a depth field with values below, inside and far above the colour range
+    zf = _depth_field((93, 177), 22)
+    zf = np.ascontiguousarray(np.where(np.isnan(zf), np.float32(0.0), zf), np.float32)
+    h2, w2 = zf.shape
+    for lo, hi in ((0.5, 10.0), (1.0, 1.5), (0.0, 30.0)):
+        out = torch.empty((h2, w2, 3), dtype=torch.uint8, device="cuda")
+        depth_colorize_device(torch.from_numpy(zf).cuda().data_ptr(), w2, h2, out.data_ptr(), lut, lo, hi)
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), oracle.ref_colorize(zf, lo, hi)), (lo, hi)
