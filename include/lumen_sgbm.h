@@ -113,23 +113,18 @@ const char* lumen_last_error_string(void);
  * the numDirections default. */
 lumen_status lumen_sgbm_debug_set_paths(lumen_sgbm* h, uint32_t path_mask);
 /* Aggregation schedule: 0 = automatic (autotuner / heuristic), 1 = one kernel
- * per direction, 2 = two fused wavefront sweeps (rows of a band in lockstep),
- * 3 = two fused wavefront sweeps with decoupled row warps and ticket-ordered
- * bands, 4 = two fused wavefront sweeps with lockstep row bands and helper
- * warps for the band hand-offs (the 4-path default), 5 = schedule 4 with
- * consecutive bands in thread-block clusters of up to 8 CTAs that hand rows
- * over through distributed shared memory, 6 = four lag-free two-path sweeps,
- * two over rows and two over columns (the 8-path default for padded
- * disparities up to 320; 4 paths or wider ranges fall back to schedule 4).
- * Outputs are identical for every schedule. */
+ * per direction, 4 = two fused wavefront sweeps with lockstep row bands and
+ * helper warps for the band hand-offs (the 4-path default and the batched
+ * form's kernel), 6 = four lag-free two-path sweeps, two over rows and two
+ * over columns (the 8-path default for padded disparities up to 320; 4 paths
+ * or wider ranges fall back to schedule 4).  Other values are refused
+ * (LUMEN_ERR_INVALID_ARGUMENT).  Outputs are identical for every schedule. */
 lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule);
-/* Pin the fused-sweep configuration: lanes per pixel (8, 16 or 32) and warps
- * per thread block (schedule 2: 2, 4, 8 or 16; rows per band = warps * 32 /
- * lanes).  Schedules 3-5 take `warps` as their rows per band: schedule 3 with
- * 32 lanes, 4 or 8 rows; schedules 4 and 5 with 32 lanes, 4, 8 or 16 rows;
- * schedule 4 with 8 lanes (padded disparities up to 128) or 16 lanes (up to
- * 256), rows as lane teams, 8, 16 or 32 rows.  0, 0 restores the automatic
- * choice.  Values are identical for every setting. */
+/* Pin the schedule-4 configuration: lanes per row (8, 16 or 32) and rows per
+ * band (`warps_per_block`): 32 lanes with 4, 8 or 16 rows; 8 lanes (padded
+ * disparities up to 128) or 16 lanes (up to 256), rows as lane teams, with
+ * 8, 16 or 32 rows.  0, 0 restores the automatic choice.  Values are
+ * identical for every setting. */
 lumen_status lumen_sgbm_set_tuning(lumen_sgbm* h, int lanes_per_pixel, int warps_per_block);
 /* The schedule and configuration the last compute used: {schedule, lanes, warps}. */
 lumen_status lumen_sgbm_get_tuning(const lumen_sgbm* h, int out[3]);
@@ -166,7 +161,7 @@ lumen_status lumen_sgbm_debug_trace_copy(lumen_sgbm* h, unsigned long long* dst,
 unsigned long long lumen_sgbm_debug_launch_count(const lumen_sgbm* h);
 /* Iteration limit of every device-side wait (0 restores the default, 2^22). */
 lumen_status lumen_sgbm_debug_set_wait_limit(lumen_sgbm* h, long long spins);
-/* Failure-path self test of schedules 3-6: while enabled, one wait of a band
+/* Failure-path self test of schedules 4 and 6: while enabled, one wait of a band
  * that imports from the band above can never be satisfied, so it runs out
  * after the wait limit and the compute returns LUMEN_ERR_TIMEOUT (no fault, no
  * hang; the handle stays usable). */

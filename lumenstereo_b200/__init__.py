@@ -248,7 +248,7 @@ class StereoSGBM:
         _check(_lib.lib().lumen_sgbm_debug_set_wait_limit(self._h, spins))
 
     def stall_test(self, enable: bool = True) -> None:
-        """Make one device-side wait of schedules 3-6 unsatisfiable (failure-path test)."""
+        """Make one device-side wait of schedules 4 and 6 unsatisfiable (failure-path test)."""
         _check(_lib.lib().lumen_sgbm_debug_stall_test(self._h, 1 if enable else 0))
 
     def set_tuning(self, lanes_per_pixel: int = 0, warps_per_block: int = 0) -> None:
@@ -281,7 +281,7 @@ class StereoSGBM:
         _check(_lib.lib().lumen_sgbm_debug_trace(self._h, int(enable)))
 
     def trace(self) -> np.ndarray:
-        """Band timeline of the last schedule-4/5 launch: one row per band
+        """Band timeline of the last schedule-4 launch: one row per band
         ticket (2*band + sweep): [first row at the middle pixel ns, last row at
         the middle pixel ns, end ns, sm << 48 | import polls << 32 | export
         polls << 16 | row waits]."""

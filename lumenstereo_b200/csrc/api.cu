@@ -282,8 +282,8 @@ extern "C" lumen_status lumen_sgbm_debug_set_paths(lumen_sgbm* h, uint32_t mask)
 
 extern "C" lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule) {
     if (!h) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL handle");
-    if (schedule < 0 || schedule > 6)
-        return fail(LUMEN_ERR_INVALID_ARGUMENT, "schedule must be 0, 1, 2, 3, 4, 5 or 6");
+    if (!(schedule == 0 || schedule == 1 || schedule == 4 || schedule == 6))
+        return fail(LUMEN_ERR_INVALID_ARGUMENT, "schedule must be 0 (automatic), 1, 4 or 6");
     h->schedule = schedule;
     return LUMEN_OK;
 }
@@ -449,7 +449,7 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
     PairView pv{h->cost.as<uint8_t>(), gl, h->agg.as<uint16_t>()};
     const bool sweepable = (mask == 0xFFu || mask == 0x0Fu);
     int sched = h->schedule;
-    SweepConfig cfg = h->forced.T ? h->forced : sweep_default_config(Dp, wrap);
+    SweepConfig cfg = h->forced.T ? h->forced : SweepConfig{32, 16};
     bool cfgChosen = h->forced.T != 0;  // pinned or tuned, not a schedule's default
     if (!h->forced.T && sched == 0) {
         auto it = h->tuned.find(tune_key(W, H, p, mask, wrap));
@@ -462,7 +462,7 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
     // untuned default: the four lag-free sweeps for 8 paths (schedule 6, which
     // falls back to schedule 4 where it has no instance), schedule 4 for 4 paths
     if (sched == 0) sched = mask == 0xFFu ? 6 : (sweepable ? 4 : 1);
-    if (sched >= 2 && !sweepable) sched = 1;          // single-path debug masks: per-direction kernels
+    if (sched != 1 && !sweepable) sched = 1;          // single-path debug masks: per-direction kernels
     PairPlan plan6{};
     if (sched == 6) {
         // 4 paths, no instance for this range, or short of device memory for
@@ -479,19 +479,6 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
         }
     }
     WavePlan plan4{};
-    if (sched == 5) {
-        // row bands in thread-block clusters: the largest cluster that plans
-        const int R = (cfg.T == 32 && (cfg.NW == 4 || cfg.NW == 8 || cfg.NW == 16)) ? cfg.NW : 8;
-        bool planned = false;
-        for (int cl : {8, 4, 2}) {
-            if (wave_plan(k, R, wrap, mask == 0xFFu, h->numSMs, &plan4, cl) == cudaSuccess) {
-                planned = true;
-                break;
-            }
-        }
-        if (planned) cfg = SweepConfig{32, plan4.R};
-        else sched = 4;
-    }
     // untuned default of the row-band sweeps: 16-row bands, rows as 8-lane
     // teams where the disparity range allows (the best plain configuration
     // measured on 1920x1080 D128; the autotuner refines it per workload)
@@ -500,7 +487,7 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
     if (sched == 4 && cfg.T != 32 && wave_team_exists(Dp, cfg.T) &&
         (cfg.NW == 8 || cfg.NW == 16 || cfg.NW == 32)) {
         // rows as lane teams of cfg.T lanes (an autotuner candidate)
-        if (wave_plan(k, cfg.NW, wrap, mask == 0xFFu, h->numSMs, &plan4, 1, cfg.T) == cudaSuccess)
+        if (wave_plan(k, cfg.NW, wrap, mask == 0xFFu, h->numSMs, &plan4, cfg.T) == cudaSuccess)
             teamPlanned = true;
         else
             cfg = SweepConfig{32, cfg.NW};
@@ -512,21 +499,9 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
             wave_plan(k, 4, wrap, mask == 0xFFu, h->numSMs, &plan4) == cudaSuccess) {
             cfg = SweepConfig{32, plan4.R};  // lanes per pixel, rows per band
         } else {
-            sched = 3;
-            cfg = sweep_default_config(Dp, wrap);
+            sched = 1;                       // no band fits shared memory: per-direction kernels
         }
     }
-    Sweep2Plan plan2{};
-    if (sched == 3) {
-        const int R = (cfg.T == 32 && (cfg.NW == 4 || cfg.NW == 8)) ? cfg.NW : 8;
-        if (sweep2_plan(k, R, wrap, mask == 0xFFu, h->numSMs, &plan2) == cudaSuccess) {
-            cfg = SweepConfig{32, R};
-        } else {
-            sched = 2;
-            cfg = sweep_default_config(Dp, wrap);
-        }
-    }
-    if (sched == 2 && !sweep_fits(W, Dp, cfg)) sched = 1;  // very wide images: per-direction kernels
     const uint16_t* aggB = nullptr;
     const uint16_t* aggC = nullptr;
     const uint16_t* aggD = nullptr;
@@ -552,7 +527,7 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
             nl += 3;
             aggB = aggC = aggD = nullptr;
         }
-    } else if (sched == 4 || sched == 5) {
+    } else if (sched == 4) {
         LCU(h->partB.ensure(ND * 2));
         LCU(h->xring.ensure(plan4.ringBytes));
         LCU(h->counters.ensure(sizeof(unsigned) * plan4.counterWords));
@@ -575,50 +550,12 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
             nl += 1;
             aggB = nullptr;
         }
-    } else if (sched == 3) {
-        LCU(h->partB.ensure(ND * 2));
-        LCU(h->xring.ensure(plan2.ringBytes));
-        LCU(h->counters.ensure(sizeof(unsigned) * plan2.counterWords));
-        LCU(launch_aggregate_sweep2(pv, h->partB.as<uint16_t>(), k, wrap, mask == 0xFFu, plan2,
-                                    h->xring.as<uint8_t>(), h->counters.as<unsigned>(),
-                                    h->status.as<int>(), h->spinMax, s, h->stallTest));
-        h->statusPending = true;
-        nl += 1;
-        aggB = h->partB.as<uint16_t>();
-        if (h->retain || select_needs_summed_volume(D, Dp)) {
-            launch_sum_volumes(h->agg.as<uint16_t>(), aggB, h->agg.as<uint16_t>(), ND, s);
-            LCU(cudaGetLastError());
-            nl += 1;
-            aggB = nullptr;
-        }
-    } else if (sched == 2) {
-        SweepPlan plan;
-        cudaError_t pe = sweep_plan(pv, k, cfg, wrap, mask == 0xFFu, h->numSMs, &plan);
-        if (pe != cudaSuccess) {  // this configuration cannot serve these parameters
-            cfg = sweep_default_config(Dp, wrap);
-            LCU(sweep_plan(pv, k, cfg, wrap, mask == 0xFFu, h->numSMs, &plan));
-        }
-        LCU(h->partB.ensure(ND * 2));
-        LCU(h->xring.ensure(plan.ringBytes));
-        LCU(h->counters.ensure(sizeof(unsigned) * plan.counterWords));
-        LCU(launch_aggregate_sweep(pv, h->partB.as<uint16_t>(), k, wrap, mask == 0xFFu, cfg, plan,
-                                   h->xring.as<uint8_t>(), h->counters.as<unsigned>(),
-                                   h->status.as<int>(), h->spinMax, s, h->numSMs));
-        h->statusPending = true;
-        nl += 1;  // the sweep kernel (the counter reset is a memset, not a kernel)
-        aggB = h->partB.as<uint16_t>();
-        if (h->retain || select_needs_summed_volume(D, Dp)) {
-            launch_sum_volumes(h->agg.as<uint16_t>(), aggB, h->agg.as<uint16_t>(), ND, s);
-            LCU(cudaGetLastError());
-            nl += 1;
-            aggB = nullptr;
-        }
     } else {
         LCU(launch_aggregate_per_direction(pv, k, mask, wrap, s));
         nl += __builtin_popcount(mask);
     }
     h->lastSchedule = sched;
-    h->lastConfig = sched >= 2 ? cfg : SweepConfig{0, 0};
+    h->lastConfig = sched != 1 ? cfg : SweepConfig{0, 0};
     if (timed) LCU(cudaEventRecord(h->ev[3], s));
     // selection + post-processing
     LCU(launch_select(h->agg.as<uint16_t>(), aggB, wrap, W, H, D, Dp, p.minDisparity,
@@ -709,16 +646,7 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
     std::vector<std::pair<int, SweepConfig>> cands;
     cands.push_back({1, SweepConfig{0, 0}});
     if (mask == 0xFFu || mask == 0x0Fu) {
-        SweepConfig cs[8];
-        const int n = sweep_configs(Dp, cs, 8);
-        for (int i = 0; i < n; ++i) {
-            if (wrap && !(cs[i].T == 32 && cs[i].NW == 4)) continue;
-            if (!sweep_fits(width, Dp, cs[i])) continue;
-            cands.push_back({2, cs[i]});
-        }
         int rs[4];
-        const int nr = sweep2_rows_options(Dp, rs, 4);
-        for (int i = 0; i < nr; ++i) cands.push_back({3, SweepConfig{32, rs[i]}});
         const int nw = wave_rows_options(Dp, rs, 4);
         for (int i = 0; i < nw; ++i) cands.push_back({4, SweepConfig{32, rs[i]}});
         for (int tl : {8, 16}) {
@@ -727,7 +655,6 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
             cands.push_back({4, SweepConfig{tl, 16}});
             cands.push_back({4, SweepConfig{tl, 32}});
         }
-        for (int i = 0; i < nw; ++i) cands.push_back({5, SweepConfig{32, rs[i]}});
         if (mask == 0xFFu) cands.push_back({6, SweepConfig{0, 0}});
     }
     const SweepConfig savedForced = h->forced;
@@ -784,7 +711,9 @@ extern "C" lumen_status lumen_sgbm_tuning_load(lumen_sgbm* h, const char* path) 
     if (!f) return fail(LUMEN_ERR_INVALID_ARGUMENT, std::string("cannot read ") + path);
     std::string key;
     int sched, T, NW;
-    while (f >> key >> sched >> T >> NW) h->tuned[key] = {sched, SweepConfig{T, NW}};
+    while (f >> key >> sched >> T >> NW)
+        if (sched == 1 || sched == 4 || sched == 6)  // entries of retired schedules are skipped
+            h->tuned[key] = {sched, SweepConfig{T, NW}};
     return LUMEN_OK;
 }
 

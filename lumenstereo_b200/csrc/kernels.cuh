@@ -33,47 +33,12 @@ cudaError_t launch_sad_cost(const uint8_t* pl, const uint8_t* pr, int W, int H, 
 cudaError_t launch_aggregate_per_direction(const PairView& pv, const SgmConsts& k,
                                            unsigned pathMask, bool wrap, cudaStream_t s);
 
-// Sweep schedule (two fused wavefront sweeps): forward partial into pv.agg,
-// backward partial into partB.  A configuration is T lanes per pixel and NW
-// warps per CTA (rows per band = NW * 32 / T).
+// A fused-sweep configuration: T lanes per pixel (row) and NW rows per band
+// (schedule 4) -- the autotuner's unit.
 struct SweepConfig {
     int T;
     int NW;
 };
-struct SweepPlan {
-    int G;                 // CTAs per sweep
-    int nBands;            // bands per sweep
-    int K;                 // exchange ring capacity (pixels)
-    size_t ringBytes;      // bytes of exchange rings
-    size_t counterWords;   // progress counters (uint32)
-};
-int sweep_configs(int Dp, SweepConfig* out, int max);
-SweepConfig sweep_default_config(int Dp, bool wrap);
-bool sweep_fits(int W, int Dp, SweepConfig c);
-cudaError_t sweep_plan(const PairView& pv, const SgmConsts& k, SweepConfig c, bool wrap, bool diag,
-                       int numSMs, SweepPlan* plan);
-cudaError_t launch_aggregate_sweep(const PairView& pv, uint16_t* partB, const SgmConsts& k,
-                                   bool wrap, bool diag, SweepConfig c, const SweepPlan& plan,
-                                   uint8_t* xring, unsigned* counters, int* status,
-                                   long long spinMax, cudaStream_t s, int numSMs);
-
-// ---- schedule 3: decoupled-row fused sweeps (sweep2.cu, sweep2_kernel.cuh) ----
-struct Sweep2Plan {
-    int R;                 // rows per band (warps per CTA = R + 2)
-    int QB;                // import / last-row ring slots
-    int nBands;            // bands per sweep
-    int M;                 // exchange rows per sweep
-    int grid;              // CTAs launched (persistent, ticket-scheduled)
-    int smem;              // dynamic shared memory per CTA
-    size_t ringBytes;      // exchange rows, both sweeps
-    size_t counterWords;   // prod + cons + ticket
-};
-int sweep2_rows_options(int Dp, int* out, int max);
-cudaError_t sweep2_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSMs, Sweep2Plan* plan);
-cudaError_t launch_aggregate_sweep2(const PairView& pv, uint16_t* partB, const SgmConsts& k,
-                                    bool wrap, bool diag, const Sweep2Plan& plan, uint8_t* xring,
-                                    unsigned* counters, int* status, long long spinMax,
-                                    cudaStream_t s, int stallTest = 0);
 
 // ---- schedule 4: lockstep row-band fused sweeps (wave.cu, wave_kernel.cuh) ----
 struct WavePlan {
@@ -82,18 +47,15 @@ struct WavePlan {
     int nBands;            // bands per sweep
     int grid;              // CTAs launched (persistent, ticket-scheduled)
     int smem;              // dynamic shared memory per CTA
-    int CL = 1;            // CTAs per thread-block cluster (1: none)
     int T = 32;            // lanes per row (batched launches: 8 or 16)
     int nTickets = 0;      // tickets of a single-pair launch
     size_t ringBytes;      // exchange rings, both sweeps
     size_t counterWords;   // prod + cons + ticket
 };
 int wave_rows_options(int Dp, int* out, int max);
-// CL > 1: consecutive bands of a sweep run in thread-block clusters of CL CTAs
-// (hand-offs inside a cluster through distributed shared memory).
-// T < 32: rows as teams of T lanes (wave_team_lanes(Dp) only, no clusters).
+// T < 32: rows as teams of T lanes (wave_team_exists(Dp, T) only).
 cudaError_t wave_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSMs, WavePlan* plan,
-                      int CL = 1, int T = 32);
+                      int T = 32);
 // the team width of the batched launches for a padded disparity count (32:
 // none), and whether a team kernel of T lanes exists for it
 int wave_team_lanes(int Dp);

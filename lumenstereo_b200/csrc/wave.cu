@@ -77,7 +77,7 @@ int wave_rows_options(int Dp, int* out, int max) {
 // Shared-memory fit (largest helper rings) and occupancy of one kernel class
 // at a widest image Wmax.
 static cudaError_t plan_class(int Wmax, int Dp, int R, bool wrap, bool full, bool diag, int numSMs,
-                              WavePlan* plan, int CL = 1, int T = 32) {
+                              WavePlan* plan, int T = 32) {
     // 32-row bands only as lane teams (at most 8 row warps)
     if (R != 4 && R != 8 && R != 16 && !(R == 32 && T != 32)) return cudaErrorInvalidValue;
     const int NP = diag ? 3 : 1;
@@ -98,7 +98,6 @@ static cudaError_t plan_class(int Wmax, int Dp, int R, bool wrap, bool full, boo
     a.Dp = Dp;
     a.Wmax = Wmax;
     a.QI = a.QX = Q;
-    a.CL = CL;
     int perSM = 0;
     cudaError_t e = dispatch_wave(a, R, NP, wrap, full, L.total, 0, nullptr, &perSM, T);
     if (e != cudaSuccess) return e;
@@ -107,9 +106,8 @@ static cudaError_t plan_class(int Wmax, int Dp, int R, bool wrap, bool full, boo
     plan->R = R;
     plan->Q = Q;
     plan->smem = L.total;
-    plan->CL = CL;
     // capacity; callers clamp to their ticket count
-    plan->grid = CL > 1 ? perSM * CL : perSM * numSMs;
+    plan->grid = perSM * numSMs;
     return cudaSuccess;
 }
 
@@ -118,22 +116,18 @@ size_t wave_ring_bytes(int nBands, int Dp, bool diag) {
 }
 
 cudaError_t wave_plan(const SgmConsts& k, int R, bool wrap, bool diag, int numSMs, WavePlan* plan,
-                      int CL, int T) {
-    if (CL != 1 && CL != 2 && CL != 4 && CL != 8) return cudaErrorInvalidValue;
-    if (T != 32 && (CL != 1 || !wave_team_exists(k.Dp, T))) return cudaErrorInvalidValue;
-    cudaError_t e = plan_class(k.W, k.Dp, R, wrap, k.D == k.Dp, diag, numSMs, plan, CL, T);
+                      int T) {
+    if (T != 32 && !wave_team_exists(k.Dp, T)) return cudaErrorInvalidValue;
+    cudaError_t e = plan_class(k.W, k.Dp, R, wrap, k.D == k.Dp, diag, numSMs, plan, T);
     if (e != cudaSuccess) return e;
     plan->nBands = (k.H + R - 1) / R;
-    // tickets alternate the two sweeps; with clusters a ticket holds CL
-    // consecutive bands.  The oldest unfinished ticket needs the tickets
-    // holding the next wave_lookahead_bands(W) bands of its sweep running.
-    const int perTicket = CL;
-    const int groups = (plan->nBands + perTicket - 1) / perTicket;
-    plan->nTickets = 2 * groups;
-    const int window = 2 * ((wave_lookahead_bands(k.W) + perTicket - 1) / perTicket + 1);
-    const int capTickets = plan->grid / CL;  // resident CTAs (clusters) that take tickets
-    if (capTickets < std::min(plan->nTickets, window + 1)) return cudaErrorInvalidConfiguration;
-    plan->grid = std::min(plan->nTickets, capTickets) * CL;
+    // tickets alternate the two sweeps.  The oldest unfinished ticket needs
+    // the tickets holding the next wave_lookahead_bands(W) bands of its sweep
+    // running.
+    plan->nTickets = 2 * plan->nBands;
+    const int window = 2 * (wave_lookahead_bands(k.W) + 1);
+    if (plan->grid < std::min(plan->nTickets, window + 1)) return cudaErrorInvalidConfiguration;
+    plan->grid = std::min(plan->nTickets, plan->grid);
     plan->ringBytes = wave_ring_bytes(plan->nBands, k.Dp, diag);
     plan->counterWords = 4 * (size_t)plan->nBands + 32;
     return cudaSuccess;
@@ -165,7 +159,6 @@ cudaError_t launch_aggregate_wave(const PairView& pv, uint16_t* partB, const Sgm
     a.jobs = nullptr;
     a.table = nullptr;
     a.nTickets = plan.nTickets;
-    a.CL = plan.CL;
     a.Wmax = k.W;
     a.ticket = counters + 4 * plan.nBands;
     a.status = status;
@@ -187,7 +180,7 @@ cudaError_t wave_batch_plan(int Wmax, int Dp, int R, bool wrap, bool full, bool 
     // teams where they exist (8 or 16 rows per band) and were asked for, full warps otherwise
     const int T = teams ? wave_team_lanes(Dp) : 32;
     if (T != 32 && (R == 8 || R == 16) &&
-        plan_class(Wmax, Dp, R, wrap, full, diag, numSMs, plan, 1, T) == cudaSuccess)
+        plan_class(Wmax, Dp, R, wrap, full, diag, numSMs, plan, T) == cudaSuccess)
         return cudaSuccess;
     return plan_class(Wmax, Dp, R, wrap, full, diag, numSMs, plan);
 }

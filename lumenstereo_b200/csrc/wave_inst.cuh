@@ -6,33 +6,15 @@
 namespace lumen {
 
 // grid == 0: report the CTAs per SM that fit (occupancy) in *perSM, launch
-// nothing; with clusters (a.CL > 1) the clusters that fit on the whole GPU.
+// nothing.
 template <int KW, bool WRAP, bool FULL, int NP, int R, int T = 32>
 cudaError_t wave_launch_t(const WaveArgs& a, int smem, int grid, cudaStream_t s, int* perSM) {
     auto kern = wave_kernel<KW, WRAP, FULL, NP, R, T>;
     constexpr int threads = (R / (32 / T) + 2) * 32;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    if (a.CL <= 1) {
-        if (grid == 0) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, kern, threads, smem);
-        kern<<<grid, threads, smem, s>>>(a);
-        return cudaGetLastError();
-    }
-    cudaLaunchConfig_t cfg{};
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = (unsigned)a.CL;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.gridDim = dim3((unsigned)(grid ? grid : a.CL));
-    cfg.blockDim = dim3(threads);
-    cfg.dynamicSmemBytes = (size_t)smem;
-    cfg.stream = s;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    if (grid == 0) return cudaOccupancyMaxActiveClusters(perSM, kern, &cfg);
-    e = cudaLaunchKernelEx(&cfg, kern, a);
-    if (e != cudaSuccess) return e;
+    if (grid == 0) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, kern, threads, smem);
+    kern<<<grid, threads, smem, s>>>(a);
     return cudaGetLastError();
 }
 

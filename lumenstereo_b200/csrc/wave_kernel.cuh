@@ -89,8 +89,6 @@ struct WaveArgs {
     int* status;
     int Dp;
     int QI, QX;              // import / export ring slots (16 or 8)
-    int CL;                  // CTAs per thread-block cluster (1: no cluster); tickets then
-                             // cover CL consecutive bands of a sweep, one per CTA rank
     long long spinMax;
     int stallTest;           // 1: ticket 2 (a band with a predecessor) waits on a pixel never exported
     unsigned long long* trace;  // optional [nTickets][4] band timeline
@@ -160,39 +158,6 @@ __device__ __forceinline__ unsigned w_ld_acquire_cta(const unsigned* p) {
 }
 __device__ __forceinline__ void w_st_release_cta(unsigned* p, unsigned v) {
     asm volatile("st.release.cta.shared::cta.u32 [%0], %1;\n" ::"r"(w_smem_addr(p)), "r"(v) : "memory");
-}
-// Cluster scope (consecutive bands in one thread-block cluster hand rows over
-// through distributed shared memory).
-__device__ __forceinline__ unsigned w_ld_acquire_cl(const unsigned* p) {
-    unsigned v;
-    asm volatile("ld.acquire.cluster.shared::cta.u32 %0, [%1];\n" : "=r"(v) : "r"(w_smem_addr(p)) : "memory");
-    return v;
-}
-__device__ __forceinline__ void w_st_release_cl(unsigned* p, unsigned v) {
-    asm volatile("st.release.cluster.shared::cta.u32 [%0], %1;\n" ::"r"(w_smem_addr(p)), "r"(v) : "memory");
-}
-// shared::cluster address of the same shared-memory offset in CTA `rank`
-__device__ __forceinline__ uint32_t w_mapa(uint32_t smemAddr, unsigned rank) {
-    uint32_t r;
-    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(smemAddr), "r"(rank));
-    return r;
-}
-__device__ __forceinline__ void w_st_remote(uint32_t addr, uint32_t v) {
-    asm volatile("st.shared::cluster.u32 [%0], %1;\n" ::"r"(addr), "r"(v) : "memory");
-}
-__device__ __forceinline__ void w_st_release_remote(uint32_t addr, uint32_t v) {
-    asm volatile("st.release.cluster.shared::cluster.u32 [%0], %1;\n" ::"r"(addr), "r"(v) : "memory");
-}
-__device__ __forceinline__ unsigned w_ld_acquire_remote(uint32_t addr) {
-    unsigned v;
-    asm volatile("ld.acquire.cluster.shared::cluster.u32 %0, [%1];\n" : "=r"(v) : "r"(addr) : "memory");
-    return v;
-}
-// Every thread of every CTA of the cluster; orders all prior memory accesses
-// of the cluster before all later ones.
-__device__ __forceinline__ void w_cluster_sync() {
-    asm volatile("barrier.cluster.arrive.release.aligned;\n"
-                 "barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
 // Named barrier 1 over the band's row-warp threads.
 __device__ __forceinline__ void w_rows_barrier(int nThreads) {
@@ -269,65 +234,6 @@ __device__ __forceinline__ bool w_wait_cta(const unsigned* p, unsigned need, uns
         }
         // back off: a spinning helper warp would take issue slots from the rows
         __nanosleep(40);
-    }
-}
-
-// w_wait_cta for a counter that another CTA of the cluster writes (acquire at
-// cluster scope).
-__device__ __forceinline__ bool w_wait_cl(const unsigned* p, unsigned need, unsigned& cache,
-                                          volatile int* abortFlag, int* status, long long spinMax,
-                                          volatile int* polls = nullptr) {
-    if (cache >= need) return true;
-    unsigned v = w_ld_acquire_cl(p);
-    if (__all_sync(kFullMask, v >= need)) {
-        cache = __shfl_sync(kFullMask, v, 0);
-        return true;
-    }
-    if (polls && (threadIdx.x & 31) == 0) atomicAdd((int*)polls, 1);
-    long long k = 0;
-    for (;;) {
-        v = w_ld_acquire_cl(p);
-        if (__all_sync(kFullMask, v >= need)) {
-            cache = __shfl_sync(kFullMask, v, 0);
-            return true;
-        }
-        if (__shfl_sync(kFullMask, *abortFlag, 0)) return false;
-        if ((k & 1023) == 1023 && __shfl_sync(kFullMask, *(volatile int*)status, 0) != 0) {
-            *abortFlag = 1;
-            return false;
-        }
-        if (++k >= spinMax) {
-            if ((threadIdx.x & 31) == 0) atomicExch(status, (int)LUMEN_ERR_TIMEOUT);
-            *abortFlag = 1;
-            return false;
-        }
-        __nanosleep(20);
-    }
-}
-
-// Bounded wait (whole warp) until a counter in another CTA of the cluster
-// (shared::cluster address) is >= need.
-__device__ __forceinline__ bool w_wait_remote(uint32_t addr, unsigned need, unsigned& cache,
-                                              volatile int* abortFlag, int* status, long long spinMax) {
-    if (cache >= need) return true;
-    long long k = 0;
-    for (;;) {
-        const unsigned v = w_ld_acquire_remote(addr);
-        if (__all_sync(kFullMask, v >= need)) {
-            cache = __shfl_sync(kFullMask, v, 0);
-            return true;
-        }
-        if (__shfl_sync(kFullMask, *abortFlag, 0)) return false;
-        if ((k & 1023) == 1023 && __shfl_sync(kFullMask, *(volatile int*)status, 0) != 0) {
-            *abortFlag = 1;
-            return false;
-        }
-        if (++k >= spinMax) {
-            if ((threadIdx.x & 31) == 0) atomicExch(status, (int)LUMEN_ERR_TIMEOUT);
-            *abortFlag = 1;
-            return false;
-        }
-        __nanosleep(20);
     }
 }
 
@@ -445,12 +351,7 @@ wave_kernel(WaveArgs a) {
     const int tl = lane & (T - 1);  // lane within the row's team
     const int off = tl * 2 * KW;    // first disparity of this lane
 
-    // cluster mode: this CTA's rank; [16 + rank] of rank 0's sflag: the rank's stop request
-    const int CL = a.CL;
-    unsigned crank = 0;
-    if (CL > 1) asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(crank));
     if (threadIdx.x == 0) sflag[1] = 0;
-    if (threadIdx.x < 8) sflag[16 + threadIdx.x] = 0;
     for (int i = threadIdx.x; i < SB / 4; i += blockDim.x)
         reinterpret_cast<uint32_t*>(sm + L.zero)[i] = 0u;
     __syncthreads();
@@ -459,32 +360,14 @@ wave_kernel(WaveArgs a) {
     int lutP1 = -1, lutP2 = -1, maskD = -1;  // parameters the table and masks were built for
 
     for (;;) {
-        if (CL > 1) {
-            // A: every band of the cluster's previous ticket is done and no
-            // access to another CTA's shared memory is in flight.  Rank 0
-            // takes the next ticket (or stops the whole cluster) and hands it
-            // to every rank; B: tickets delivered, counters reset everywhere.
-            w_cluster_sync();
-            if (crank == 0 && threadIdx.x == 0) {
-                int stop = *(volatile int*)a.status != 0;
-                for (int i = 0; i < CL; ++i) stop |= sflag[16 + i];
-                const int tt = stop ? a.nTickets : (int)atomicAdd(a.ticket, 1u);
-                const uint32_t local = w_smem_addr((const void*)sflag);
-                for (int i = 0; i < CL; ++i) w_st_remote(w_mapa(local, (unsigned)i), (uint32_t)tt);
-            }
-            if (threadIdx.x == 0) { sflag[2] = 0; sflag[3] = 0; sflag[4] = 0; }
-            if (threadIdx.x < 4) sctr[threadIdx.x] = 0u;
-            w_cluster_sync();
-        } else {
-            if (threadIdx.x == 0) {
-                int t = (int)atomicAdd(a.ticket, 1u);
-                if (*(volatile int*)a.status != 0) t = a.nTickets;
-                sflag[0] = t;
-                sflag[2] = 0; sflag[3] = 0; sflag[4] = 0;
-            }
-            if (threadIdx.x < 4) sctr[threadIdx.x] = 0u;
-            __syncthreads();
+        if (threadIdx.x == 0) {
+            int t = (int)atomicAdd(a.ticket, 1u);
+            if (*(volatile int*)a.status != 0) t = a.nTickets;
+            sflag[0] = t;
+            sflag[2] = 0; sflag[3] = 0; sflag[4] = 0;
         }
+        if (threadIdx.x < 4) sctr[threadIdx.x] = 0u;
+        __syncthreads();
         const int t = sflag[0];
         if (t >= a.nTickets) break;
         int sw, b;
@@ -494,17 +377,13 @@ wave_kernel(WaveArgs a) {
             J = a.jobs[e >> 20];
             sw = (e >> 19) & 1;
             b = (int)(e & 0x7FFFFu);
-        } else if (CL > 1) {
-            J = a.job;
-            sw = t & 1;
-            b = (t >> 1) * CL + (int)crank;
         } else {
             J = a.job;
             sw = t & 1;
             b = t >> 1;
         }
-        const bool active = b < J.nBands;  // the last ticket of a sweep may not fill the cluster
-        const int tb = CL > 1 ? 2 * b + sw : t;  // band ticket (trace record, stall test)
+        const bool active = b < J.nBands;
+        const int tb = t;  // band ticket (trace record, stall test)
         const int W = J.W, H = J.H;
         if (J.P1 != lutP1 || J.P2 != lutP2) {
             // adaptive P2 (src/sgbm_kernels.cu:301-310) as a table of |dI|, replicated in both halves
@@ -521,11 +400,7 @@ wave_kernel(WaveArgs a) {
         const int v0 = b * R;
         const int lastActive = min(R - 1, H - 1 - v0);
         const bool hasPrev = b > 0, hasNext = b + 1 < J.nBands;
-        // hand-offs inside the cluster go CTA to CTA through shared memory:
-        // the exporting row writes straight into the next rank's import ring
-        const bool prevLocal = CL > 1 && crank > 0;
-        const bool nextLocal = CL > 1 && (int)crank < CL - 1 && hasNext;
-        const bool globalImport = hasPrev && !prevLocal, globalExport = hasNext && !nextLocal;
+        const bool globalImport = hasPrev, globalExport = hasNext;
         // ---- stage sweep-oriented image rows v0-1 .. v0+R-1 ----
         for (int i = threadIdx.x; i < (active ? (R + 1) * W : 0); i += blockDim.x) {
             const int rr = i / W, u = i - rr * W;
@@ -537,7 +412,7 @@ wave_kernel(WaveArgs a) {
             }
             simg[rr * L.Wp + u] = val;
         }
-        const unsigned stallPix = (a.stallTest && tb == (CL > 1 ? 2 * CL : 2)) ? (unsigned)W + 1u : 0u;
+        const unsigned stallPix = (a.stallTest && tb == 2) ? (unsigned)W + 1u : 0u;
         bool ok = true;
         __syncthreads();
         // [24..27]: globaltimer of the middle pixel in the first and the last row
@@ -610,10 +485,8 @@ wave_kernel(WaveArgs a) {
                 // ---- helper hand-offs (row 0 / the exporting row) ----
                 const int u0 = step, uE = step - LAG * lastActive;  // row 0's and the exporting row's pixel
                 if (warpImports && ok && u0 < W)
-                    ok = prevLocal ? w_wait_cl(&sctr[0], (unsigned)min(W, u0 + 2), impSeen, sflag + 1, a.status,
-                                               a.spinMax, a.trace ? sflag + 4 : nullptr)
-                                   : w_wait_cta(&sctr[0], (unsigned)min(W, u0 + 2), impSeen, sflag + 1, a.status,
-                                                a.spinMax, a.trace ? sflag + 4 : nullptr);
+                    ok = w_wait_cta(&sctr[0], (unsigned)min(W, u0 + 2), impSeen, sflag + 1, a.status,
+                                    a.spinMax, a.trace ? sflag + 4 : nullptr);
                 if (warpExports && ok && uE >= QX && uE < W)
                     ok = w_wait_cta(&sctr[3], (unsigned)(uE - QX + 1), expSeen, sflag + 1, a.status,
                                     a.spinMax, a.trace ? sflag + 4 : nullptr);
@@ -689,10 +562,7 @@ wave_kernel(WaveArgs a) {
                     __syncwarp();
                     if (tl == 0 && on && ok) {
                         if (exporter) w_st_release_cta(&sctr[2], (unsigned)(u + 1));
-                        if (importer0) {
-                            if (prevLocal) w_st_release_cl(&sctr[1], (unsigned)u);
-                            else w_st_release_cta(&sctr[1], (unsigned)u);
-                        }
+                        if (importer0) w_st_release_cta(&sctr[1], (unsigned)u);
                     }
                 }
                 if (RW > 1) w_rows_barrier(RW * 32);
@@ -737,32 +607,7 @@ wave_kernel(WaveArgs a) {
             }
         } else {
             // ===================== export warp: this band's last row =====================
-            if (nextLocal) {
-                // into the next rank's import ring, through distributed shared memory
-                const uint32_t rImp = w_mapa(w_smem_addr(sm + L.imp), crank + 1);
-                const uint32_t rAvail = w_mapa(w_smem_addr(&sctr[0]), crank + 1);
-                const uint32_t rFree = w_mapa(w_smem_addr(&sctr[1]), crank + 1);
-                unsigned availSeen = 0, freeSeen = 0;
-                for (int u = 0; u < W && ok; ++u) {
-                    ok = w_wait_cta(&sctr[2], (unsigned)(u + 1), availSeen, sflag + 1, a.status, a.spinMax);
-                    if (ok && u >= QI)
-                        ok = w_wait_remote(rFree, (unsigned)(u - QI + 1), freeSeen, sflag + 1, a.status, a.spinMax);
-                    if (!ok) break;
-                    const uint4* src = reinterpret_cast<const uint4*>(sm + L.exp + (u & (QX - 1)) * SB);
-                    const uint32_t dst = rImp + (uint32_t)((u & (QI - 1)) * SB);
-                    for (int i = lane; i < SB / 16; i += 32) {
-                        const uint4 v = src[i];
-                        asm volatile("st.shared::cluster.v4.u32 [%0], {%1, %2, %3, %4};\n" ::"r"(dst + 16 * i),
-                                     "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
-                                     : "memory");
-                    }
-                    __syncwarp();
-                    if (lane == 0) {
-                        w_st_release_cta(&sctr[3], (unsigned)(u + 1));
-                        w_st_release_remote(rAvail, (unsigned)(u + 1));
-                    }
-                }
-            } else if (globalExport) {
+            if (globalExport) {
                 uint8_t* xout = J.xring + ((size_t)(sw * J.nBands + b) * kWK) * SB;
                 unsigned* oprod = J.prod + sw * J.nBands + b;
                 const unsigned* ocons = J.cons + sw * J.nBands + b;
@@ -795,13 +640,6 @@ wave_kernel(WaveArgs a) {
             auto sat = [](int x) { return (unsigned long long)min(x, 0xFFFF); };
             rec[3] = ((unsigned long long)smid << 48) | (sat(sflag[2]) << 32) | (sat(sflag[3]) << 16) |
                      sat(sflag[4]);
-        }
-        if (CL > 1) {
-            // every rank reaches the next cluster barrier; rank 0 turns a stop
-            // request into the cluster's common exit
-            if (threadIdx.x == 0)
-                w_st_remote(w_mapa(w_smem_addr((const void*)(sflag + 16 + crank)), 0u), stop ? 1u : 0u);
-            continue;
         }
         if (stop) break;
     }

@@ -5,8 +5,9 @@ calls of src/calibration.cpp:253-266).
 
 CPU: the oracle's numpy restatement of the maps is pinned to maps OpenCV made
 (tests/golden/maps/rectify_maps.npz, written by tests/golden/maps/make_rectify_maps.py).
-GPU: the device maps agree with those within 2e-3 px (double on the device,
-float storage; OpenCV accumulates along the row); the device depth agrees
+GPU: the device maps agree with those within one float ulp (double on the
+device, float storage; OpenCV accumulates along the row) and rectify an image
+to the same bytes as OpenCV's maps; the device depth agrees
 with the IEEE float32 restatement within 4 ulp (the division is the
 fast-math one, like the reference's build)."""
 import os
@@ -36,15 +37,24 @@ def test_oracle_maps_match_opencv():
 
 @pytest.mark.gpu
 def test_device_maps_match_opencv():
+    """Device maps within one float ulp of OpenCV's, and an image rectified
+    through them identical to one rectified through OpenCV's maps."""
     torch = pytest.importorskip("torch")
-    from lumenstereo_b200 import rectify_maps_device
+    from lumenstereo_b200 import rectify_image_gpu, rectify_maps_device
+    rng = np.random.Generator(np.random.PCG64(31))
     for w, h, K, D, R, P, mx, my in _cams():
         dx = torch.empty((h, w), dtype=torch.float32, device="cuda")
         dy = torch.empty((h, w), dtype=torch.float32, device="cuda")
         rectify_maps_device(K, D, R, P, w, h, dx.data_ptr(), dy.data_ptr())
         torch.cuda.synchronize()
-        assert np.abs(dx.cpu().numpy() - mx).max() <= 2e-3
-        assert np.abs(dy.cpu().numpy() - my).max() <= 2e-3
+        gx, gy = dx.cpu().numpy(), dy.cpu().numpy()
+        ulp_x = np.abs(gx.view(np.int32).astype(np.int64) - mx.view(np.int32))
+        ulp_y = np.abs(gy.view(np.int32).astype(np.int64) - my.view(np.int32))
+        assert ulp_x.max() <= 1 and ulp_y.max() <= 1, (int(ulp_x.max()), int(ulp_y.max()))
+        img = rng.integers(0, 256, (h, w), dtype=np.uint8)
+        ours = rectify_image_gpu(img, gx, gy)
+        theirs = rectify_image_gpu(img, mx, my)
+        assert np.array_equal(ours, theirs), int((ours != theirs).sum())
 
 
 @pytest.mark.gpu
