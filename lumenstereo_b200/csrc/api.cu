@@ -73,6 +73,8 @@ struct lumen_sgbm {
     DevBuf inL, inR, gray[2], pref[2], census[2], cost, agg, dispL, dispR, out, dbgLR, magic;
     DevBuf partB, xring, counters, status;  // sweep schedule: backward partial, exchange rings
     DevBuf partC, partD;                    // schedule 6: the column sweeps' partials
+    DevBuf pairBuf;                         // schedule 6: band-boundary row buffers (epoch-tagged words)
+    unsigned pairEpoch = 0;                 // epoch of the last schedule-6 launch into pairBuf
     DevBuf trace;                           // lumen_sgbm_debug_trace: band timeline of schedule 4
     int traceOn = 0;
     size_t traceWords = 0;
@@ -175,7 +177,7 @@ extern "C" lumen_status lumen_sgbm_destroy(lumen_sgbm* h) {
     for (DevBuf* b : {&h->inL, &h->inR, &h->gray[0], &h->gray[1], &h->pref[0], &h->pref[1],
                       &h->census[0], &h->census[1], &h->cost, &h->agg, &h->dispL, &h->dispR,
                       &h->out, &h->dbgLR, &h->magic, &h->partB, &h->partC, &h->partD, &h->xring,
-                      &h->counters, &h->status, &h->trace})
+                      &h->pairBuf, &h->counters, &h->status, &h->trace})
         b->release();
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
@@ -467,11 +469,17 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
     if (sched == 6) {
         // 4 paths, no instance for this range, or short of device memory for
         // the four partial volumes and the row buffers: schedule 4
-        bool ok6 = mask == 0xFFu && pair_plan(k, wrap, h->numSMs, &plan6) == cudaSuccess;
+        // rows per band: a pinned or tuned 16 / 32, else the default
+        const int R6 = (cfgChosen && (cfg.NW == 16 || cfg.NW == 32)) ? cfg.NW : 0;
+        bool ok6 = mask == 0xFFu && pair_plan(k, wrap, h->numSMs, &plan6, R6) == cudaSuccess;
         if (ok6)
             ok6 = h->partB.ensure(ND * 2) == cudaSuccess && h->partC.ensure(ND * 2) == cudaSuccess &&
-                  h->partD.ensure(ND * 2) == cudaSuccess && h->xring.ensure(plan6.xbufBytes) == cudaSuccess &&
-                  h->counters.ensure(sizeof(unsigned) * plan6.counterWords) == cudaSuccess;
+                  h->partD.ensure(ND * 2) == cudaSuccess;
+        if (ok6 && h->pairBuf.n < plan6.xbufBytes) {
+            ok6 = h->pairBuf.ensure(plan6.xbufBytes) == cudaSuccess;
+            h->pairEpoch = 0xFFFFFFFFu;                // a new buffer: zeroed before its first use
+        }
+        if (ok6) ok6 = h->counters.ensure(sizeof(unsigned) * plan6.counterWords) == cudaSuccess;
         if (!ok6) {
             (void)cudaGetLastError();                  // a failed allocation is not a sticky error
             sched = 4;
@@ -509,12 +517,20 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
         LCU(h->partB.ensure(ND * 2));
         LCU(h->partC.ensure(ND * 2));
         LCU(h->partD.ensure(ND * 2));
-        LCU(h->xring.ensure(plan6.xbufBytes));
         LCU(h->counters.ensure(sizeof(unsigned) * plan6.counterWords));
+        // every word of the row buffers must carry an epoch below the launch's:
+        // zero them when they are new (marked by the epoch at its maximum) and
+        // before the epoch would wrap
+        if (h->pairEpoch >= 0xFFFFFFF0u) {
+            LCU(cudaMemsetAsync(h->pairBuf.p, 0, h->pairBuf.n, s));
+            h->pairEpoch = 0;
+        }
+        const unsigned epoch = ++h->pairEpoch;
         uint16_t* const parts[4] = {h->agg.as<uint16_t>(), h->partB.as<uint16_t>(), h->partC.as<uint16_t>(),
                                     h->partD.as<uint16_t>()};
-        LCU(launch_aggregate_pair(pv, parts, k, wrap, plan6, h->xring.as<uint8_t>(), h->counters.as<unsigned>(),
-                                  h->status.as<int>(), h->spinMax, s, h->stallTest));
+        LCU(launch_aggregate_pair(pv, parts, k, wrap, plan6, h->pairBuf.as<unsigned long long>(), epoch,
+                                  h->counters.as<unsigned>(), h->status.as<int>(), h->spinMax, s,
+                                  h->stallTest));
         h->statusPending = true;
         nl += 1;
         cfg = SweepConfig{plan6.T, plan6.R};
@@ -655,7 +671,10 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
             cands.push_back({4, SweepConfig{tl, 16}});
             cands.push_back({4, SweepConfig{tl, 32}});
         }
-        if (mask == 0xFFu) cands.push_back({6, SweepConfig{0, 0}});
+        if (mask == 0xFFu) {
+            cands.push_back({6, SweepConfig{8, 16}});   // schedule 6 takes `warps` as its rows per band
+            cands.push_back({6, SweepConfig{8, 32}});
+        }
     }
     const SweepConfig savedForced = h->forced;
     const int savedSched = h->schedule;

@@ -91,14 +91,20 @@ struct PairPlan {
     int grid;              // CTAs launched (persistent, ticket-scheduled)
     int smem;              // dynamic shared memory per CTA
     size_t xbufBytes;      // band-boundary row buffers, all sweeps
-    size_t counterWords;   // progress per band + ticket
+    size_t counterWords;   // the ticket counter
 };
-// cudaErrorInvalidValue: no instance for these disparities / sizes
-cudaError_t pair_plan(const SgmConsts& k, bool wrap, int numSMs, PairPlan* plan);
-// part[0..3]: the four sweeps' partial volumes (part[0] may be pv.agg)
+// lanes per row of schedule 6 for a padded disparity count (0: no instance)
+int pair_lanes(int Dp);
+// R: rows per band, 16 or 32 (0: the default, 16).  cudaErrorInvalidValue: no
+// instance for these disparities / sizes
+cudaError_t pair_plan(const SgmConsts& k, bool wrap, int numSMs, PairPlan* plan, int R = 0);
+// part[0..3]: the four sweeps' partial volumes (part[0] may be pv.agg).  xbuf:
+// the row buffers (plan.xbufBytes), every word of which holds an epoch below
+// `epoch` (zero-filled when allocated, then one epoch per launch, increasing).
 cudaError_t launch_aggregate_pair(const PairView& pv, uint16_t* const part[4], const SgmConsts& k, bool wrap,
-                                  const PairPlan& plan, uint8_t* xbuf, unsigned* counters, int* status,
-                                  long long spinMax, cudaStream_t s, int stallTest = 0);
+                                  const PairPlan& plan, unsigned long long* xbuf, unsigned epoch,
+                                  unsigned* counters, int* status, long long spinMax, cudaStream_t s,
+                                  int stallTest = 0);
 
 // aggB (nullable): second partial volume summed with agg (mod 2^16 when wrap);
 // aggC, aggD (nullable, both or neither): two more (schedule 6).

@@ -8,32 +8,52 @@
 
 namespace lumen {
 
-extern template cudaError_t pair_launch_t<4, 8>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
-extern template cudaError_t pair_launch_t<8, 8>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
-extern template cudaError_t pair_launch_t<6, 16>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
-extern template cudaError_t pair_launch_t<8, 16>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
-extern template cudaError_t pair_launch_t<10, 16>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
-
-constexpr int kPairRows = 16;
+#define LUMEN_PAIR_EXTERN(KW, T, R) \
+    extern template cudaError_t pair_launch_t<KW, T, R>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
+LUMEN_PAIR_EXTERN(4, 8, 16)
+LUMEN_PAIR_EXTERN(8, 8, 16)
+LUMEN_PAIR_EXTERN(4, 8, 32)
+LUMEN_PAIR_EXTERN(8, 8, 32)
+LUMEN_PAIR_EXTERN(6, 16, 16)
+LUMEN_PAIR_EXTERN(8, 16, 16)
+LUMEN_PAIR_EXTERN(10, 16, 16)
+LUMEN_PAIR_EXTERN(6, 16, 32)
+LUMEN_PAIR_EXTERN(8, 16, 32)
+LUMEN_PAIR_EXTERN(10, 16, 32)
+#undef LUMEN_PAIR_EXTERN
 
 // lanes per row for a padded disparity count (0: no instance)
-static int pair_lanes(int Dp) { return Dp <= 128 ? 8 : Dp <= 320 ? 16 : 0; }
+int pair_lanes(int Dp) { return Dp <= 128 ? 8 : Dp <= 320 ? 16 : 0; }
 
-static cudaError_t pair_dispatch(const PairArgs& a, int Dp, bool wrap, bool full, int smem, int grid,
+static cudaError_t pair_dispatch(const PairArgs& a, int Dp, int R, bool wrap, bool full, int smem, int grid,
                                  cudaStream_t s, int* perSM) {
-    switch (Dp) {
-    case 64: return pair_launch_t<4, 8>(a, wrap, full, smem, grid, s, perSM);
-    case 128: return pair_launch_t<8, 8>(a, wrap, full, smem, grid, s, perSM);
-    case 192: return pair_launch_t<6, 16>(a, wrap, full, smem, grid, s, perSM);
-    case 256: return pair_launch_t<8, 16>(a, wrap, full, smem, grid, s, perSM);
-    case 320: return pair_launch_t<10, 16>(a, wrap, full, smem, grid, s, perSM);
-    default: return cudaErrorInvalidValue;
+    if (R == 16) {
+        switch (Dp) {
+        case 64: return pair_launch_t<4, 8, 16>(a, wrap, full, smem, grid, s, perSM);
+        case 128: return pair_launch_t<8, 8, 16>(a, wrap, full, smem, grid, s, perSM);
+        case 192: return pair_launch_t<6, 16, 16>(a, wrap, full, smem, grid, s, perSM);
+        case 256: return pair_launch_t<8, 16, 16>(a, wrap, full, smem, grid, s, perSM);
+        case 320: return pair_launch_t<10, 16, 16>(a, wrap, full, smem, grid, s, perSM);
+        default: return cudaErrorInvalidValue;
+        }
     }
+    if (R == 32) {
+        switch (Dp) {
+        case 64: return pair_launch_t<4, 8, 32>(a, wrap, full, smem, grid, s, perSM);
+        case 128: return pair_launch_t<8, 8, 32>(a, wrap, full, smem, grid, s, perSM);
+        case 192: return pair_launch_t<6, 16, 32>(a, wrap, full, smem, grid, s, perSM);
+        case 256: return pair_launch_t<8, 16, 32>(a, wrap, full, smem, grid, s, perSM);
+        case 320: return pair_launch_t<10, 16, 32>(a, wrap, full, smem, grid, s, perSM);
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    return cudaErrorInvalidValue;
 }
 
-cudaError_t pair_plan(const SgmConsts& k, bool wrap, int numSMs, PairPlan* plan) {
+cudaError_t pair_plan(const SgmConsts& k, bool wrap, int numSMs, PairPlan* plan, int R) {
     if (!pair_lanes(k.Dp)) return cudaErrorInvalidValue;
-    const int R = kPairRows;
+    if (R == 0) R = 16;
+    if (R != 16 && R != 32) return cudaErrorInvalidValue;
     PairPlan p{};
     p.R = R;
     p.T = pair_lanes(k.Dp);
@@ -44,26 +64,26 @@ cudaError_t pair_plan(const SgmConsts& k, bool wrap, int numSMs, PairPlan* plan)
     if (p.smem > 227 * 1024) return cudaErrorInvalidValue;
     PairArgs dummy{};
     int perSM = 0;
-    cudaError_t e = pair_dispatch(dummy, k.Dp, wrap, k.D == k.Dp, p.smem, 0, nullptr, &perSM);
+    cudaError_t e = pair_dispatch(dummy, k.Dp, R, wrap, k.D == k.Dp, p.smem, 0, nullptr, &perSM);
     if (e != cudaSuccess) return e;
     if (perSM < 1) return cudaErrorInvalidConfiguration;
     p.grid = std::min(p.nTickets, perSM * numSMs);
-    p.xbufBytes = pair_xbase(3, p.nb1, k.W, k.H, p.nb0, p.nb1) * (size_t)pair_slot_bytes(k.Dp);
-    p.counterWords = (size_t)pair_poff(3, p.nb0, p.nb1) + p.nb1 + 1;   // progress per band + ticket
+    p.xbufBytes = pair_xbase(3, p.nb1, k.W, k.H, p.nb0, p.nb1) * (size_t)pair_ll_words(k.Dp) * 8;
+    p.counterWords = 1;   // the ticket counter
     *plan = p;
     return cudaSuccess;
 }
 
 cudaError_t launch_aggregate_pair(const PairView& pv, uint16_t* const part[4], const SgmConsts& k, bool wrap,
-                                  const PairPlan& plan, uint8_t* xbuf, unsigned* counters, int* status,
-                                  long long spinMax, cudaStream_t s, int stallTest) {
+                                  const PairPlan& plan, unsigned long long* xbuf, unsigned epoch,
+                                  unsigned* counters, int* status, long long spinMax, cudaStream_t s,
+                                  int stallTest) {
     PairArgs a{};
     PairJob& J = a.job;
     J.cost = pv.cost;
     J.img = pv.img;
     for (int i = 0; i < 4; ++i) J.part[i] = part[i];
     J.xbuf = xbuf;
-    J.prod = counters;
     J.W = k.W;
     J.H = k.H;
     J.D = k.D;
@@ -76,14 +96,15 @@ cudaError_t launch_aggregate_pair(const PairView& pv, uint16_t* const part[4], c
     J.bsub = k.bsub;
     a.nTickets = plan.nTickets;
     a.Lmax = std::max(k.W, k.H);
-    a.ticket = counters + plan.counterWords - 1;
+    a.ticket = counters;
     a.status = status;
     a.spinMax = spinMax;
+    a.epoch = epoch;
     a.stallTest = stallTest;
     cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned) * plan.counterWords, s);
     if (e != cudaSuccess) return e;
     int perSM = 0;
-    return pair_dispatch(a, k.Dp, wrap, k.D == k.Dp, plan.smem, plan.grid, s, &perSM);
+    return pair_dispatch(a, k.Dp, plan.R, wrap, k.D == k.Dp, plan.smem, plan.grid, s, &perSM);
 }
 
 }  // namespace lumen

@@ -19,18 +19,24 @@
 //
 // Work decomposition:
 //  * a CTA owns a band of R consecutive sweep rows, each row a team of T
-//    lanes (a lane holds 2*KW disparities as KW packed uint16x2 words); all
-//    rows advance in lockstep, one barrier per step;
+//    lanes (a lane holds 2*KW disparities as KW packed uint16x2 words); the
+//    row warps advance in lockstep, one barrier per step, which also takes
+//    the OR of every row's stop request so all rows leave at the same step;
 //  * row r reads row r-1's diagonal vector of pixel u-1 from a two-slot
 //    shared-memory ring written one step earlier;
-//  * the band's first row reads the band above's last row from a per-boundary
-//    row buffer in global memory: the producing row stores every pixel's
-//    vector there and publishes its progress every kPE pixels (release at
-//    GPU scope); the consuming row waits for pixel u (acquire, every lane)
-//    and loads it during step u for use at step u+1, so the load overlaps a
-//    step.  The row buffers hold whole rows, so a band never waits on the
-//    band below it: bands only depend on earlier tickets and any number of
-//    resident CTAs makes progress;
+//  * the band's last row writes its diagonal vector of every pixel into a
+//    per-boundary row buffer in global memory as 64-bit (payload, epoch)
+//    words, plain stores with no fence: a word is valid once its high half
+//    holds this launch's epoch.  The producing rows never wait on global
+//    memory;
+//  * an import warp outside the row barrier polls the band above's row
+//    buffer a few pixels ahead, copies every pixel whose words all carry the
+//    epoch into a kPQ-slot shared-memory ring and publishes the count (release
+//    at CTA scope); row 0 takes pixel u-1 from that ring at step u.  After
+//    each step's barrier the rows publish how many pixels row 0 has consumed,
+//    which frees ring slots.  The row buffers hold whole rows, so a band
+//    waits only on the band above it, never on the one below: bands depend
+//    only on earlier tickets and any number of resident CTAs makes progress;
 //  * matching costs are prefetched kPPF-1 pixels ahead with cp.async;
 //    adaptive P2 is looked up from staged image rows;
 //  * bands are handed out by a ticket counter, the four sweeps interleaved,
@@ -45,69 +51,75 @@
 namespace lumen {
 
 struct PairJob {
-    const uint8_t* cost;     // [H][W][Dp]
-    const uint8_t* img;      // [H][W] left gray image (adaptive P2)
-    uint16_t* part[4];       // per-sweep partial sums, [H][W][Dp]
-    uint8_t* xbuf;           // band-boundary rows (pair_xbase), pair_slot_bytes(Dp) bytes a pixel
-    unsigned* prod;          // [pair_poff(4)] pixels of band b's last row published
+    const uint8_t* cost;           // [H][W][Dp]
+    const uint8_t* img;            // [H][W] left gray image (adaptive P2)
+    uint16_t* part[4];             // per-sweep partial sums, [H][W][Dp]
+    unsigned long long* xbuf;      // band-boundary rows: pair_ll_words(Dp) words a pixel (pair_xbase)
     int W, H, D;
-    int nb[2];               // bands of the row sweeps (0, 1) and of the column sweeps (2, 3)
+    int nb[2];                     // bands of the row sweeps (0, 1) and of the column sweeps (2, 3)
     int P1, P2, costScale;
     uint32_t p1x2, bsub;
 };
 
 struct PairArgs {
     PairJob job;
-    int nTickets;            // 2 * nb[0] + 2 * nb[1]
-    int Lmax;                // max(W, H): staged image row length
+    int nTickets;                  // 2 * nb[0] + 2 * nb[1]
+    int Lmax;                      // max(W, H): staged image row length
     unsigned* ticket;
     int* status;
     long long spinMax;
-    int stallTest;           // 1: ticket 4 (band 1 of sweep 0) waits on a pixel never published
+    unsigned epoch;                // high half of every row-buffer word this launch writes
+    int stallTest;                 // 1: ticket 4 (band 1 of sweep 0) waits for an epoch never written
 };
 
-// Bounded wait (whole warp) until the global counter *p >= need; every lane
-// acquires its own sufficient value, so each lane's later loads of the data
-// the counter publishes are ordered after it.
-__device__ __forceinline__ bool p_wait_gpu(const unsigned* p, unsigned need, unsigned& cache,
-                                           volatile int* abortFlag, int* status, long long spinMax) {
-    if (cache >= need) return true;
-    long long k = 0;
-    for (;;) {
-        const unsigned v = w_ld_acquire_gpu(p);
-        if (__all_sync(kFullMask, v >= need)) {
-            cache = __shfl_sync(kFullMask, v, 0);
-            return true;
-        }
-        if (__shfl_sync(kFullMask, *abortFlag, 0)) return false;
-        if ((k & 63) == 63 && __shfl_sync(kFullMask, *(volatile int*)status, 0) != 0) {
-            *abortFlag = 1;
-            return false;
-        }
-        if (++k >= spinMax) {
-            if ((threadIdx.x & 31) == 0) atomicExch(status, (int)LUMEN_ERR_TIMEOUT);
-            *abortFlag = 1;
-            return false;
-        }
-        __nanosleep(32);
-    }
+// 64-bit (payload, epoch) words of the row buffers: volatile accesses reach
+// the GPU-wide L2 and each 64-bit element is single-copy atomic, so a reader
+// sees a word either from an earlier launch or complete from this one.
+__device__ __forceinline__ void ll_store2(unsigned long long* p, unsigned long long a, unsigned long long b) {
+    asm volatile("st.volatile.global.v2.u64 [%0], {%1, %2};\n" ::"l"(p), "l"(a), "l"(b) : "memory");
+}
+__device__ __forceinline__ void ll_load2(const unsigned long long* p, unsigned long long& a,
+                                         unsigned long long& b) {
+    asm volatile("ld.volatile.global.v2.u64 {%0, %1}, [%2];\n" : "=l"(a), "=l"(b) : "l"(p) : "memory");
+}
+
+// Named barrier 1 over the row warps' threads with an OR reduction: every
+// row thread gets the OR of all of their `v`.
+__device__ __forceinline__ bool rows_barrier_or(int nThreads, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n"
+        " .reg .pred p, q;\n"
+        " setp.ne.u32 p, %1, 0;\n"
+        " bar.red.or.pred q, 1, %2, p;\n"
+        " selp.u32 %0, 1, 0, q;\n"
+        "}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(nThreads)
+        : "memory");
+    return r != 0;
 }
 
 template <int KW, bool WRAP, bool FULL, int R, int T>
-__global__ void __launch_bounds__(R / (32 / T) * 32)
+__global__ void __launch_bounds__((R / (32 / T) + 1) * 32)
 pair_kernel(PairArgs a) {
     constexpr int DP = 2 * KW * T;       // padded disparities
     constexpr int SB = pair_slot_bytes(DP);
+    constexpr int NL = pair_ll_words(DP);
+    constexpr int PAIRS = NL / 2;        // 16-byte pairs of row-buffer words a pixel
     constexpr int RPW = 32 / T;          // rows per warp
     static_assert(R % RPW == 0, "whole warps of rows");
-    constexpr int RW = R / RPW;          // warps
-    static_assert(KW % 2 == 0, "a lane's cost bytes are whole 4-byte words");
+    constexpr int RW = R / RPW;          // row warps; warp RW imports
+    static_assert(KW % 2 == 0, "a lane's cost bytes are whole 4-byte words; its words pair up");
+    static_assert((kPQ & (kPQ - 1)) == 0 && kPG <= kPQ && kPG <= 32, "import ring");
     extern __shared__ __align__(128) uint8_t sm[];
     const PairSmem L = pair_smem(a.Lmax, DP, R);
     uint8_t* simg = sm + L.img;
     const uint32_t* p2lut = reinterpret_cast<const uint32_t*>(sm + L.lut);
     // [0] ticket, [1] abort
     volatile int* sflag = reinterpret_cast<volatile int*>(sm + L.misc);
+    // [0] pixels of the band above in the import ring, [1] pixels row 0 has consumed
+    unsigned* sctr = reinterpret_cast<unsigned*>(sm + L.misc) + 8;
     const uint8_t* const zeroSlot = sm + L.zero;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -133,6 +145,7 @@ pair_kernel(PairArgs a) {
             sflag[0] = t;
             sflag[1] = 0;
         }
+        if (threadIdx.x < 2) sctr[threadIdx.x] = 0u;
         __syncthreads();
         const int t = sflag[0];
         if (t >= a.nTickets) break;
@@ -159,136 +172,183 @@ pair_kernel(PairArgs a) {
             simg[rr * L.Lp + u] = val;
         }
         __syncthreads();
-
-        const bool rowOn = r <= lastActive;
-        const int v = v0 + min(r, lastActive);
-        int x0, y0;
-        pair_xy(s, 0, v, W, H, x0, y0);
-        const ptrdiff_t du = s == 0 ? 1 : s == 1 ? -1 : s == 2 ? (ptrdiff_t)W : -(ptrdiff_t)W;
-        const ptrdiff_t pix0 = (ptrdiff_t)y0 * W + x0;
-        uint16_t* const part = s == 0 ? J.part[0] : s == 1 ? J.part[1] : s == 2 ? J.part[2] : J.part[3];
-        uint16_t* pout = part + pix0 * DP + off;
-        const ptrdiff_t pstep = du * DP;
-        uint8_t* const costRing = sm + L.cost + r * kPPF * DP;
-        const uint8_t* irow = simg + (r + 1) * L.Lp;
-        const uint8_t* iprev = simg + r * L.Lp;
-        uint8_t* const mySlots = sm + L.slots + r * 2 * SB;
-        const uint8_t* const upSlots = sm + L.slots + (r > 0 ? r - 1 : 0) * 2 * SB;
-        const bool exporter = rowOn && r == lastActive && hasNext;
-        const bool warpExports = hasNext && warp == lastActive / RPW;
-        const bool warpImports = hasPrev && warp == 0;   // row 0 is in warp 0
-        uint8_t* const xout = hasNext ? J.xbuf + pair_xbase(s, b, W, H, J.nb[0], J.nb[1]) * SB : nullptr;
-        const uint8_t* const xin = hasPrev ? J.xbuf + pair_xbase(s, b - 1, W, H, J.nb[0], J.nb[1]) * SB : nullptr;
-        unsigned* const prodOut = J.prod + pair_poff(s, J.nb[0], J.nb[1]) + b;
-        const unsigned* const prodIn = J.prod + pair_poff(s, J.nb[0], J.nb[1]) + (b > 0 ? b - 1 : 0);
-        const unsigned stallNeed = (a.stallTest && t == 4) ? (unsigned)Ws + 1u : 0u;
-
-        auto prefetch = [&](int step) {
-            const int p = step + kPPF - 1;
-            if (rowOn && p >= 0 && p < Ws) {
-                const uint8_t* src = J.cost + (pix0 + (ptrdiff_t)p * du) * DP + off;
-                const uint32_t dst = w_smem_addr(costRing + (p % kPPF) * DP + off);
-                if constexpr ((2 * KW) % 16 == 0) {
-#pragma unroll
-                    for (int q = 0; q < (2 * KW) / 16; ++q) w_cp_async16(dst + 16 * q, src + 16 * q);
-                } else {
-#pragma unroll
-                    for (int q = 0; q < KW / 2; ++q)
-                        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst + 4 * q),
-                                     "l"(src + 4 * q)
-                                     : "memory");
-                }
-            }
-            w_cp_commit();
-        };
-        for (int st = -(kPPF - 1); st < 0; ++st) prefetch(st);
-
-        uint32_t LH[KW], imp[KW];
-#pragma unroll
-        for (int w = 0; w < KW; ++w) { LH[w] = 0; imp[w] = 0; }
-        uint32_t minH = 0, impMin = 0;
-        unsigned seen = 0;
         bool ok = true;
-        for (int u = 0; u < Ws; ++u) {
-            // ---- the band above's pixel u-1 (loaded last step); load pixel u for the next step ----
-            uint32_t pred[KW];
+
+        if (warp < RW) {
+            // ===================== row warps, lockstep =====================
+            const bool rowOn = r <= lastActive;
+            const int v = v0 + min(r, lastActive);
+            int x0, y0;
+            pair_xy(s, 0, v, W, H, x0, y0);
+            const ptrdiff_t du = s == 0 ? 1 : s == 1 ? -1 : s == 2 ? (ptrdiff_t)W : -(ptrdiff_t)W;
+            const ptrdiff_t pix0 = (ptrdiff_t)y0 * W + x0;
+            uint16_t* const part = s == 0 ? J.part[0] : s == 1 ? J.part[1] : s == 2 ? J.part[2] : J.part[3];
+            uint16_t* pout = part + pix0 * DP + off;
+            const ptrdiff_t pstep = du * DP;
+            uint8_t* const costRing = sm + L.cost + r * kPPF * DP;
+            const uint8_t* irow = simg + (r + 1) * L.Lp;
+            const uint8_t* iprev = simg + r * L.Lp;
+            uint8_t* const mySlots = sm + L.slots + r * 2 * SB;
+            const uint8_t* const upSlots = sm + L.slots + (r > 0 ? r - 1 : 0) * 2 * SB;
+            const uint8_t* const impRing = sm + L.imp;
+            const bool exporter = rowOn && r == lastActive && hasNext;
+            unsigned long long* xo =
+                exporter ? J.xbuf + pair_xbase(s, b, W, H, J.nb[0], J.nb[1]) * NL + tl * KW : nullptr;
+            const unsigned long long ep = (unsigned long long)a.epoch << 32;
+
+            auto prefetch = [&](int step) {
+                const int p = step + kPPF - 1;
+                if (rowOn && p >= 0 && p < Ws) {
+                    const uint8_t* src = J.cost + (pix0 + (ptrdiff_t)p * du) * DP + off;
+                    const uint32_t dst = w_smem_addr(costRing + (p % kPPF) * DP + off);
+                    if constexpr ((2 * KW) % 16 == 0) {
 #pragma unroll
-            for (int w = 0; w < KW; ++w) pred[w] = imp[w];
-            const uint32_t predMin = impMin;
-            if (warpImports && u + 1 < Ws) {
-                ok = ok && p_wait_gpu(prodIn, stallNeed ? stallNeed : (unsigned)(u + 1), seen, sflag + 1,
-                                      a.status, a.spinMax);
-                if (ok && r == 0) {
-                    const uint8_t* src = xin + (size_t)u * SB;
-                    load_words<KW>(reinterpret_cast<const uint16_t*>(src) + off, imp);
-                    impMin = *reinterpret_cast<const uint32_t*>(src + 2 * DP);
+                        for (int q = 0; q < (2 * KW) / 16; ++q) w_cp_async16(dst + 16 * q, src + 16 * q);
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < KW / 2; ++q)
+                            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst + 4 * q),
+                                         "l"(src + 4 * q)
+                                         : "memory");
+                    }
                 }
-            }
-            // ---- cost of this step's pixel ----
-            prefetch(u);
-            w_cp_wait<kPPF - 1>();
-            uint32_t Cw[KW];
-            load_cost_words<KW>(costRing + (u % kPPF) * DP + off, Cw);
-            if (WRAP || J.costScale != 1) {
+                w_cp_commit();
+            };
+            for (int st = -(kPPF - 1); st < 0; ++st) prefetch(st);
+
+            uint32_t LH[KW];
 #pragma unroll
-                for (int w = 0; w < KW; ++w) Cw[w] = scale_cost<WRAP>(Cw[w], J.costScale);
-            }
-            // ---- adaptive P2: horizontal predecessor (u-1, v), diagonal (u-1, v-1) ----
-            const int um = max(u - 1, 0);
-            const int cur = irow[u];
-            const uint32_t p2h = p2lut[abs(cur - irow[um])];
-            const uint32_t p2d = p2lut[abs(cur - iprev[um])];
-            // ---- horizontal path (its state starts at 0: L = C at u = 0) ----
-            uint32_t LnH[KW];
-            wave_step<KW, T, WRAP, FULL>(LH, Cw, minH, p2h, J.p1x2, J.bsub, mk, LnH);
-            // ---- diagonal path from the row above, pixel u-1 ----
-            uint32_t Lp[KW], mp;
-            if (u == 0 || v == 0) {
-                load_words<KW>(reinterpret_cast<const uint16_t*>(zeroSlot) + off, Lp);
-                mp = 0u;
-            } else if (r == 0) {
+            for (int w = 0; w < KW; ++w) LH[w] = 0;
+            uint32_t minH = 0;
+            unsigned impSeen = 0;
+            for (int u = 0; u < Ws; ++u) {
+                // ---- the band above's pixel u-1 must be in the import ring (warp 0 holds row 0) ----
+                if (warp == 0 && hasPrev && u >= 1 && ok)
+                    ok = w_wait_cta(&sctr[0], (unsigned)u, impSeen, sflag + 1, a.status, a.spinMax);
+                // ---- cost of this step's pixel ----
+                prefetch(u);
+                w_cp_wait<kPPF - 1>();
+                uint32_t Cw[KW];
+                load_cost_words<KW>(costRing + (u % kPPF) * DP + off, Cw);
+                if (WRAP || J.costScale != 1) {
 #pragma unroll
-                for (int w = 0; w < KW; ++w) Lp[w] = pred[w];
-                mp = predMin;
-            } else {
-                const uint8_t* slot = upSlots + ((u - 1) & 1) * SB;
+                    for (int w = 0; w < KW; ++w) Cw[w] = scale_cost<WRAP>(Cw[w], J.costScale);
+                }
+                // ---- adaptive P2: horizontal predecessor (u-1, v), diagonal (u-1, v-1) ----
+                const int um = max(u - 1, 0);
+                const int cur = irow[u];
+                const uint32_t p2h = p2lut[abs(cur - irow[um])];
+                const uint32_t p2d = p2lut[abs(cur - iprev[um])];
+                // ---- horizontal path (its state starts at 0: L = C at u = 0) ----
+                uint32_t LnH[KW];
+                wave_step<KW, T, WRAP, FULL>(LH, Cw, minH, p2h, J.p1x2, J.bsub, mk, LnH);
+                // ---- diagonal path from the row above, pixel u-1 ----
+                const uint8_t* slot = (u == 0 || v == 0) ? zeroSlot
+                                      : r == 0           ? impRing + ((u - 1) & (kPQ - 1)) * SB
+                                                         : upSlots + ((u - 1) & 1) * SB;
+                uint32_t Lp[KW];
                 load_words<KW>(reinterpret_cast<const uint16_t*>(slot) + off, Lp);
-                mp = *reinterpret_cast<const uint32_t*>(slot + 2 * DP);
-            }
-            uint32_t LnD[KW];
-            wave_step<KW, T, WRAP, FULL>(Lp, Cw, mp, p2d, J.p1x2, J.bsub, mk, LnD);
-            minH = wave_min_t<KW, T>(LnH);
-            const uint32_t minD = wave_min_t<KW, T>(LnD);
-            uint32_t S[KW];
+                const uint32_t mp = *reinterpret_cast<const uint32_t*>(slot + 2 * DP);
+                uint32_t LnD[KW];
+                wave_step<KW, T, WRAP, FULL>(Lp, Cw, mp, p2d, J.p1x2, J.bsub, mk, LnD);
+                minH = wave_min_t<KW, T>(LnH);
+                const uint32_t minD = wave_min_t<KW, T>(LnD);
+                uint32_t S[KW];
 #pragma unroll
-            for (int w = 0; w < KW; ++w) {
-                LH[w] = LnH[w];
-                S[w] = WRAP ? __vadd2(LnH[w], LnD[w]) : LnH[w] + LnD[w];
-            }
-            // ---- hand the diagonal vector to the row below / the band below ----
-            {
-                uint8_t* slot = mySlots + (u & 1) * SB;
-                store_words<KW>(reinterpret_cast<uint16_t*>(slot) + off, LnD);
-                if (tl == 0) *reinterpret_cast<uint32_t*>(slot + 2 * DP) = minD;
-            }
-            if (rowOn) {
-                store_words<KW>(pout, S);
-                pout += pstep;
-                if (exporter) {
-                    uint8_t* dst = xout + (size_t)u * SB;
-                    store_words<KW>(reinterpret_cast<uint16_t*>(dst) + off, LnD);
-                    if (tl == 0) *reinterpret_cast<uint32_t*>(dst + 2 * DP) = minD;
+                for (int w = 0; w < KW; ++w) {
+                    LH[w] = LnH[w];
+                    S[w] = WRAP ? __vadd2(LnH[w], LnD[w]) : LnH[w] + LnD[w];
                 }
+                // ---- hand the diagonal vector to the row below / the band below ----
+                {
+                    uint8_t* my = mySlots + (u & 1) * SB;
+                    store_words<KW>(reinterpret_cast<uint16_t*>(my) + off, LnD);
+                    if (tl == 0) *reinterpret_cast<uint32_t*>(my + 2 * DP) = minD;
+                }
+                if (rowOn) {
+                    store_words<KW>(pout, S);
+                    pout += pstep;
+                    if (exporter) {
+#pragma unroll
+                        for (int w = 0; w < KW; w += 2) ll_store2(xo + w, ep | LnD[w], ep | LnD[w + 1]);
+                        if (tl == 0) ll_store2(xo + DP / 2, ep | minD, ep);   // the minimum and the pad word
+                        xo += NL;
+                    }
+                }
+                // every row has finished step u (row 0 is done with pixel u-1 of the
+                // import ring); all rows stop together when any of them must
+                if (rows_barrier_or(RW * 32, !ok || sflag[1] != 0)) {
+                    ok = false;
+                    break;
+                }
+                if (threadIdx.x == 0 && hasPrev) w_st_release_cta(&sctr[1], (unsigned)u);
             }
-            if (warpExports && ((u % kPE) == kPE - 1 || u == Ws - 1)) {
-                __syncwarp();
-                if (exporter && tl == 0) w_st_release_gpu(prodOut, (unsigned)(u + 1));
+            w_cp_wait<0>();
+        } else if (hasPrev) {
+            // ===================== import warp: the band above's last row =====================
+            const unsigned long long* xin = J.xbuf + pair_xbase(s, b - 1, W, H, J.nb[0], J.nb[1]) * NL;
+            const unsigned want = (a.stallTest && t == 4) ? a.epoch + 1u : a.epoch;
+            const int nImp = Ws - 1;     // row 0 uses pixels 0 .. Ws-2
+            constexpr int PER = (kPG * PAIRS + 31) / 32;
+            unsigned freeSeen = 0;
+            long long spins = 0;
+            int p0 = 0;
+            while (p0 < nImp && ok) {
+                const int g = min(kPG, nImp - p0);
+                // ring space: pixel p replaces pixel p - kPQ, which row 0 must have consumed
+                if (p0 + g > kPQ)
+                    ok = w_wait_cta(&sctr[1], (unsigned)(p0 + g - kPQ), freeSeen, sflag + 1, a.status, a.spinMax);
+                if (!ok) break;
+                unsigned long long va[PER], vb[PER];
+                unsigned bad = 0;   // pixels (bit g') with a word not yet written by this launch
+#pragma unroll
+                for (int j = 0; j < PER; ++j) {
+                    const int f = lane + 32 * j;
+                    const int px = f / PAIRS, q = f - px * PAIRS;
+                    va[j] = vb[j] = 0;
+                    if (px < g) {
+                        ll_load2(xin + (size_t)(p0 + px) * NL + 2 * q, va[j], vb[j]);
+                        if ((unsigned)(va[j] >> 32) != want || (unsigned)(vb[j] >> 32) != want) bad |= 1u << px;
+                    }
+                }
+                bad = __reduce_or_sync(kFullMask, bad);
+                const int n = bad ? __ffs(bad) - 1 : g;   // the leading pixels that are complete
+                if (n > 0) {
+#pragma unroll
+                    for (int j = 0; j < PER; ++j) {
+                        const int f = lane + 32 * j;
+                        const int px = f / PAIRS, q = f - px * PAIRS;
+                        if (px < n) {
+                            uint8_t* dst = sm + L.imp + ((p0 + px) & (kPQ - 1)) * SB + 8 * q;
+                            *reinterpret_cast<uint2*>(dst) = make_uint2((uint32_t)va[j], (uint32_t)vb[j]);
+                        }
+                    }
+                    __syncwarp();
+                    if (lane == 0) w_st_release_cta(&sctr[0], (unsigned)(p0 + n));
+                    p0 += n;
+                    spins = 0;
+                    continue;
+                }
+                // nothing new: bounded wait for the band above
+                if (sflag[1]) {
+                    ok = false;
+                    break;
+                }
+                if ((spins & 63) == 63 && *(volatile int*)a.status != 0) {
+                    sflag[1] = 1;
+                    ok = false;
+                    break;
+                }
+                if (++spins >= a.spinMax) {
+                    if (lane == 0) atomicExch(a.status, (int)LUMEN_ERR_TIMEOUT);
+                    sflag[1] = 1;
+                    ok = false;
+                    break;
+                }
+                __nanosleep(32);
             }
-            w_rows_barrier(RW * 32);
-            if (sflag[1]) break;
         }
-        w_cp_wait<0>();
-        __syncthreads();
+        if (__syncthreads_or(!ok || sflag[1] != 0)) break;
     }
 }
 
@@ -296,19 +356,19 @@ pair_kernel(PairArgs a) {
 
 namespace lumen {
 
-// Launch of one instance (the host picks KW and T from the padded disparity count).
-template <int KW, int T>
+// Launch of one instance (the host picks KW, T and R from the padded
+// disparity count and the shared memory).  grid == 0: occupancy query only.
+template <int KW, int T, int R>
 cudaError_t pair_launch_t(const PairArgs& a, bool wrap, bool full, int smem, int grid, cudaStream_t s,
                           int* perSM) {
-    constexpr int R = 16;
-    constexpr int threads = R / (32 / T) * 32;
+    constexpr int threads = (R / (32 / T) + 1) * 32;
     void (*k)(PairArgs) = wrap ? (full ? pair_kernel<KW, true, true, R, T> : pair_kernel<KW, true, false, R, T>)
                                : (full ? pair_kernel<KW, false, true, R, T> : pair_kernel<KW, false, false, R, T>);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, k, threads, smem);
     if (e != cudaSuccess) return e;
-    if (grid <= 0) return cudaSuccess;   // occupancy query only
+    if (grid <= 0) return cudaSuccess;
     k<<<grid, threads, smem, s>>>(a);
     return cudaGetLastError();
 }

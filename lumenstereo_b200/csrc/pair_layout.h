@@ -1,7 +1,7 @@
 // pair_layout.h -- the index arithmetic of schedule 6 (pair_kernel.cuh) that
 // host and device share: sweep geometry, ticket order, band-boundary row
-// buffers, progress counters and the shared-memory carve-up.  Plain C++ so
-// host tests compile it without nvcc (tests/cpp/pair_layout_test.cpp).
+// buffers and the shared-memory carve-up.  Plain C++ so host tests compile it
+// without nvcc (tests/cpp/pair_layout_test.cpp).
 #pragma once
 #include <cstddef>
 
@@ -14,12 +14,22 @@
 namespace lumen {
 
 constexpr int kPPF = 8;    // per-row cost ring (pixels); kPPF-1 prefetched ahead
-constexpr int kPE = 4;     // a band's last row publishes its progress every kPE pixels
+constexpr int kPQ = 32;    // import ring: pixels of the band above held for row 0
+constexpr int kPG = 8;     // pixels the import warp polls and copies at a time
 
+// Shared-memory slot of one pixel's diagonal vector: Dp uint16 values, the
+// vector's minimum (uint32) and padding to 16 bytes.
 LUMEN_PAIR_HD constexpr int pair_slot_bytes(int Dp) { return 2 * Dp + 16; }
 
+// Band-boundary row buffers hold, per pixel, the slot's Dp / 2 + 1 payload
+// words as 64-bit (payload, epoch) words -- the epoch of the launch that wrote
+// them in the high half -- padded to an even count so every pixel starts on a
+// 16-byte boundary.  A reader takes a word once its epoch is the current one:
+// no fence or progress counter is needed between the bands.
+LUMEN_PAIR_HD constexpr int pair_ll_words(int Dp) { return Dp / 2 + 2; }
+
 struct PairSmem {
-    int img, cost, slots, zero, lut, misc, total, Lp;
+    int img, cost, slots, imp, zero, lut, misc, total, Lp;
 };
 LUMEN_PAIR_HD PairSmem pair_smem(int Lmax, int Dp, int R) {
     PairSmem s;
@@ -33,6 +43,8 @@ LUMEN_PAIR_HD PairSmem pair_smem(int Lmax, int Dp, int R) {
     o += R * kPPF * Dp;
     s.slots = o;
     o += R * 2 * SB;
+    s.imp = o;
+    o += kPQ * SB;
     s.zero = o;   // all-zero slot: a path that starts reads it (L' = 0, min L' = 0 gives L = C)
     o += SB;
     s.lut = o;
@@ -66,16 +78,14 @@ LUMEN_PAIR_HD void pair_ticket(int t, int nb0, int nb1, int& s, int& b) {
     b = m + (t2 >> 1);
 }
 
-// first pixel (in slots) of the row buffer of sweep s, boundary b (the last row of band b)
+// first pixel (in row-buffer slots) of the row buffer of sweep s, boundary b
+// (the last row of band b)
 LUMEN_PAIR_HD size_t pair_xbase(int s, int b, int W, int H, int nb0, int nb1) {
     const size_t rows = (size_t)nb0 * W;
     if (s == 0) return (size_t)b * W;
     if (s == 1) return rows + (size_t)b * W;
     if (s == 2) return 2 * rows + (size_t)b * H;
     return 2 * rows + (size_t)nb1 * H + (size_t)b * H;
-}
-LUMEN_PAIR_HD int pair_poff(int s, int nb0, int nb1) {
-    return s < 2 ? s * nb0 : 2 * nb0 + (s - 2) * nb1;
 }
 
 }  // namespace lumen

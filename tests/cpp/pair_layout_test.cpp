@@ -5,9 +5,10 @@
 //  * each sweep visits every pixel once, and the predecessor of its
 //    horizontal and diagonal path is the reference path's previous pixel
 //    (LR/TLBR, RL/BRTL, TB/TRBL, BT/BLTR);
-//  * band-boundary row buffers and progress counters never overlap and stay
-//    inside the sizes the host allocates;
-//  * the shared-memory carve-up keeps the cp.async and vector alignments.
+//  * band-boundary row buffers never overlap and stay inside the size the
+//    host allocates;
+//  * the shared-memory carve-up and the row-buffer words keep the cp.async
+//    and vector alignments.
 // Prints "ok" and exits 0 on success.
 #include <cstdio>
 #include <random>
@@ -54,8 +55,6 @@ int main() {
                 CHECK(x0 == prev);       // consecutive, disjoint
                 prev = x0 + (size_t)Ws;
                 CHECK(prev <= total);
-                CHECK(pair_poff(s, nb0, nb1) + b == (s < 2 ? s * nb0 : 2 * nb0 + (s - 2) * nb1) + b);
-                CHECK(pair_poff(s, nb0, nb1) + b < nT);   // the ticket counter sits at nT
             }
         }
         CHECK(prev == total);
@@ -92,16 +91,26 @@ int main() {
             CHECK((int)seen.size() == W * H);
         }
     }
-    // shared memory: alignments of the cost ring (cp.async 16 B), slots and zero slot
-    for (int Dp : {64, 128, 192, 256, 320})
-        for (int L = 1; L < 8000; L += 37) {
-            const PairSmem m = pair_smem(L, Dp, R);
-            CHECK(m.Lp >= L && m.Lp % 16 == 0);
-            CHECK(m.cost % 128 == 0 && m.cost >= (R + 1) * L);
-            CHECK(m.slots % 16 == 0 && m.zero % 16 == 0 && m.lut % 4 == 0 && m.misc % 4 == 0);
-            CHECK(pair_slot_bytes(Dp) % 16 == 0);
-            CHECK(m.total == m.misc + 128);
-        }
+    // shared memory: alignments of the cost ring (cp.async 16 B), slots, import
+    // ring and zero slot; row-buffer words: every pixel starts on 16 bytes and
+    // the import warp's 8-byte pairs land inside a slot
+    for (int Dp : {64, 128, 192, 256, 320}) {
+        CHECK(pair_ll_words(Dp) % 2 == 0 && pair_ll_words(Dp) >= Dp / 2 + 1);
+        CHECK(8 * (pair_ll_words(Dp) / 2) <= pair_slot_bytes(Dp));   // 8-byte pairs of payload into a slot
+        CHECK(4 * (Dp / 2) == 2 * Dp);                               // the minimum's word sits at byte 2 Dp
+        for (int RR : {16, 32})
+            for (int L = 1; L < 8000; L += 37) {
+                const PairSmem m = pair_smem(L, Dp, RR);
+                CHECK(m.Lp >= L && m.Lp % 16 == 0);
+                CHECK(m.cost % 128 == 0 && m.cost >= (RR + 1) * L);
+                CHECK(m.slots % 16 == 0 && m.imp % 16 == 0 && m.zero % 16 == 0 && m.lut % 4 == 0 &&
+                      m.misc % 4 == 0);
+                CHECK(m.imp - m.slots == RR * 2 * pair_slot_bytes(Dp));
+                CHECK(m.zero - m.imp == kPQ * pair_slot_bytes(Dp));
+                CHECK(pair_slot_bytes(Dp) % 16 == 0);
+                CHECK(m.total == m.misc + 128);
+            }
+    }
     std::printf("ok\n");
     return 0;
 }
