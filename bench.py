@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--lanes", type=int, default=32,
                     help="lanes per row with --schedule 4 --rows (8/16: lane teams)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve", "epilogue"],
+    ap.add_argument("--mode", default="plain", choices=["plain", "batch", "serve", "epilogue", "ops"],
                     help="plain: one pair per call (default); batch: the 64-pair mixed stream; "
                          "serve: Poisson request stream through the served form")
     ap.add_argument("--pairs", type=int, default=0,
@@ -733,6 +733,24 @@ def run_epilogue(args):
         print(json.dumps(res), flush=True)
 
 
+def run_ops(args):
+    """Issue rate of the packed minima the recurrence can use (the library's
+    lumen_debug_op_rates): ns per warp-instruction per SM, and the ratio to
+    the two-input __vminu2."""
+    import ctypes as C
+    import torch
+    from lumenstereo_b200 import _check, _lib
+    torch.cuda.set_device(0)
+    out = (C.c_float * 4)()
+    _check(_lib.lib().lumen_debug_op_rates(out))
+    names = ["vminu2", "vimin3_u16x2", "viaddmin_u16x2", "iadd"]
+    res = {"metric": "ns per warp-instruction per SM", "unit": "ns", "higher_is_better": False,
+           "n_gpus": 1, "data": "synthetic", "dtype": "u16x2",
+           "ops": {n: float(v) for n, v in zip(names, out)},
+           "relative_to_vminu2": {n: float(v) / float(out[0]) for n, v in zip(names, out)}}
+    print(json.dumps(res), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -743,6 +761,8 @@ def main():
         run_serve(args)
     elif args.mode == "epilogue":
         run_epilogue(args)
+    elif args.mode == "ops":
+        run_ops(args)
     else:
         run_ours(args)
 

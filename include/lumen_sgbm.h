@@ -161,6 +161,11 @@ lumen_status lumen_sgbm_debug_trace_copy(lumen_sgbm* h, unsigned long long* dst,
 unsigned long long lumen_sgbm_debug_launch_count(const lumen_sgbm* h);
 /* Iteration limit of every device-side wait (0 restores the default, 2^22). */
 lumen_status lumen_sgbm_debug_set_wait_limit(lumen_sgbm* h, long long spins);
+/* Issue-rate probe (no counterpart in the reference): device ns per
+ * warp-instruction per SM of __vminu2, __vimin3_u16x2, __viaddmin_u16x2 and a
+ * 32-bit add, each timed with CUDA events over independent chains on every
+ * SM (out[0..3]).  Informs how the recurrence's minima are written. */
+lumen_status lumen_debug_op_rates(float out[4]);
 /* Failure-path self test of schedules 4 and 6: while enabled, one wait of a band
  * that imports from the band above can never be satisfied, so it runs out
  * after the wait limit and the compute returns LUMEN_ERR_TIMEOUT (no fault, no
@@ -312,6 +317,10 @@ typedef struct lumen_server_options {
     int max_inflight;           /* batch slots on the device at once, 1..8; default 2 */
     int watchdog_ms;            /* host deadline of a batch, 0 = none; default 60000 */
     long long spin_limit;       /* device-side wait limit, 0 = default (2^24) */
+    int plain_fallback;         /* 1 (default): the requests of a batch whose launch fails or
+                                   whose device-side waits run out are computed again one by one
+                                   through the plain call (lumen_sgbm_compute_device with the
+                                   default wait limit); 0: they complete with the batch's error */
 } lumen_server_options;
 typedef struct lumen_request_info {
     lumen_status status;
@@ -325,6 +334,7 @@ typedef struct lumen_server_stats {
     unsigned long long submitted, completed, rejected, failed, batches, watchdog_expired;
     size_t budget_bytes, admitted_bytes, peak_admitted_bytes;
     int queue_depth, peak_queue_depth, inflight_batches, peak_batch_pairs;
+    unsigned long long fallbacks; /* requests served by the plain-call fallback */
 } lumen_server_stats;
 void lumen_server_options_default(lumen_server_options* o);
 lumen_status lumen_server_create(const lumen_server_options* o, lumen_server** out);
@@ -358,6 +368,9 @@ lumen_status lumen_server_submit(lumen_server* s, const lumen_stereo_params* par
 lumen_status lumen_server_wait(lumen_server* s, unsigned long long request_id, int timeout_ms,
                                lumen_request_info* info);
 lumen_status lumen_server_get_stats(lumen_server* s, lumen_server_stats* out);
+/* Failure injection on the host (tests): the next `n` batch launches fail
+ * before any device work, as a launch that cannot be enqueued would. */
+lumen_status lumen_server_debug_fail_batches(lumen_server* s, int n);
 
 /* ---- Census cost volume without device allocation.  No counterpart in the
  * reference: it serves callers that cannot call cudaMalloc (a real-time loop

@@ -383,7 +383,8 @@ class StereoServer:
     """
 
     def __init__(self, budget_bytes: int = 40 << 30, max_batch_pairs: int = 32, rows_per_band: int = 8,
-                 max_inflight: int = 2, watchdog_ms: int = 60000, spin_limit: int = 0):
+                 max_inflight: int = 2, watchdog_ms: int = 60000, spin_limit: int = 0,
+                 plain_fallback: bool = True):
         o = _lib.CServerOptions()
         _lib.lib().lumen_server_options_default(C.byref(o))
         o.device_budget_bytes = budget_bytes
@@ -392,6 +393,7 @@ class StereoServer:
         o.max_inflight = max_inflight
         o.watchdog_ms = watchdog_ms
         o.spin_limit = spin_limit
+        o.plain_fallback = 1 if plain_fallback else 0
         self._h = C.c_void_p()
         self._outs = {}
         _check(_lib.lib().lumen_server_create(C.byref(o), C.byref(self._h)))
@@ -447,6 +449,11 @@ class StereoServer:
         out = self._outs.pop(request_id)
         return out, {"latency_ms": info.latency_ms, "queue_ms": info.queue_ms, "device_ms": info.device_ms,
                      "batch_pairs": info.batch_pairs, "batch_id": info.batch_id}
+
+    def debug_fail_batches(self, n: int) -> None:
+        """Failure injection (tests): the next ``n`` batch launches fail on
+        the host before any device work."""
+        _check(_lib.lib().lumen_server_debug_fail_batches(self._h, n))
 
     def stats(self) -> dict:
         s = _lib.CServerStats()

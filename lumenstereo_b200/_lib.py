@@ -37,7 +37,7 @@ class CParams(C.Structure):
 class CServerOptions(C.Structure):
     _fields_ = [("device_budget_bytes", C.c_size_t), ("max_batch_pairs", C.c_int),
                 ("rows_per_band", C.c_int), ("max_inflight", C.c_int), ("watchdog_ms", C.c_int),
-                ("spin_limit", C.c_longlong)]
+                ("spin_limit", C.c_longlong), ("plain_fallback", C.c_int)]
 
 
 class CRequestInfo(C.Structure):
@@ -50,7 +50,8 @@ class CServerStats(C.Structure):
                                               "watchdog_expired")] + \
                [(n, C.c_size_t) for n in ("budget_bytes", "admitted_bytes", "peak_admitted_bytes")] + \
                [(n, C.c_int) for n in ("queue_depth", "peak_queue_depth", "inflight_batches",
-                                       "peak_batch_pairs")]
+                                       "peak_batch_pairs")] + \
+               [("fallbacks", C.c_ulonglong)]
 
 
 def _declare(lib):
@@ -105,6 +106,8 @@ def _declare(lib):
         "lumen_server_submit": (i, [vp, C.POINTER(CParams), i, vp, vp, i, i, vp, C.POINTER(C.c_ulonglong)]),
         "lumen_server_wait": (i, [vp, C.c_ulonglong, i, C.POINTER(CRequestInfo)]),
         "lumen_server_get_stats": (i, [vp, C.POINTER(CServerStats)]),
+        "lumen_server_debug_fail_batches": (i, [vp, i]),
+        "lumen_debug_op_rates": (i, [C.POINTER(C.c_float)]),
         "lumen_disparity_to_depth_device": (i, [vp, i, i, sz, C.c_float, C.c_float, C.c_float, vp, sz, vp]),
         "lumen_rectify_maps_device": (i, [vp, vp, vp, vp, i, i, vp, vp, vp]),
         "lumen_disparity_to_depth_color_device": (i, [vp, i, i, sz, C.c_float, C.c_float, C.c_float, vp, sz,

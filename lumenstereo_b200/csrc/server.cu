@@ -158,6 +158,8 @@ struct lumen_server {
     lumen_server_stats st{};
     std::thread thread;
     std::string fatal;  // a CUDA error that stopped the loop
+    lumen_sgbm* plain = nullptr;  // the plain call of the fallback (server thread only)
+    int failNext = 0;             // injected batch-launch failures still to come (S->mu)
 };
 
 namespace {
@@ -180,50 +182,100 @@ void complete(lumen_server* S, Request* r, lumen_status st, const std::string& e
     else S->st.failed++;
 }
 
+// The request's images and output inside its arena slice, its raw input
+// uploaded and rectified on stream `s` when it has a calibration: the first
+// steps of a batch launch, and of the plain-call fallback.
+struct ReqBufs {
+    uint8_t* dl;
+    uint8_t* dr;
+    int16_t* dOut;
+    size_t used;  // bytes of the slice these take (the batch core's buffers follow)
+};
+
+lumen_status stage_request(lumen_server* S, Request* r, cudaStream_t s, ReqBufs* out) {
+    uint8_t* base = S->arenaBase + r->off;
+    const size_t img = image_bytes(r->W, r->H), n = (size_t)r->W * r->H;
+    uint8_t* dl = base;
+    uint8_t* dr = base + img;
+    size_t o = 2 * img;
+    uint8_t* raw = nullptr;
+    if (r->calib >= 0) {
+        raw = base + o;
+        o += 2 * img;
+    }
+    int16_t* dOut = reinterpret_cast<int16_t*>(base + o);
+    o += align256(n * 2);
+    uint8_t* up = raw ? raw : dl;
+    if (cudaMemcpyAsync(up, r->in, n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(up + img, r->in + n, n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return sfail(LUMEN_ERR_CUDA, "server: input upload failed");
+    if (raw) {
+        lumen_server::Calib c{};
+        {
+            std::lock_guard<std::mutex> g(S->calibMu);
+            c = S->calib[r->calib];
+        }
+        if (c.maps) {
+            const size_t m = (size_t)r->W * r->H;
+            launch_remap(raw, raw + img, c.maps, c.maps + m, c.maps + 2 * m, c.maps + 3 * m, dl, dr, r->W, r->H, 1,
+                         2, s);
+            if (cudaGetLastError() != cudaSuccess) return sfail(LUMEN_ERR_CUDA, "server: remap launch failed");
+        } else {
+            lumen_status rs = lumen_rectifier_rectify_device(c.rect, raw, raw + img, 1, dl, dr, s);
+            if (rs != LUMEN_OK) return rs;
+        }
+    }
+    *out = ReqBufs{dl, dr, dOut, o};
+    return LUMEN_OK;
+}
+
+// The plain-call fallback for one request of a failed batch (server thread,
+// the request's arena slice still reserved, nothing of the batch still
+// running on the device): staged again from the pinned input, computed by
+// lumen_sgbm_compute_device with the default wait limit, copied to the
+// caller's buffer.  Blocks the server loop while it runs.
+lumen_status plain_fallback(lumen_server* S, Request* r, cudaStream_t s) {
+    lumen_status st = LUMEN_OK;
+    if (!S->plain) st = lumen_sgbm_create(&r->p, &S->plain);
+    else st = lumen_sgbm_set_params(S->plain, &r->p);
+    if (st != LUMEN_OK) return st;
+    ReqBufs q{};
+    st = stage_request(S, r, s, &q);
+    if (st != LUMEN_OK) return st;
+    st = lumen_sgbm_compute_device(S->plain, q.dl, q.dr, r->W, r->H, (size_t)r->W, 1, q.dOut,
+                                   (size_t)r->W * 2, s);
+    if (st != LUMEN_OK) return st;
+    const size_t n = (size_t)r->W * r->H;
+    if (cudaMemcpyAsync(r->out, q.dOut, n * 2, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return sfail(LUMEN_ERR_CUDA, "server: plain-call fallback failed");
+    std::memcpy(r->user, r->out, n * 2);
+    return LUMEN_OK;
+}
+
 lumen_status slot_launch(lumen_server* S, Slot& sl, std::vector<Request*>& adm) {
     const int R = S->opt.rows_per_band;
+    {
+        std::lock_guard<std::mutex> g(S->mu);
+        if (S->failNext > 0) {
+            --S->failNext;
+            return sfail(LUMEN_ERR_CUDA, "server: batch launch failed (injected)");
+        }
+    }
     sl.tLaunch = Clock::now();  // the watchdog counts from the start of the enqueue
     sl.reqs = adm;
     sl.pairs.clear();
     sl.groups.clear();
     sl.batchId = S->nextBatch++;
     for (Request* r : adm) {
-        uint8_t* base = S->arenaBase + r->off;
-        const size_t img = image_bytes(r->W, r->H), n = (size_t)r->W * r->H;
-        uint8_t* dl = base;
-        uint8_t* dr = base + img;
-        size_t o = 2 * img;
-        uint8_t* raw = nullptr;
-        if (r->calib >= 0) {
-            raw = base + o;
-            o += 2 * img;
-        }
-        int16_t* dOut = reinterpret_cast<int16_t*>(base + o);
-        o += align256(n * 2);
-        uint8_t* up = raw ? raw : dl;
-        if (cudaMemcpyAsync(up, r->in, n, cudaMemcpyHostToDevice, sl.s) != cudaSuccess ||
-            cudaMemcpyAsync(up + img, r->in + n, n, cudaMemcpyHostToDevice, sl.s) != cudaSuccess)
-            return sfail(LUMEN_ERR_CUDA, "server: input upload failed");
-        if (raw) {
-            lumen_server::Calib c{};
-            {
-                std::lock_guard<std::mutex> g(S->calibMu);
-                c = S->calib[r->calib];
-            }
-            if (c.maps) {
-                const size_t m = (size_t)r->W * r->H;
-                launch_remap(raw, raw + img, c.maps, c.maps + m, c.maps + 2 * m, c.maps + 3 * m, dl, dr, r->W,
-                             r->H, 1, 2, sl.s);
-                if (cudaGetLastError() != cudaSuccess) return sfail(LUMEN_ERR_CUDA, "server: remap launch failed");
-            } else {
-                lumen_status rs = lumen_rectifier_rectify_device(c.rect, raw, raw + img, 1, dl, dr, sl.s);
-                if (rs != LUMEN_OK) return rs;
-            }
-        }
+        ReqBufs b{};
+        lumen_status rs = stage_request(S, r, sl.s, &b);
+        if (rs != LUMEN_OK) return rs;
         BatchPair q;
-        lumen_status ps = batch_pair_init(q, &r->p, dl, dr, r->W, r->H, dOut);
+        lumen_status ps = batch_pair_init(q, &r->p, b.dl, b.dr, r->W, r->H, b.dOut);
         if (ps != LUMEN_OK) return ps;
-        q.base = base;
+        q.base = S->arenaBase + r->off;
+        size_t o = b.used;
         batch_pair_layout(q, R, o);
         sl.pairs.push_back(q);
     }
@@ -279,13 +331,23 @@ lumen_status slot_launch(lumen_server* S, Slot& sl, std::vector<Request*>& adm) 
     return LUMEN_OK;
 }
 
-// Returns the requests' memory and finishes the ones the watchdog has not.
+// Returns the requests' memory and finishes the ones the watchdog has not;
+// when the batch's device-side waits ran out, those go through the plain-call
+// fallback first (if enabled).
 void slot_retire(lumen_server* S, Slot& sl) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, sl.evStart, sl.evDone);
     const int dev = *sl.hStatus;
+    std::vector<lumen_status> fb(sl.reqs.size(), LUMEN_OK);
+    if (dev != 0 && S->opt.plain_fallback) {
+        // only the server thread completes requests, so `done` is stable here
+        for (size_t i = 0; i < sl.reqs.size(); ++i)
+            if (!sl.reqs[i]->done) fb[i] = plain_fallback(S, sl.reqs[i], sl.s);
+    }
     std::lock_guard<std::mutex> g(S->mu);
+    size_t idx = 0;
     for (Request* r : sl.reqs) {
+        const lumen_status f = fb[idx++];
         r->inFlight = false;
         S->arena.release(r->off, r->need);
         S->st.admitted_bytes -= r->need;
@@ -294,6 +356,9 @@ void slot_retire(lumen_server* S, Slot& sl) {
             if (dev == 0) {
                 std::memcpy(r->user, r->out, (size_t)r->W * r->H * 2);
                 complete(S, r, LUMEN_OK, "");
+            } else if (S->opt.plain_fallback) {
+                if (f == LUMEN_OK) S->st.fallbacks++;
+                complete(S, r, f, f == LUMEN_OK ? "" : "the plain-call fallback of a timed-out batch failed");
             } else {
                 complete(S, r, static_cast<lumen_status>(dev), "a bounded device-side wait timed out in a served batch");
             }
@@ -405,21 +470,29 @@ void server_loop(lumen_server* S) {
         if (!adm.empty()) {
             const unsigned long long bid = S->nextBatch;
             lumen_status ls = slot_launch(S, *freeSlot, adm);
-            std::lock_guard<std::mutex> g(S->mu);
+            std::unique_lock<std::mutex> g(S->mu);
             for (Request* r : adm) {
                 r->batchPairs = (int)adm.size();
                 r->batchId = bid;
             }
             if (ls != LUMEN_OK) {
                 // nothing of this batch may still be queued on the device once
-                // its memory is reused
+                // its memory is reused (or the fallback reuses it)
                 cudaStreamSynchronize(freeSlot->s);
                 cudaStreamSynchronize(S->agg);
-                for (Request* r : adm) {
+                std::vector<lumen_status> fb(adm.size(), ls);
+                if (S->opt.plain_fallback) {
+                    g.unlock();   // the fallback runs device work: submitters keep going meanwhile
+                    for (size_t i = 0; i < adm.size(); ++i) fb[i] = plain_fallback(S, adm[i], freeSlot->s);
+                    g.lock();
+                }
+                for (size_t i = 0; i < adm.size(); ++i) {
+                    Request* r = adm[i];
                     S->arena.release(r->off, r->need);
                     S->st.admitted_bytes -= r->need;
                     r->inFlight = false;
-                    complete(S, r, ls, "server: batch launch failed");
+                    if (fb[i] == LUMEN_OK) S->st.fallbacks++;
+                    complete(S, r, fb[i], fb[i] == LUMEN_OK ? "" : "server: batch launch failed");
                 }
                 freeSlot->busy = false;
                 S->st.inflight_batches--;
@@ -440,6 +513,7 @@ extern "C" void lumen_server_options_default(lumen_server_options* o) {
     o->max_inflight = 2;
     o->watchdog_ms = 60000;
     o->spin_limit = 0;
+    o->plain_fallback = 1;
 }
 
 extern "C" lumen_status lumen_server_create(const lumen_server_options* opt, lumen_server** out) {
@@ -529,6 +603,7 @@ extern "C" lumen_status lumen_server_destroy(lumen_server* S) {
         if (kv.second.rect) lumen_rectifier_destroy(kv.second.rect);
         if (kv.second.maps) cudaFree(kv.second.maps);
     }
+    if (S->plain) lumen_sgbm_destroy(S->plain);
     if (S->agg) cudaStreamDestroy(S->agg);
     if (S->magic) cudaFree(S->magic);
     if (S->arenaBase) cudaFree(S->arenaBase);
@@ -691,6 +766,13 @@ extern "C" lumen_status lumen_server_wait(lumen_server* S, unsigned long long id
     }
     lk.unlock();
     if (st != LUMEN_OK) return sfail(st, err);
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_server_debug_fail_batches(lumen_server* S, int n) {
+    if (!S || n < 0) return sfail(LUMEN_ERR_INVALID_ARGUMENT, "lumen_server_debug_fail_batches: bad argument");
+    std::lock_guard<std::mutex> g(S->mu);
+    S->failNext = n;
     return LUMEN_OK;
 }
 

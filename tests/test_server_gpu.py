@@ -103,7 +103,8 @@ def test_device_wait_limit_and_watchdog_report_timeouts():
     left, right, _ = synth.make_pair(synth.PairSpec(640, 480, 4, 1, 60, 2.0, 41))
     # every device-side wait gives up after one poll: the batch reports
     # LUMEN_ERR_TIMEOUT through its status word, the server keeps serving
-    with StereoServer(budget_bytes=1 << 30, spin_limit=1) as srv:
+    # (the plain-call fallback off, so the timeout reaches the caller)
+    with StereoServer(budget_bytes=1 << 30, spin_limit=1, plain_fallback=False) as srv:
         ids = [srv.submit(p, left, right) for _ in range(3)]
         errs = 0
         for i in ids:
@@ -116,7 +117,7 @@ def test_device_wait_limit_and_watchdog_report_timeouts():
     # a host deadline far below a batch's run time: the requests complete with
     # TIMEOUT while the GPU work finishes in the background
     big_l, big_r, _ = synth.make_pair(synth.PairSpec(1920, 1080, 8, 1, 60, 2.0, 42))
-    with StereoServer(budget_bytes=4 << 30, watchdog_ms=1, max_batch_pairs=4) as srv:
+    with StereoServer(budget_bytes=4 << 30, watchdog_ms=1, max_batch_pairs=4, plain_fallback=False) as srv:
         ids = [srv.submit(p, big_l, big_r) for _ in range(4)]
         for i in ids:
             with pytest.raises(TimeoutException):
@@ -132,3 +133,44 @@ def test_device_wait_limit_and_watchdog_report_timeouts():
         except TimeoutException:
             out, _ = srv.wait(rid)
     assert np.array_equal(out, ref)
+
+
+def test_plain_call_fallback_on_failed_and_timed_out_batches():
+    """A batch whose launch fails on the host (injected) or whose device-side
+    waits run out: each of its requests is computed again by the plain call
+    and equals the plain result; with the fallback off the failure reaches
+    the caller; either way the server keeps serving."""
+    reqs = _requests()[:5]
+    refs = _plain(reqs)
+    with StereoServer(budget_bytes=1 << 30, max_batch_pairs=8) as srv:
+        _register(srv)
+        srv.debug_fail_batches(1)
+        ids = [srv.submit(p, l, r, calib_id=c) for p, l, r, c in reqs]
+        outs = [srv.wait(i)[0] for i in ids]
+        st = srv.stats()
+        assert st["fallbacks"] >= 1 and st["failed"] == 0
+        # the next batches run normally again
+        again = [srv.wait(srv.submit(p, l, r, calib_id=c))[0] for p, l, r, c in reqs]
+        assert srv.stats()["fallbacks"] == st["fallbacks"]
+    for k, ref in enumerate(refs):
+        assert np.array_equal(outs[k], ref), k
+        assert np.array_equal(again[k], ref), k
+    # device-side waits that give up after one poll: the plain call (default
+    # wait limit) serves every request of those batches
+    p = StereoParams(maxDisparity=128, numDirections=8, speckleWindowSize=0)
+    left, right, _ = synth.make_pair(synth.PairSpec(640, 480, 4, 1, 60, 2.0, 43))
+    with StereoSGBM(p) as s:
+        ref = s.compute(left, right)
+    with StereoServer(budget_bytes=1 << 30, spin_limit=1) as srv:
+        ids = [srv.submit(p, left, right) for _ in range(3)]
+        outs = [srv.wait(i)[0] for i in ids]
+        st = srv.stats()
+    assert all(np.array_equal(o, ref) for o in outs)
+    assert st["failed"] == 0 and st["completed"] == 3
+    # fallback off: the injected failure is the requests' error
+    with StereoServer(budget_bytes=1 << 30, plain_fallback=False) as srv:
+        srv.debug_fail_batches(1)
+        with pytest.raises(Exception):
+            srv.wait(srv.submit(p, left, right))
+        out, _ = srv.wait(srv.submit(p, left, right))
+        assert np.array_equal(out, ref)
