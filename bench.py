@@ -618,7 +618,8 @@ def run_serve(args):
             th.join()
             span = max(done_at) - t_start
             st = srv.stats()
-            sweep.append({"offered_per_s": rate, "achieved_pairs_per_s": n / span,
+            sweep.append({"offered_per_s": rate, "requests": n, "seconds": span,
+                          "achieved_pairs_per_s": n / span,
                           "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                           "p999_ms": float(np.percentile(lat, 99.9)), "mean_batch_pairs": float(np.mean(bsz)),
                           "peak_queue_depth": st["peak_queue_depth"]})
