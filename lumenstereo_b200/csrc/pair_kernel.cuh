@@ -29,10 +29,11 @@
 //    words, plain stores with no fence: a word is valid once its high half
 //    holds this launch's epoch.  The producing rows never wait on global
 //    memory;
-//  * an import warp outside the row barrier polls the band above's row
-//    buffer a few pixels ahead, copies every pixel whose words all carry the
-//    epoch into a kPQ-slot shared-memory ring and publishes the count (release
-//    at CTA scope); row 0 takes pixel u-1 from that ring at step u.  After
+//  * an import warp outside the row barrier probes one word of the band
+//    above's next pixel (backing off while nothing arrives), then loads up to
+//    kPG pixels, copies every leading pixel whose words all carry the epoch
+//    into a kPQ-slot shared-memory ring and publishes the count (release at
+//    CTA scope); row 0 takes pixel u-1 from that ring at step u.  After
 //    each step's barrier the rows publish how many pixels row 0 has consumed,
 //    which frees ring slots.  The row buffers hold whole rows, so a band
 //    waits only on the band above it, never on the one below: bands depend
@@ -196,10 +197,17 @@ pair_kernel(PairArgs a) {
                 exporter ? J.xbuf + pair_xbase(s, b, W, H, J.nb[0], J.nb[1]) * NL + tl * KW : nullptr;
             const unsigned long long ep = (unsigned long long)a.epoch << 32;
 
+            // cost of pixel p = step + kPPF - 1 of this row: `cofs` (bytes from
+            // J.cost) follows p, incremented instead of recomputed; the calls
+            // come with step = -(kPPF - 1), -(kPPF - 2), ..., i.e. p = 0, 1, ...
+            ptrdiff_t cofs = pix0 * DP + off;
+            const ptrdiff_t cstep = du * DP;
             auto prefetch = [&](int step) {
                 const int p = step + kPPF - 1;
+                const ptrdiff_t o = cofs;
+                cofs += cstep;
                 if (rowOn && p >= 0 && p < Ws) {
-                    const uint8_t* src = J.cost + (pix0 + (ptrdiff_t)p * du) * DP + off;
+                    const uint8_t* src = J.cost + o;
                     const uint32_t dst = w_smem_addr(costRing + (p % kPPF) * DP + off);
                     if constexpr ((2 * KW) % 16 == 0) {
 #pragma unroll
@@ -292,6 +300,7 @@ pair_kernel(PairArgs a) {
             constexpr int PER = (kPG * PAIRS + 31) / 32;
             unsigned freeSeen = 0;
             long long spins = 0;
+            unsigned nap = 32;   // back-off between probes (ns), doubled while nothing arrives
             int p0 = 0;
             while (p0 < nImp && ok) {
                 const int g = min(kPG, nImp - p0);
@@ -299,6 +308,31 @@ pair_kernel(PairArgs a) {
                 if (p0 + g > kPQ)
                     ok = w_wait_cta(&sctr[1], (unsigned)(p0 + g - kPQ), freeSeen, sflag + 1, a.status, a.spinMax);
                 if (!ok) break;
+                // probe: one lane reads pixel p0's minimum word; the full load and
+                // check of up to kPG pixels follows only once it carries the epoch,
+                // so a waiting import warp takes few issue slots from the rows
+                unsigned long long pa = 0, pb = 0;
+                if (lane == 0) ll_load2(xin + (size_t)p0 * NL + DP / 2, pa, pb);
+                if (!__shfl_sync(kFullMask, (unsigned)(pa >> 32) == want ? 1u : 0u, 0)) {
+                    if (sflag[1]) {
+                        ok = false;
+                        break;
+                    }
+                    if ((spins & 63) == 63 && *(volatile int*)a.status != 0) {
+                        sflag[1] = 1;
+                        ok = false;
+                        break;
+                    }
+                    if (++spins >= a.spinMax) {
+                        if (lane == 0) atomicExch(a.status, (int)LUMEN_ERR_TIMEOUT);
+                        sflag[1] = 1;
+                        ok = false;
+                        break;
+                    }
+                    __nanosleep(nap);
+                    nap = min(nap * 2u, 256u);
+                    continue;
+                }
                 unsigned long long va[PER], vb[PER];
                 unsigned bad = 0;   // pixels (bit g') with a word not yet written by this launch
 #pragma unroll
@@ -327,6 +361,7 @@ pair_kernel(PairArgs a) {
                     if (lane == 0) w_st_release_cta(&sctr[0], (unsigned)(p0 + n));
                     p0 += n;
                     spins = 0;
+                    nap = 32;
                     continue;
                 }
                 // nothing new: bounded wait for the band above
@@ -345,7 +380,7 @@ pair_kernel(PairArgs a) {
                     ok = false;
                     break;
                 }
-                __nanosleep(32);
+                __nanosleep(32);   // the probe saw the epoch: the rest of the pixel is on its way
             }
         }
         if (__syncthreads_or(!ok || sflag[1] != 0)) break;

@@ -6,8 +6,8 @@ the GPU test makes two calls in a row (the second smaller and with another
 disparity range, so the array still holds the first call's descriptors) and
 checks each against the oracle's Census cost volume and against the cost
 volume of the ordinary entry point, lumen_sgbm_compute.  Cost volumes are
-integers: the tolerance is zero.  It also checks that the calls take no
-device memory.
+integers: the tolerance is zero.  It also checks that, once the library's
+device code is loaded, the calls take no device memory.
 
 The file name makes pytest collect it after every other test file, so a run
 that stops at the first failure has run everything else before it.  The test
@@ -63,6 +63,15 @@ def test_no_alloc_matches_compute_two_calls():
     lib = _lib.lib()
     dev = torch.device("cuda", torch.cuda.current_device())
     stream = torch.cuda.current_stream(dev)
+    # A first call loads the library's device code on this device; with lazy
+    # module loading that is when the driver commits the fixed scratch array
+    # (its 16 MiB show up once in the free-memory count).  Calls after it must
+    # take no device memory at all.
+    tiny = torch.zeros((16, 16), dtype=torch.uint8, device=dev)
+    tiny_cost = torch.zeros((16, 16, 16), dtype=torch.uint8, device=dev)
+    assert lib.lumen_census_cost_noalloc(tiny.data_ptr(), tiny.data_ptr(), 16, 16, 0, 16,
+                                         tiny_cost.data_ptr(), 16, stream.cuda_stream) == _lib.OK
+    stream.synchronize()
     cases = [  # (pair spec, minDisparity, maxDisparity, cost_stride)
         (synth.PairSpec(1920, 1080, 8, 4, 100, 2.0, 11), 0, 128, 128),
         (synth.PairSpec(640, 480, 5, 4, 60, 2.0, 12), 7, 83, 80),
