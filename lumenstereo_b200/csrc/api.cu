@@ -469,9 +469,12 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
     if (sched == 6) {
         // 4 paths, no instance for this range, or short of device memory for
         // the four partial volumes and the row buffers: schedule 4
-        // rows per band: a pinned or tuned 16 / 32, else the default
+        // rows per band and lanes per row: a pinned or tuned configuration
+        // when schedule 6 has that instance, else the defaults
         const int R6 = (cfgChosen && (cfg.NW == 16 || cfg.NW == 32)) ? cfg.NW : 0;
-        bool ok6 = mask == 0xFFu && pair_plan(k, wrap, h->numSMs, &plan6, R6) == cudaSuccess;
+        const int T6 = cfgChosen ? cfg.T : 0;
+        bool ok6 = mask == 0xFFu && (pair_plan(k, wrap, h->numSMs, &plan6, R6, T6) == cudaSuccess ||
+                                     pair_plan(k, wrap, h->numSMs, &plan6, R6) == cudaSuccess);
         if (ok6)
             ok6 = h->partB.ensure(ND * 2) == cudaSuccess && h->partC.ensure(ND * 2) == cudaSuccess &&
                   h->partD.ensure(ND * 2) == cudaSuccess;
@@ -672,8 +675,15 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
             cands.push_back({4, SweepConfig{tl, 32}});
         }
         if (mask == 0xFFu) {
-            cands.push_back({6, SweepConfig{8, 16}});   // schedule 6 takes `warps` as its rows per band
-            cands.push_back({6, SweepConfig{8, 32}});
+            // schedule 6 takes `warps` as its rows per band; lanes other than
+            // its default exist for padded disparities up to 128
+            const int t6 = pair_lanes(Dp);
+            if (t6) {
+                cands.push_back({6, SweepConfig{t6, 16}});
+                cands.push_back({6, SweepConfig{t6, 32}});
+                if (Dp <= 128) cands.push_back({6, SweepConfig{16, 16}});
+                if (Dp == 128) cands.push_back({6, SweepConfig{32, 16}});
+            }
         }
     }
     const SweepConfig savedForced = h->forced;

@@ -20,13 +20,29 @@ LUMEN_PAIR_EXTERN(10, 16, 16)
 LUMEN_PAIR_EXTERN(6, 16, 32)
 LUMEN_PAIR_EXTERN(8, 16, 32)
 LUMEN_PAIR_EXTERN(10, 16, 32)
+LUMEN_PAIR_EXTERN(2, 16, 16)
+LUMEN_PAIR_EXTERN(4, 16, 16)
+LUMEN_PAIR_EXTERN(2, 32, 16)
 #undef LUMEN_PAIR_EXTERN
 
 // lanes per row for a padded disparity count (0: no instance)
 int pair_lanes(int Dp) { return Dp <= 128 ? 8 : Dp <= 320 ? 16 : 0; }
 
-static cudaError_t pair_dispatch(const PairArgs& a, int Dp, int R, bool wrap, bool full, int smem, int grid,
-                                 cudaStream_t s, int* perSM) {
+// whether an instance with T lanes per row and R rows per band exists
+static bool pair_instance(int Dp, int T, int R) {
+    if (T == pair_lanes(Dp)) return R == 16 || R == 32;
+    return R == 16 && ((T == 16 && (Dp == 64 || Dp == 128)) || (T == 32 && Dp == 128));
+}
+
+static cudaError_t pair_dispatch(const PairArgs& a, int Dp, int R, int T, bool wrap, bool full, int smem,
+                                 int grid, cudaStream_t s, int* perSM) {
+    if (T != pair_lanes(Dp)) {
+        // wider teams for the narrow ranges: fewer words per lane, more warps
+        if (R == 16 && T == 16 && Dp == 64) return pair_launch_t<2, 16, 16>(a, wrap, full, smem, grid, s, perSM);
+        if (R == 16 && T == 16 && Dp == 128) return pair_launch_t<4, 16, 16>(a, wrap, full, smem, grid, s, perSM);
+        if (R == 16 && T == 32 && Dp == 128) return pair_launch_t<2, 32, 16>(a, wrap, full, smem, grid, s, perSM);
+        return cudaErrorInvalidValue;
+    }
     if (R == 16) {
         switch (Dp) {
         case 64: return pair_launch_t<4, 8, 16>(a, wrap, full, smem, grid, s, perSM);
@@ -50,13 +66,14 @@ static cudaError_t pair_dispatch(const PairArgs& a, int Dp, int R, bool wrap, bo
     return cudaErrorInvalidValue;
 }
 
-cudaError_t pair_plan(const SgmConsts& k, bool wrap, int numSMs, PairPlan* plan, int R) {
+cudaError_t pair_plan(const SgmConsts& k, bool wrap, int numSMs, PairPlan* plan, int R, int T) {
     if (!pair_lanes(k.Dp)) return cudaErrorInvalidValue;
     if (R == 0) R = 16;
-    if (R != 16 && R != 32) return cudaErrorInvalidValue;
+    if (T == 0) T = pair_lanes(k.Dp);
+    if (!pair_instance(k.Dp, T, R)) return cudaErrorInvalidValue;
     PairPlan p{};
     p.R = R;
-    p.T = pair_lanes(k.Dp);
+    p.T = T;
     p.nb0 = (k.H + R - 1) / R;
     p.nb1 = (k.W + R - 1) / R;
     p.nTickets = 2 * p.nb0 + 2 * p.nb1;
@@ -64,7 +81,7 @@ cudaError_t pair_plan(const SgmConsts& k, bool wrap, int numSMs, PairPlan* plan,
     if (p.smem > 227 * 1024) return cudaErrorInvalidValue;
     PairArgs dummy{};
     int perSM = 0;
-    cudaError_t e = pair_dispatch(dummy, k.Dp, R, wrap, k.D == k.Dp, p.smem, 0, nullptr, &perSM);
+    cudaError_t e = pair_dispatch(dummy, k.Dp, R, T, wrap, k.D == k.Dp, p.smem, 0, nullptr, &perSM);
     if (e != cudaSuccess) return e;
     if (perSM < 1) return cudaErrorInvalidConfiguration;
     p.grid = std::min(p.nTickets, perSM * numSMs);
@@ -104,7 +121,7 @@ cudaError_t launch_aggregate_pair(const PairView& pv, uint16_t* const part[4], c
     cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned) * plan.counterWords, s);
     if (e != cudaSuccess) return e;
     int perSM = 0;
-    return pair_dispatch(a, k.Dp, plan.R, wrap, k.D == k.Dp, plan.smem, plan.grid, s, &perSM);
+    return pair_dispatch(a, k.Dp, plan.R, plan.T, wrap, k.D == k.Dp, plan.smem, plan.grid, s, &perSM);
 }
 
 }  // namespace lumen
