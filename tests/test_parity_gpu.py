@@ -207,6 +207,29 @@ def test_parity_schedule6_pair_sweeps(D, size, census, oracle_mod):
         assert np.array_equal(s.compute(left, right), disp)
 
 
+@pytest.mark.parametrize("lanes,rows", [(8, 32), (16, 16), (32, 16)])
+@pytest.mark.parametrize("D,size", [(40, (131, 53)), (64, (40, 200)), (128, (97, 150)), (100, (700, 90))])
+def test_parity_schedule6_configurations(D, size, lanes, rows, oracle_mod):
+    """Every schedule-6 configuration the autotuner can pick (32-row bands,
+    16- and 32-lane rows for padded disparities up to 128) reproduces the
+    oracle's summed volume bit for bit, both cost modes, partial last bands
+    included."""
+    w, h = size
+    left, right, _ = synth.make_pair(synth.PairSpec(w, h, 4, 1, min(D - 1, 40), 2.0, 300 + D + w))
+    for census in (0, 1):
+        pd = params_dict(maxDisparity=D, numDirections=8, speckleWindowSize=0, matchingCostMode=census)
+        ref_disp, ref = oracle_mod.sgbm(pd, left, right, intermediates=True)
+        with StereoSGBM(to_params(pd)) as s:
+            s.set_schedule(6)
+            s.set_tuning(lanes, rows)
+            s.retain_intermediates(True)
+            disp = s.compute(left, right)
+            agg = s.intermediate("agg", (h, w, D), np.uint16)
+            assert s.get_tuning() == (6, lanes, rows), s.get_tuning()
+        assert np.array_equal(agg, ref["agg"]), (census, lanes, rows)
+        assert_subpix_close(disp, ref_disp)
+
+
 def test_schedule6_matches_schedule4_full_size():
     """1920x1080 D128 SAD and Census, 8 paths: the four-partial selection of
     schedule 6 gives schedule 4's maps (no intermediates retained)."""
