@@ -297,8 +297,8 @@ extern "C" lumen_status lumen_sgbm_set_tuning(lumen_sgbm* h, int lanes, int warp
         return LUMEN_OK;
     }
     if (!(lanes == 8 || lanes == 16 || lanes == 32) ||
-        !(warps == 2 || warps == 4 || warps == 8 || warps == 16 || warps == 32))
-        return fail(LUMEN_ERR_INVALID_ARGUMENT, "lanes must be 8/16/32 and warps 2/4/8/16/32");
+        !(warps == 2 || warps == 4 || warps == 8 || warps == 16 || warps == 24 || warps == 32))
+        return fail(LUMEN_ERR_INVALID_ARGUMENT, "lanes must be 8/16/32 and warps 2/4/8/16/24/32");
     h->forced = SweepConfig{lanes, warps};
     return LUMEN_OK;
 }
@@ -471,7 +471,7 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
         // the four partial volumes and the row buffers: schedule 4
         // rows per band and lanes per row: a pinned or tuned configuration
         // when schedule 6 has that instance, else the defaults
-        const int R6 = (cfgChosen && (cfg.NW == 16 || cfg.NW == 32)) ? cfg.NW : 0;
+        const int R6 = (cfgChosen && (cfg.NW == 16 || cfg.NW == 24 || cfg.NW == 32)) ? cfg.NW : 0;
         const int T6 = cfgChosen ? cfg.T : 0;
         bool ok6 = mask == 0xFFu && (pair_plan(k, wrap, h->numSMs, &plan6, R6, T6) == cudaSuccess ||
                                      pair_plan(k, wrap, h->numSMs, &plan6, R6) == cudaSuccess);
@@ -680,6 +680,7 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
             const int t6 = pair_lanes(Dp);
             if (t6) {
                 cands.push_back({6, SweepConfig{t6, 16}});
+                cands.push_back({6, SweepConfig{t6, 24}});
                 cands.push_back({6, SweepConfig{t6, 32}});
                 if (Dp <= 128) cands.push_back({6, SweepConfig{16, 16}});
                 if (Dp == 128) cands.push_back({6, SweepConfig{32, 16}});

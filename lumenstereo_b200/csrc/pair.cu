@@ -20,6 +20,11 @@ LUMEN_PAIR_EXTERN(10, 16, 16)
 LUMEN_PAIR_EXTERN(6, 16, 32)
 LUMEN_PAIR_EXTERN(8, 16, 32)
 LUMEN_PAIR_EXTERN(10, 16, 32)
+LUMEN_PAIR_EXTERN(4, 8, 24)
+LUMEN_PAIR_EXTERN(8, 8, 24)
+LUMEN_PAIR_EXTERN(6, 16, 24)
+LUMEN_PAIR_EXTERN(8, 16, 24)
+LUMEN_PAIR_EXTERN(10, 16, 24)
 LUMEN_PAIR_EXTERN(2, 16, 16)
 LUMEN_PAIR_EXTERN(4, 16, 16)
 LUMEN_PAIR_EXTERN(2, 32, 16)
@@ -30,7 +35,7 @@ int pair_lanes(int Dp) { return Dp <= 128 ? 8 : Dp <= 320 ? 16 : 0; }
 
 // whether an instance with T lanes per row and R rows per band exists
 static bool pair_instance(int Dp, int T, int R) {
-    if (T == pair_lanes(Dp)) return R == 16 || R == 32;
+    if (T == pair_lanes(Dp)) return R == 16 || R == 24 || R == 32;
     return R == 16 && ((T == 16 && (Dp == 64 || Dp == 128)) || (T == 32 && Dp == 128));
 }
 
@@ -50,6 +55,16 @@ static cudaError_t pair_dispatch(const PairArgs& a, int Dp, int R, int T, bool w
         case 192: return pair_launch_t<6, 16, 16>(a, wrap, full, smem, grid, s, perSM);
         case 256: return pair_launch_t<8, 16, 16>(a, wrap, full, smem, grid, s, perSM);
         case 320: return pair_launch_t<10, 16, 16>(a, wrap, full, smem, grid, s, perSM);
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    if (R == 24) {
+        switch (Dp) {
+        case 64: return pair_launch_t<4, 8, 24>(a, wrap, full, smem, grid, s, perSM);
+        case 128: return pair_launch_t<8, 8, 24>(a, wrap, full, smem, grid, s, perSM);
+        case 192: return pair_launch_t<6, 16, 24>(a, wrap, full, smem, grid, s, perSM);
+        case 256: return pair_launch_t<8, 16, 24>(a, wrap, full, smem, grid, s, perSM);
+        case 320: return pair_launch_t<10, 16, 24>(a, wrap, full, smem, grid, s, perSM);
         default: return cudaErrorInvalidValue;
         }
     }

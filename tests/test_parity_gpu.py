@@ -207,11 +207,14 @@ def test_parity_schedule6_pair_sweeps(D, size, census, oracle_mod):
         assert np.array_equal(s.compute(left, right), disp)
 
 
-@pytest.mark.parametrize("lanes,rows", [(8, 32), (16, 16), (32, 16)])
-@pytest.mark.parametrize("D,size", [(40, (131, 53)), (64, (40, 200)), (128, (97, 150)), (100, (700, 90))])
+@pytest.mark.parametrize("D,size,lanes,rows",
+                         [(D, size, lanes, rows)
+                          for D, size in [(40, (131, 53)), (64, (40, 200)), (128, (97, 150)), (100, (700, 90))]
+                          for lanes, rows in [(8, 24), (8, 32), (16, 16), (32, 16)]] +
+                         [(D, size, 16, rows) for D, size in [(150, (160, 70)), (290, (330, 61))] for rows in (24, 32)])
 def test_parity_schedule6_configurations(D, size, lanes, rows, oracle_mod):
-    """Every schedule-6 configuration the autotuner can pick (32-row bands,
-    16- and 32-lane rows for padded disparities up to 128) reproduces the
+    """Every schedule-6 configuration the autotuner can pick (24- and 32-row
+    bands, 16- and 32-lane rows for padded disparities up to 128) reproduces the
     oracle's summed volume bit for bit, both cost modes, partial last bands
     included."""
     w, h = size
