@@ -386,6 +386,199 @@ sad_cost_kernel(const uint8_t* __restrict__ pl, const uint8_t* __restrict__ pr, 
     }
 }
 
+// ---------------------------------------------------------------------------
+// SAD cost for the 5x5 window (blockSize 5, the default) and 16-bit sums.
+//
+// Same sums, counts and divisions as sad_cost_kernel; a leaner schedule.  A
+// CTA owns 32 output columns x 32 output rows and all Dp disparities; thread
+// (quad q, column lane cl) owns disparities 4q..4q+3 of the columns cl,
+// cl + CLN, ... of the tile plus its 2-pixel apron.  It keeps their column
+// sums (two uint16x2 words: d0,d2 / d1,d3) in registers and slides them down
+// the rows: one __vabsdiffu4 for the entering row and one for the leaving
+// row per column and quad.  The right rows are staged reversed (disparity
+// ascending = address ascending) in four copies shifted by 0..3 bytes, so
+// every quad is one aligned 32-bit load.  Column sums go through shared
+// memory once per row; the window sums slide along x over a run of columns
+// per thread, and the interior (full window, every disparity of the quad
+// valid) divides by one constant per row.
+// ---------------------------------------------------------------------------
+constexpr int kS5X = 32;   // output columns per CTA
+constexpr int kS5Y = 32;   // output rows per CTA
+constexpr int kS5R = 2;    // window radius
+constexpr int kS5C = kS5X + 2 * kS5R;  // columns with apron
+constexpr int kS5Ring = 2 * kS5R + 2;  // staged rows
+
+__host__ __device__ constexpr int s5_quads(int KP) { return 16 * KP; }
+// column lanes per quad: the largest power of two with Q * CLN <= 256
+__host__ __device__ constexpr int s5_cln(int KP) {
+    return 256 / s5_quads(KP) >= 16 ? 16 : 256 / s5_quads(KP) >= 8 ? 8 : 256 / s5_quads(KP) >= 4 ? 4
+         : 256 / s5_quads(KP) >= 2 ? 2 : 1;
+}
+__host__ __device__ constexpr int s5_rspan(int KP) { return (kS5C + 64 * KP + 3 + 4 + 15) & ~15; }
+
+template <int KP>
+__global__ void __launch_bounds__(256)
+sad5_cost_kernel(const uint8_t* __restrict__ pl, const uint8_t* __restrict__ pr, int W, int H,
+                 int D, int minD, const uint32_t* __restrict__ magic, uint8_t* __restrict__ cost) {
+    constexpr int Dp = 64 * KP, Q = s5_quads(KP), CLN = s5_cln(KP);
+    constexpr int NCOL = (kS5C + CLN - 1) / CLN;  // columns per thread (some idle at the end)
+    constexpr int RUN = kS5X / CLN;               // output columns per thread
+    constexpr int RS = s5_rspan(KP);              // reversed right-row span (bytes, per copy)
+    static_assert(kS5X % CLN == 0, "runs tile the output columns");
+    __shared__ __align__(16) uint8_t sL[kS5Ring][kS5C + 12];
+    __shared__ __align__(16) uint8_t sR[kS5Ring][4][RS];
+    __shared__ __align__(16) uint2 cs[kS5C][Q];
+    const int x0 = blockIdx.x * kS5X, y0 = blockIdx.y * kS5Y;
+    const int yEnd = min(H, y0 + kS5Y);
+    const int q = threadIdx.x % Q, cl = threadIdx.x / Q;
+    const int d0 = 4 * q;
+    const int lx0 = x0 - kS5R;                 // image column of tile column 0
+    const int rtop = lx0 + kS5C - 1 - minD;    // right column at reversed index 0
+    const int nthreads = Q * CLN;
+
+    auto stage_row = [&](int gy) {             // row gy into ring slot gy % kS5Ring
+        const int slot = gy % kS5Ring;
+        for (int i = threadIdx.x; i < kS5C; i += nthreads) {
+            const int gx = lx0 + i;
+            sL[slot][i] = (gx >= 0 && gx < W) ? pl[(size_t)gy * W + gx] : 0;
+        }
+        for (int i = threadIdx.x; i < 4 * RS; i += nthreads) {
+            const int k = i / RS, j = i - k * RS;
+            const int gx = rtop - (j + k);
+            sR[slot][k][j] = (gx >= 0 && gx < W) ? pr[(size_t)gy * W + gx] : 0;
+        }
+    };
+    // A of one row for tile column c: (d0,d2) and (d1,d3) as uint16x2 words
+    auto absdiff = [&](int slot, int c, uint32_t mask, uint32_t& ev, uint32_t& od) {
+        const uint32_t l4 = (uint32_t)sL[slot][c] * 0x01010101u;
+        const int j0 = (kS5C - 1 - c) + d0;    // reversed index of (column c, d0)
+        const uint32_t r4 = *reinterpret_cast<const uint32_t*>(&sR[slot][j0 & 3][j0 & ~3]);
+        const uint32_t v = __vabsdiffu4(l4, r4) & mask;
+        ev = v & 0x00FF00FFu;
+        od = (v >> 8) & 0x00FF00FFu;
+    };
+
+    // column validity masks (per band: they depend on x and d only)
+    uint32_t msk[NCOL];
+#pragma unroll
+    for (int i = 0; i < NCOL; ++i) {
+        const int c = cl + i * CLN;
+        const int xg = lx0 + c;
+        uint32_t m = 0;
+        if (c < kS5C && xg >= 0 && xg < W) {
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+                if (xg - minD - (d0 + b) >= 0 && d0 + b < D) m |= 0xFFu << (8 * b);
+        }
+        msk[i] = m;
+    }
+    // initial column sums of the first output row
+    for (int gy = max(0, y0 - kS5R); gy <= min(H - 1, y0 + kS5R); ++gy) stage_row(gy);
+    __syncthreads();
+    uint32_t cev[NCOL], cod[NCOL];
+#pragma unroll
+    for (int i = 0; i < NCOL; ++i) {
+        cev[i] = 0;
+        cod[i] = 0;
+        const int c = cl + i * CLN;
+        if (c < kS5C && msk[i])
+            for (int gy = max(0, y0 - kS5R); gy <= min(H - 1, y0 + kS5R); ++gy) {
+                uint32_t e, o;
+                absdiff(gy % kS5Ring, c, msk[i], e, o);
+                cev[i] += e;
+                cod[i] += o;
+            }
+    }
+    // output geometry of this thread's run
+    const int px0 = cl * RUN;                 // first output column (tile-relative)
+    for (int y = y0; y < yEnd; ++y) {
+        if (y > y0) {
+            // slide down: add row y + r, remove row y - r - 1 (both staged)
+            const int yin = y + kS5R, yout = y - kS5R - 1;
+            const bool hasIn = yin < H, hasOut = yout >= 0;
+            const int sin = hasIn ? yin % kS5Ring : 0, sout = hasOut ? yout % kS5Ring : 0;
+#pragma unroll
+            for (int i = 0; i < NCOL; ++i) {
+                const int c = cl + i * CLN;
+                if (c < kS5C && msk[i]) {
+                    uint32_t e, o;
+                    if (hasIn) {
+                        absdiff(sin, c, msk[i], e, o);
+                        cev[i] += e;
+                        cod[i] += o;
+                    }
+                    if (hasOut) {
+                        absdiff(sout, c, msk[i], e, o);
+                        cev[i] -= e;
+                        cod[i] -= o;
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NCOL; ++i) {
+            const int c = cl + i * CLN;
+            if (c < kS5C) cs[c][q] = make_uint2(cev[i], cod[i]);
+        }
+        __syncthreads();
+        // stage the row the next step enters (its ring slot held row y - r - 1)
+        if (y + 1 < yEnd && y + 1 + kS5R < H) stage_row(y + 1 + kS5R);
+        // window sums along x, then counts and divisions
+        const int cy = min(H - 1, y + kS5R) - max(0, y - kS5R) + 1;
+        const int full = cy * (2 * kS5R + 1);
+        const uint32_t mfull = magic[full];
+        uint32_t pe = 0, po = 0;
+#pragma unroll
+        for (int k = 0; k < 2 * kS5R + 1; ++k) {
+            const uint2 v = cs[px0 + k][q];
+            pe += v.x;
+            po += v.y;
+        }
+        uint8_t* crow = cost + ((size_t)y * W) * Dp + d0;
+#pragma unroll
+        for (int t = 0; t < RUN; ++t) {
+            const int px = px0 + t;
+            const int x = x0 + px;
+            if (t > 0) {
+                const uint2 vin = cs[px + 2 * kS5R][q];
+                const uint2 vout = cs[px - 1][q];
+                pe += vin.x - vout.x;
+                po += vin.y - vout.y;
+            }
+            if (x < W) {
+                const uint32_t s0 = pe & 0xFFFFu, s2 = pe >> 16, s1 = po & 0xFFFFu, s3 = po >> 16;
+                uint32_t outw;
+                const bool interior = (x - kS5R >= 0) && (x + kS5R <= W - 1) &&
+                                      (x - kS5R - minD - d0 - 3 >= 0) && (d0 + 4 <= D);
+                if (interior) {
+                    outw = __umulhi(s0, mfull) | (__umulhi(s1, mfull) << 8) | (__umulhi(s2, mfull) << 16) |
+                           (__umulhi(s3, mfull) << 24);
+                } else {
+                    const uint32_t sv[4] = {s0, s1, s2, s3};
+                    outw = 0;
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        const int d = d0 + b;
+                        uint32_t v;
+                        if (d >= D) {
+                            v = 0;
+                        } else {
+                            const int ad = minD + d;
+                            const int clo = max(max(-kS5R, -x), ad - x);
+                            const int chi = min(kS5R, W - 1 - x);
+                            const int cnt = cy * max(0, chi - clo + 1);
+                            v = cnt > 0 ? (cnt == 1 ? sv[b] : __umulhi(sv[b], magic[cnt])) : 255u;
+                        }
+                        outw |= v << (8 * b);
+                    }
+                }
+                *reinterpret_cast<uint32_t*>(crow + (size_t)x * Dp) = outw;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // ceil(2^32 / c) for c >= 2 (c = 0, 1 unused): sum / c == umulhi(sum, m[c])
 // whenever sum * (m[c]*c - 2^32) < 2^32, which holds for every SAD window sum.
 __global__ void magic_kernel(uint32_t* m, int n) {
@@ -468,13 +661,28 @@ size_t sad_cost_smem(int Dp, int r) {
     return (size_t)((g.ring * (g.ncolp + g.rw) + 15) & ~15) + (size_t)g.ncol * (Dp / 4) * 8;
 }
 
+template <int KP>
+static cudaError_t launch_sad5(const uint8_t* pl, const uint8_t* pr, int W, int H, int D, int minD,
+                               const uint32_t* magic, uint8_t* cost, cudaStream_t s) {
+    dim3 g((W + kS5X - 1) / kS5X, (H + kS5Y - 1) / kS5Y);
+    sad5_cost_kernel<KP><<<g, s5_quads(KP) * s5_cln(KP), 0, s>>>(pl, pr, W, H, D, minD, magic, cost);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_sad_cost(const uint8_t* pl, const uint8_t* pr, int W, int H, int D, int Dp,
                             int minD, int r, const uint32_t* magic, int wide, uint8_t* cost,
                             cudaStream_t s) {
-    if (r == 2 && !wide) {
-        // the default 5x5 window (sad5.cu); Dp = 512 takes the general kernel
-        const cudaError_t e = launch_sad5w(pl, pr, W, H, D, Dp, minD, magic, cost, s);
-        if (e != cudaErrorInvalidValue) return e;
+    if (r == kS5R && !wide) {
+        switch (Dp / 64) {
+        case 1: return launch_sad5<1>(pl, pr, W, H, D, minD, magic, cost, s);
+        case 2: return launch_sad5<2>(pl, pr, W, H, D, minD, magic, cost, s);
+        case 3: return launch_sad5<3>(pl, pr, W, H, D, minD, magic, cost, s);
+        case 4: return launch_sad5<4>(pl, pr, W, H, D, minD, magic, cost, s);
+        case 5: return launch_sad5<5>(pl, pr, W, H, D, minD, magic, cost, s);
+        case 6: return launch_sad5<6>(pl, pr, W, H, D, minD, magic, cost, s);
+        case 7: return launch_sad5<7>(pl, pr, W, H, D, minD, magic, cost, s);
+        default: break;  // Dp = 512: its column sums exceed the static shared memory
+        }
     }
     const size_t smem = sad_cost_smem(Dp, r);
     return wide ? launch_sad_kp<true>(pl, pr, W, H, D, Dp, minD, r, magic, cost, smem, s)

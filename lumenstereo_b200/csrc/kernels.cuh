@@ -26,10 +26,6 @@ cudaError_t launch_census_cost(const uint32_t* cl, const uint32_t* cr, int W, in
 size_t sad_cost_smem(int Dp, int r);
 // Reciprocal table of the SAD window sizes: m[c] = ceil(2^32 / c), n entries.
 cudaError_t launch_magic(uint32_t* m, int n, cudaStream_t s);
-// The 5x5 window (sad5.cu) for padded disparity counts up to 448
-// (cudaErrorInvalidValue otherwise).
-cudaError_t launch_sad5w(const uint8_t* pl, const uint8_t* pr, int W, int H, int D, int Dp, int minD,
-                         const uint32_t* magic, uint8_t* cost, cudaStream_t s);
 cudaError_t launch_sad_cost(const uint8_t* pl, const uint8_t* pr, int W, int H, int D, int Dp,
                             int minD, int r, const uint32_t* magic, int wide, uint8_t* cost,
                             cudaStream_t s);
