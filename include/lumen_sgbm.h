@@ -124,9 +124,8 @@ lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule);
  * band (`warps_per_block`).  Schedule 4: 32 lanes with 4, 8 or 16 rows; 8
  * lanes (padded disparities up to 128) or 16 lanes (up to 256), rows as lane
  * teams, with 8, 16 or 32 rows.  Schedule 6: its lanes per row (8 up to 128
- * padded disparities, 16 up to 320) with 16, 24 or 32 rows, or 16 / 32 lanes
- * with 16 rows for padded disparities up to 128; a configuration without an
- * instance falls back to the default.  0, 0 restores the automatic choice.
+ * padded disparities, 16 up to 320) with 16, 24 or 32 rows; a configuration
+ * without an instance falls back to the default.  0, 0 restores the automatic choice.
  * Values are identical for every setting. */
 lumen_status lumen_sgbm_set_tuning(lumen_sgbm* h, int lanes_per_pixel, int warps_per_block);
 /* The schedule and configuration the last compute used: {schedule, lanes, warps}. */

@@ -675,15 +675,12 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
             cands.push_back({4, SweepConfig{tl, 32}});
         }
         if (mask == 0xFFu) {
-            // schedule 6 takes `warps` as its rows per band; lanes other than
-            // its default exist for padded disparities up to 128
+            // schedule 6 takes `warps` as its rows per band
             const int t6 = pair_lanes(Dp);
             if (t6) {
                 cands.push_back({6, SweepConfig{t6, 16}});
                 cands.push_back({6, SweepConfig{t6, 24}});
                 cands.push_back({6, SweepConfig{t6, 32}});
-                if (Dp <= 128) cands.push_back({6, SweepConfig{16, 16}});
-                if (Dp == 128) cands.push_back({6, SweepConfig{32, 16}});
             }
         }
     }

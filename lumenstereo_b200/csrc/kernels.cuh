@@ -95,10 +95,9 @@ struct PairPlan {
 };
 // lanes per row of schedule 6 for a padded disparity count (0: no instance)
 int pair_lanes(int Dp);
-// R: rows per band, 16 or 32 (0: the default, 16); T: lanes per row (0: the
-// default, pair_lanes(Dp); 16 or 32 also for padded disparities up to 128
-// with 16-row bands).  cudaErrorInvalidValue: no instance for these
-// disparities / sizes
+// R: rows per band, 16, 24 or 32 (0: the default, 16); T: lanes per row (0 or
+// pair_lanes(Dp)).  cudaErrorInvalidValue: no instance for these disparities
+// / sizes
 cudaError_t pair_plan(const SgmConsts& k, bool wrap, int numSMs, PairPlan* plan, int R = 0, int T = 0);
 // part[0..3]: the four sweeps' partial volumes (part[0] may be pv.agg).  xbuf:
 // the row buffers (plan.xbufBytes), every word of which holds an epoch below

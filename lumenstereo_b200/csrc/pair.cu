@@ -25,29 +25,21 @@ LUMEN_PAIR_EXTERN(8, 8, 24)
 LUMEN_PAIR_EXTERN(6, 16, 24)
 LUMEN_PAIR_EXTERN(8, 16, 24)
 LUMEN_PAIR_EXTERN(10, 16, 24)
-LUMEN_PAIR_EXTERN(2, 16, 16)
-LUMEN_PAIR_EXTERN(4, 16, 16)
-LUMEN_PAIR_EXTERN(2, 32, 16)
 #undef LUMEN_PAIR_EXTERN
 
 // lanes per row for a padded disparity count (0: no instance)
 int pair_lanes(int Dp) { return Dp <= 128 ? 8 : Dp <= 320 ? 16 : 0; }
 
-// whether an instance with T lanes per row and R rows per band exists
+// whether an instance with T lanes per row and R rows per band exists (wider
+// teams for the narrow ranges were measured slower on 1080p D128 -- 2.67 and
+// 2.73 ms against 2.03 ms with 8 lanes -- and are not built)
 static bool pair_instance(int Dp, int T, int R) {
-    if (T == pair_lanes(Dp)) return R == 16 || R == 24 || R == 32;
-    return R == 16 && ((T == 16 && (Dp == 64 || Dp == 128)) || (T == 32 && Dp == 128));
+    return T == pair_lanes(Dp) && (R == 16 || R == 24 || R == 32);
 }
 
 static cudaError_t pair_dispatch(const PairArgs& a, int Dp, int R, int T, bool wrap, bool full, int smem,
                                  int grid, cudaStream_t s, int* perSM) {
-    if (T != pair_lanes(Dp)) {
-        // wider teams for the narrow ranges: fewer words per lane, more warps
-        if (R == 16 && T == 16 && Dp == 64) return pair_launch_t<2, 16, 16>(a, wrap, full, smem, grid, s, perSM);
-        if (R == 16 && T == 16 && Dp == 128) return pair_launch_t<4, 16, 16>(a, wrap, full, smem, grid, s, perSM);
-        if (R == 16 && T == 32 && Dp == 128) return pair_launch_t<2, 32, 16>(a, wrap, full, smem, grid, s, perSM);
-        return cudaErrorInvalidValue;
-    }
+    if (T != pair_lanes(Dp)) return cudaErrorInvalidValue;
     if (R == 16) {
         switch (Dp) {
         case 64: return pair_launch_t<4, 8, 16>(a, wrap, full, smem, grid, s, perSM);

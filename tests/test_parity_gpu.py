@@ -210,11 +210,11 @@ def test_parity_schedule6_pair_sweeps(D, size, census, oracle_mod):
 @pytest.mark.parametrize("D,size,lanes,rows",
                          [(D, size, lanes, rows)
                           for D, size in [(40, (131, 53)), (64, (40, 200)), (128, (97, 150)), (100, (700, 90))]
-                          for lanes, rows in [(8, 24), (8, 32), (16, 16), (32, 16)]] +
+                          for lanes, rows in [(8, 24), (8, 32)]] +
                          [(D, size, 16, rows) for D, size in [(150, (160, 70)), (290, (330, 61))] for rows in (24, 32)])
 def test_parity_schedule6_configurations(D, size, lanes, rows, oracle_mod):
     """Every schedule-6 configuration the autotuner can pick (24- and 32-row
-    bands, 16- and 32-lane rows for padded disparities up to 128) reproduces the
+    bands) reproduces the
     oracle's summed volume bit for bit, both cost modes, partial last bands
     included."""
     w, h = size
