@@ -461,20 +461,21 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
             cfgChosen = true;
         }
     }
-    // untuned default: the four lag-free sweeps for 8 paths (schedule 6, which
-    // falls back to schedule 4 where it has no instance), schedule 4 for 4 paths
-    if (sched == 0) sched = mask == 0xFFu ? 6 : (sweepable ? 4 : 1);
+    // untuned default: the four lag-free sweeps (schedule 6; with 4 paths one
+    // path a sweep), which falls back to schedule 4 where it has no instance
+    if (sched == 0) sched = sweepable ? 6 : 1;
     if (sched != 1 && !sweepable) sched = 1;          // single-path debug masks: per-direction kernels
     PairPlan plan6{};
     if (sched == 6) {
-        // 4 paths, no instance for this range, or short of device memory for
-        // the four partial volumes and the row buffers: schedule 4
-        // rows per band and lanes per row: a pinned or tuned configuration
-        // when schedule 6 has that instance, else the defaults
+        // no instance for this range, or short of device memory for the four
+        // partial volumes and the row buffers: schedule 4.  Rows per band and
+        // lanes per row: a pinned or tuned configuration when schedule 6 has
+        // that instance, else the defaults
+        const bool diag = mask == 0xFFu;
         const int R6 = (cfgChosen && (cfg.NW == 16 || cfg.NW == 24 || cfg.NW == 32)) ? cfg.NW : 0;
         const int T6 = cfgChosen ? cfg.T : 0;
-        bool ok6 = mask == 0xFFu && (pair_plan(k, wrap, h->numSMs, &plan6, R6, T6) == cudaSuccess ||
-                                     pair_plan(k, wrap, h->numSMs, &plan6, R6) == cudaSuccess);
+        bool ok6 = pair_plan(k, wrap, diag, h->numSMs, &plan6, R6, T6) == cudaSuccess ||
+                   pair_plan(k, wrap, diag, h->numSMs, &plan6) == cudaSuccess;
         if (ok6)
             ok6 = h->partB.ensure(ND * 2) == cudaSuccess && h->partC.ensure(ND * 2) == cudaSuccess &&
                   h->partD.ensure(ND * 2) == cudaSuccess;
@@ -524,11 +525,14 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
         // every word of the row buffers must carry an epoch below the launch's:
         // zero them when they are new (marked by the epoch at its maximum) and
         // before the epoch would wrap
-        if (h->pairEpoch >= 0xFFFFFFF0u) {
-            LCU(cudaMemsetAsync(h->pairBuf.p, 0, h->pairBuf.n, s));
-            h->pairEpoch = 0;
+        unsigned epoch = 0;
+        if (plan6.diag) {
+            if (h->pairEpoch >= 0xFFFFFFF0u) {
+                LCU(cudaMemsetAsync(h->pairBuf.p, 0, h->pairBuf.n, s));
+                h->pairEpoch = 0;
+            }
+            epoch = ++h->pairEpoch;
         }
-        const unsigned epoch = ++h->pairEpoch;
         uint16_t* const parts[4] = {h->agg.as<uint16_t>(), h->partB.as<uint16_t>(), h->partC.as<uint16_t>(),
                                     h->partD.as<uint16_t>()};
         LCU(launch_aggregate_pair(pv, parts, k, wrap, plan6, h->pairBuf.as<unsigned long long>(), epoch,
@@ -674,11 +678,11 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
             cands.push_back({4, SweepConfig{tl, 16}});
             cands.push_back({4, SweepConfig{tl, 32}});
         }
-        if (mask == 0xFFu) {
-            // schedule 6 takes `warps` as its rows per band
-            const int t6 = pair_lanes(Dp);
-            if (t6) {
-                cands.push_back({6, SweepConfig{t6, 16}});
+        // schedule 6 takes `warps` as its rows per band (4 paths: 16 only)
+        const int t6 = pair_lanes(Dp);
+        if (t6) {
+            cands.push_back({6, SweepConfig{t6, 16}});
+            if (mask == 0xFFu) {
                 cands.push_back({6, SweepConfig{t6, 24}});
                 cands.push_back({6, SweepConfig{t6, 32}});
             }

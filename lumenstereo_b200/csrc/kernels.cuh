@@ -86,6 +86,7 @@ cudaError_t launch_aggregate_wave(const PairView& pv, uint16_t* partB, const Sgm
 // ---- schedule 6: four lag-free two-path sweeps (pair.cu, pair_kernel.cuh) ----
 struct PairPlan {
     int R, T;              // rows per band, lanes per row
+    bool diag;             // 8 paths (the diagonals ride along); false: LR, RL, TB, BT alone
     int nb0, nb1;          // bands of the row sweeps, of the column sweeps
     int nTickets;          // 2 * nb0 + 2 * nb1
     int grid;              // CTAs launched (persistent, ticket-scheduled)
@@ -95,10 +96,12 @@ struct PairPlan {
 };
 // lanes per row of schedule 6 for a padded disparity count (0: no instance)
 int pair_lanes(int Dp);
-// R: rows per band, 16, 24 or 32 (0: the default, 16); T: lanes per row (0 or
-// pair_lanes(Dp)).  cudaErrorInvalidValue: no instance for these disparities
-// / sizes
-cudaError_t pair_plan(const SgmConsts& k, bool wrap, int numSMs, PairPlan* plan, int R = 0, int T = 0);
+// diag: 8 paths; false: the 4 paths LR, RL, TB, BT (one per sweep, no band
+// hand-offs).  R: rows per band, 16, 24 or 32 with diag, 16 without (0: the
+// default, 16); T: lanes per row (0 or pair_lanes(Dp)).
+// cudaErrorInvalidValue: no instance for these disparities / sizes
+cudaError_t pair_plan(const SgmConsts& k, bool wrap, bool diag, int numSMs, PairPlan* plan, int R = 0,
+                      int T = 0);
 // part[0..3]: the four sweeps' partial volumes (part[0] may be pv.agg).  xbuf:
 // the row buffers (plan.xbufBytes), every word of which holds an epoch below
 // `epoch` (zero-filled when allocated, then one epoch per launch, increasing).

@@ -25,7 +25,15 @@ LUMEN_PAIR_EXTERN(8, 8, 24)
 LUMEN_PAIR_EXTERN(6, 16, 24)
 LUMEN_PAIR_EXTERN(8, 16, 24)
 LUMEN_PAIR_EXTERN(10, 16, 24)
+#define LUMEN_PAIR_EXTERN4(KW, T) \
+    extern template cudaError_t pair_launch_t<KW, T, 16, false>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
+LUMEN_PAIR_EXTERN4(4, 8)
+LUMEN_PAIR_EXTERN4(8, 8)
+LUMEN_PAIR_EXTERN4(6, 16)
+LUMEN_PAIR_EXTERN4(8, 16)
+LUMEN_PAIR_EXTERN4(10, 16)
 #undef LUMEN_PAIR_EXTERN
+#undef LUMEN_PAIR_EXTERN4
 
 // lanes per row for a padded disparity count (0: no instance)
 int pair_lanes(int Dp) { return Dp <= 128 ? 8 : Dp <= 320 ? 16 : 0; }
@@ -33,13 +41,24 @@ int pair_lanes(int Dp) { return Dp <= 128 ? 8 : Dp <= 320 ? 16 : 0; }
 // whether an instance with T lanes per row and R rows per band exists (wider
 // teams for the narrow ranges were measured slower on 1080p D128 -- 2.67 and
 // 2.73 ms against 2.03 ms with 8 lanes -- and are not built)
-static bool pair_instance(int Dp, int T, int R) {
-    return T == pair_lanes(Dp) && (R == 16 || R == 24 || R == 32);
+static bool pair_instance(int Dp, int T, int R, bool diag) {
+    return T == pair_lanes(Dp) && (diag ? (R == 16 || R == 24 || R == 32) : R == 16);
 }
 
-static cudaError_t pair_dispatch(const PairArgs& a, int Dp, int R, int T, bool wrap, bool full, int smem,
-                                 int grid, cudaStream_t s, int* perSM) {
+static cudaError_t pair_dispatch(const PairArgs& a, int Dp, int R, int T, bool diag, bool wrap, bool full,
+                                 int smem, int grid, cudaStream_t s, int* perSM) {
     if (T != pair_lanes(Dp)) return cudaErrorInvalidValue;
+    if (!diag) {
+        if (R != 16) return cudaErrorInvalidValue;
+        switch (Dp) {
+        case 64: return pair_launch_t<4, 8, 16, false>(a, wrap, full, smem, grid, s, perSM);
+        case 128: return pair_launch_t<8, 8, 16, false>(a, wrap, full, smem, grid, s, perSM);
+        case 192: return pair_launch_t<6, 16, 16, false>(a, wrap, full, smem, grid, s, perSM);
+        case 256: return pair_launch_t<8, 16, 16, false>(a, wrap, full, smem, grid, s, perSM);
+        case 320: return pair_launch_t<10, 16, 16, false>(a, wrap, full, smem, grid, s, perSM);
+        default: return cudaErrorInvalidValue;
+        }
+    }
     if (R == 16) {
         switch (Dp) {
         case 64: return pair_launch_t<4, 8, 16>(a, wrap, full, smem, grid, s, perSM);
@@ -73,14 +92,15 @@ static cudaError_t pair_dispatch(const PairArgs& a, int Dp, int R, int T, bool w
     return cudaErrorInvalidValue;
 }
 
-cudaError_t pair_plan(const SgmConsts& k, bool wrap, int numSMs, PairPlan* plan, int R, int T) {
+cudaError_t pair_plan(const SgmConsts& k, bool wrap, bool diag, int numSMs, PairPlan* plan, int R, int T) {
     if (!pair_lanes(k.Dp)) return cudaErrorInvalidValue;
     if (R == 0) R = 16;
     if (T == 0) T = pair_lanes(k.Dp);
-    if (!pair_instance(k.Dp, T, R)) return cudaErrorInvalidValue;
+    if (!pair_instance(k.Dp, T, R, diag)) return cudaErrorInvalidValue;
     PairPlan p{};
     p.R = R;
     p.T = T;
+    p.diag = diag;
     p.nb0 = (k.H + R - 1) / R;
     p.nb1 = (k.W + R - 1) / R;
     p.nTickets = 2 * p.nb0 + 2 * p.nb1;
@@ -88,11 +108,12 @@ cudaError_t pair_plan(const SgmConsts& k, bool wrap, int numSMs, PairPlan* plan,
     if (p.smem > 227 * 1024) return cudaErrorInvalidValue;
     PairArgs dummy{};
     int perSM = 0;
-    cudaError_t e = pair_dispatch(dummy, k.Dp, R, T, wrap, k.D == k.Dp, p.smem, 0, nullptr, &perSM);
+    cudaError_t e = pair_dispatch(dummy, k.Dp, R, T, diag, wrap, k.D == k.Dp, p.smem, 0, nullptr, &perSM);
     if (e != cudaSuccess) return e;
     if (perSM < 1) return cudaErrorInvalidConfiguration;
     p.grid = std::min(p.nTickets, perSM * numSMs);
-    p.xbufBytes = pair_xbase(3, p.nb1, k.W, k.H, p.nb0, p.nb1) * (size_t)pair_ll_words(k.Dp) * 8;
+    // band-boundary rows only when the diagonals cross the bands
+    p.xbufBytes = diag ? pair_xbase(3, p.nb1, k.W, k.H, p.nb0, p.nb1) * (size_t)pair_ll_words(k.Dp) * 8 : 0;
     p.counterWords = 1;   // the ticket counter
     *plan = p;
     return cudaSuccess;
@@ -128,7 +149,7 @@ cudaError_t launch_aggregate_pair(const PairView& pv, uint16_t* const part[4], c
     cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned) * plan.counterWords, s);
     if (e != cudaSuccess) return e;
     int perSM = 0;
-    return pair_dispatch(a, k.Dp, plan.R, plan.T, wrap, k.D == k.Dp, plan.smem, plan.grid, s, &perSM);
+    return pair_dispatch(a, k.Dp, plan.R, plan.T, plan.diag, wrap, k.D == k.Dp, plan.smem, plan.grid, s, &perSM);
 }
 
 }  // namespace lumen

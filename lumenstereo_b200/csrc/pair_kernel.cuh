@@ -101,8 +101,11 @@ __device__ __forceinline__ bool rows_barrier_or(int nThreads, bool v) {
     return r != 0;
 }
 
-template <int KW, bool WRAP, bool FULL, int R, int T>
-__global__ void __launch_bounds__((R / (32 / T) + 1) * 32)
+// DIAG = false: the four paths LR, RL, TB, BT alone (4-path mode).  Then no
+// row depends on another: bands have no import warp, no hand-off and no
+// per-step barrier, every row warp runs free.
+template <int KW, bool WRAP, bool FULL, int R, int T, bool DIAG = true>
+__global__ void __launch_bounds__((R / (32 / T) + (DIAG ? 1 : 0)) * 32)
 pair_kernel(PairArgs a) {
     constexpr int DP = 2 * KW * T;       // padded disparities
     constexpr int SB = pair_slot_bytes(DP);
@@ -157,7 +160,7 @@ pair_kernel(PairArgs a) {
         const int nbS = tr ? J.nb[1] : J.nb[0];
         const int v0 = b * R;
         const int lastActive = min(R - 1, Hs - 1 - v0);
-        const bool hasPrev = b > 0, hasNext = b + 1 < nbS;
+        const bool hasPrev = DIAG && b > 0, hasNext = DIAG && b + 1 < nbS;
         // ---- stage sweep rows v0-1 .. v0+R-1 of the image (column sweeps: row index fastest) ----
         for (int i = threadIdx.x; i < (R + 1) * Ws; i += blockDim.x) {
             int rr, u;
@@ -246,10 +249,21 @@ pair_kernel(PairArgs a) {
                 const int um = max(u - 1, 0);
                 const int cur = irow[u];
                 const uint32_t p2h = p2lut[abs(cur - irow[um])];
-                const uint32_t p2d = p2lut[abs(cur - iprev[um])];
                 // ---- horizontal path (its state starts at 0: L = C at u = 0) ----
                 uint32_t LnH[KW];
                 wave_step<KW, T, WRAP, FULL>(LH, Cw, minH, p2h, J.p1x2, J.bsub, mk, LnH);
+                if constexpr (!DIAG) {
+                    // one path a sweep: its vector is the sweep's partial sum
+                    minH = wave_min_t<KW, T>(LnH);
+#pragma unroll
+                    for (int w = 0; w < KW; ++w) LH[w] = LnH[w];
+                    if (rowOn) {
+                        store_words<KW>(pout, LnH);
+                        pout += pstep;
+                    }
+                    continue;
+                }
+                const uint32_t p2d = p2lut[abs(cur - iprev[um])];
                 // ---- diagonal path from the row above, pixel u-1 ----
                 const uint8_t* slot = (u == 0 || v == 0) ? zeroSlot
                                       : r == 0           ? impRing + ((u - 1) & (kPQ - 1)) * SB
@@ -393,12 +407,12 @@ namespace lumen {
 
 // Launch of one instance (the host picks KW, T and R from the padded
 // disparity count and the shared memory).  grid == 0: occupancy query only.
-template <int KW, int T, int R>
+template <int KW, int T, int R, bool DIAG = true>
 cudaError_t pair_launch_t(const PairArgs& a, bool wrap, bool full, int smem, int grid, cudaStream_t s,
                           int* perSM) {
-    constexpr int threads = (R / (32 / T) + 1) * 32;
-    void (*k)(PairArgs) = wrap ? (full ? pair_kernel<KW, true, true, R, T> : pair_kernel<KW, true, false, R, T>)
-                               : (full ? pair_kernel<KW, false, true, R, T> : pair_kernel<KW, false, false, R, T>);
+    constexpr int threads = (R / (32 / T) + (DIAG ? 1 : 0)) * 32;
+    void (*k)(PairArgs) = wrap ? (full ? pair_kernel<KW, true, true, R, T, DIAG> : pair_kernel<KW, true, false, R, T, DIAG>)
+                               : (full ? pair_kernel<KW, false, true, R, T, DIAG> : pair_kernel<KW, false, false, R, T, DIAG>);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, k, threads, smem);

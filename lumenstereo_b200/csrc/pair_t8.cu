@@ -6,4 +6,6 @@ template cudaError_t pair_launch_t<4, 8, 16>(const PairArgs&, bool, bool, int, i
 template cudaError_t pair_launch_t<8, 8, 16>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
 template cudaError_t pair_launch_t<4, 8, 32>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
 template cudaError_t pair_launch_t<8, 8, 32>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
+template cudaError_t pair_launch_t<4, 8, 16, false>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
+template cudaError_t pair_launch_t<8, 8, 16, false>(const PairArgs&, bool, bool, int, int, cudaStream_t, int*);
 }  // namespace lumen
