@@ -233,6 +233,29 @@ def test_parity_schedule6_configurations(D, size, lanes, rows, oracle_mod):
         assert_subpix_close(disp, ref_disp)
 
 
+@pytest.mark.parametrize("D,size", [(40, (131, 53)), (64, (40, 200)), (128, (97, 150)), (150, (160, 70)),
+                                    (290, (330, 41)), (16, (700, 9))])
+def test_parity_schedule6_four_paths(D, size, oracle_mod):
+    """4 paths through schedule 6 (LR, RL, TB, BT, one path a sweep, no band
+    hand-offs): the summed volume equals the oracle's bit for bit, both cost
+    modes, wider and taller images than a band, partial last bands."""
+    w, h = size
+    left, right, _ = synth.make_pair(synth.PairSpec(w, h, 4, 1, min(D - 1, 40), 2.0, 500 + D + w))
+    for census in (0, 1):
+        pd = params_dict(maxDisparity=D, numDirections=4, speckleWindowSize=0, matchingCostMode=census)
+        ref_disp, ref = oracle_mod.sgbm(pd, left, right, intermediates=True)
+        with StereoSGBM(to_params(pd)) as s:
+            s.set_schedule(6)
+            s.retain_intermediates(True)
+            disp = s.compute(left, right)
+            agg = s.intermediate("agg", (h, w, D), np.uint16)
+            assert s.get_tuning()[0] == 6
+        assert np.array_equal(agg, ref["agg"]), census
+        assert_subpix_close(disp, ref_disp)
+        with StereoSGBM(to_params(pd)) as s:   # the default picks it too, without retained volumes
+            assert np.array_equal(s.compute(left, right), disp)
+
+
 def test_schedule6_matches_schedule4_full_size():
     """1920x1080 D128 SAD and Census, 8 paths: the four-partial selection of
     schedule 6 gives schedule 4's maps (no intermediates retained)."""
