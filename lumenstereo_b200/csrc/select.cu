@@ -51,8 +51,15 @@ __device__ __forceinline__ int16_t subpixel_disp(float c0, float c1, float c2, i
 //    takes the min with the new pixel's keys.  The slot that leaves the top
 //    of the team holds a complete right pixel; it and the partial slots at a
 //    segment's two ends go to a row array in shared memory by atomicMin.
-// Subpixel neighbours are re-read from the (L1/L2-resident) volumes.  The
-// 1/16-px outputs equal the reference's bit for bit.
+// Subpixel neighbours (the costs at d - 1 and d + 1 of the winning pixel's
+// own vector) travel with the keys when NB: every element carries the
+// packed pair (c[d-1] << 16 | c[d+1]), taken from the lane's registers and
+// one shuffle from each neighbouring lane; a slot or a left-view minimum
+// that takes a key takes its pair, and the row array holds 64-bit
+// (key << 32 | pair) records.  Nothing is re-read, so the volumes cross
+// HBM once.  Without NB (rows too wide for 8 bytes a pixel of shared
+// memory) the neighbours are re-read from the volumes.  The 1/16-px
+// outputs equal the reference's bit for bit either way.
 // ---------------------------------------------------------------------------
 // w = a + b (+ c + d when NV == 4) over a lane's KS words (mod 2^16 per half when wrap)
 __device__ __forceinline__ uint32_t vsum(uint32_t x, uint32_t y, bool wrap) { return wrap ? __vadd2(x, y) : x + y; }
@@ -106,17 +113,23 @@ __device__ __forceinline__ uint32_t vol_cost(const uint16_t* __restrict__ a, con
     return v & 0xFFFFu;
 }
 
-template <int TL, int KS, bool FULL, int NV>
-__global__ void __launch_bounds__(256)
+// two CTAs an SM (128 registers) while the words fit; wider lanes take more registers
+template <int TL, int KS, bool FULL, int NV, bool NB>
+__global__ void __launch_bounds__(256, KS <= 8 ? 2 : 1)
 select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict__ aggB,
                     const uint16_t* __restrict__ aggC, const uint16_t* __restrict__ aggD, int wrap,
                     int W, int D, int Dp, int minD, int UR, int S, int16_t* __restrict__ dispL,
                     int16_t* __restrict__ dispR) {
     constexpr int M = 2 * KS;
     constexpr uint32_t INF = 0xFFFFFFFFu;
+    constexpr unsigned long long INF64 = ~0ull;
     extern __shared__ uint32_t rec[];  // [W] right-view keys of the row
+    unsigned long long* const rec64 = reinterpret_cast<unsigned long long*>(rec);  // [W] (key << 32 | pair), NB
     const int y = blockIdx.x;
-    for (int i = threadIdx.x; i < W; i += blockDim.x) rec[i] = INF;
+    for (int i = threadIdx.x; i < W; i += blockDim.x) {
+        if constexpr (NB) rec64[i] = INF64;
+        else rec[i] = INF;
+    }
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int tl = lane & (TL - 1);
@@ -128,9 +141,9 @@ select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict
     const uint16_t* rowB = aggB ? aggB + rowOff + d0 : nullptr;
     const uint16_t* rowC = NV == 4 ? aggC + rowOff + d0 : nullptr;
     const uint16_t* rowD = NV == 4 ? aggD + rowOff + d0 : nullptr;
-    uint32_t R[M];
+    uint32_t R[M], N[M];   // slot keys; NB: their neighbour pairs
 #pragma unroll
-    for (int j = 0; j < M; ++j) R[j] = INF;
+    for (int j = 0; j < M; ++j) R[j] = INF, N[j] = 0;
     uint32_t wn[KS];
     if (xs < W)
         slide_load<KS, NV>(rowA + (size_t)xs * Dp, rowB ? rowB + (size_t)xs * Dp : nullptr,
@@ -155,28 +168,60 @@ select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict
             const uint32_t leaving = R[q];
             const uint32_t incoming = __shfl_up_sync(kFullMask, leaving, 1, TL);
             R[q] = tl == 0 ? INF : incoming;
+            if constexpr (NB) N[q] = __shfl_up_sync(kFullMask, N[q], 1, TL);
+            // NB: the words holding d0 - 1 (previous lane) and d0 + M (next lane)
+            uint32_t prevW = 0, nextW = 0;
+            if constexpr (NB) {
+                prevW = __shfl_up_sync(kFullMask, w[KS - 1], 1, TL);
+                nextW = __shfl_down_sync(kFullMask, w[0], 1, TL);
+            }
             const uint32_t pxmask = px ? 0u : INF;
-            uint32_t k1 = INF, k2 = INF;
+            uint32_t k1 = INF, k2 = INF, n1 = 0;
 #pragma unroll
             for (int j = 0; j < M; ++j) {
                 const uint32_t c = (j & 1) ? (w[j >> 1] & 0xFFFF0000u) : (w[j >> 1] << 16);
                 uint32_t key = (c + (uint32_t)(d0 + j)) | pxmask;
                 if (!FULL) key |= (j < nv) ? 0u : INF;
                 const int p = ((j - u - 1) % M + M) % M;  // logical j after the slide
-                R[p] = min(R[p], key);
-                k2 = min(k2, max(k1, key));
-                k1 = min(k1, key);
+                if constexpr (NB) {
+                    // (c[d-1] << 16 | c[d+1]): odd j sits in the high half of its word
+                    const int i = j >> 1;
+                    const uint32_t nb = (j & 1) ? __byte_perm(w[i], i + 1 < KS ? w[i + 1] : nextW, 0x1054)
+                                                : __byte_perm(i > 0 ? w[i - 1] : prevW, w[i], 0x3276);
+                    const bool lt = key < R[p];
+                    R[p] = lt ? key : R[p];
+                    N[p] = lt ? nb : N[p];
+                    const bool l1 = key < k1;
+                    k2 = min(k2, max(k1, key));
+                    n1 = l1 ? nb : n1;
+                    k1 = l1 ? key : k1;
+                } else {
+                    R[p] = min(R[p], key);
+                    k2 = min(k2, max(k1, key));
+                    k1 = min(k1, key);
+                }
             }
             // complete right pixel: the top slot of the team
             if (tl == TL - 1) {
                 const int xr = x - minD - (M * TL - 1);
-                if (xr >= 0 && xr < W) atomicMin(&rec[xr], R[(M - 1 - u - 1 + 2 * M) % M]);
+                const int top = (M - 1 - u - 1 + 2 * M) % M;
+                if (xr >= 0 && xr < W) {
+                    if constexpr (NB) {
+                        if (R[top] != INF) atomicMin(&rec64[xr], ((unsigned long long)R[top] << 32) | N[top]);
+                    } else {
+                        atomicMin(&rec[xr], R[top]);
+                    }
+                }
             }
             // left view: merge the lanes' two smallest keys
 #pragma unroll
             for (int o = TL / 2; o >= 1; o >>= 1) {
                 const uint32_t b1 = __shfl_xor_sync(kFullMask, k1, o);
                 const uint32_t b2 = __shfl_xor_sync(kFullMask, k2, o);
+                if constexpr (NB) {
+                    const uint32_t bn = __shfl_xor_sync(kFullMask, n1, o);
+                    n1 = b1 < k1 ? bn : n1;
+                }
                 k2 = min(max(k1, b1), min(k2, b2));
                 k1 = min(k1, b1);
             }
@@ -186,6 +231,8 @@ select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict
                 int16_t out;
                 if (UR > 0 && second != 0xFFFFu && second <= best + (best * (uint32_t)UR) / 100u) {
                     out = -1;
+                } else if (NB && bestD > 0 && bestD < D - 1) {
+                    out = subpixel_disp((float)(n1 >> 16), (float)best, (float)(n1 & 0xFFFFu), bestD, D, minD);
                 } else if (bestD > 0 && bestD < D - 1) {
                     const size_t i0 = rowOff + (size_t)x * Dp + bestD;
                     out = subpixel_disp((float)vol_cost<NV>(agg, aggB, aggC, aggD, i0 - 1), (float)best,
@@ -204,15 +251,21 @@ select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict
 #pragma unroll
         for (int j = 0; j < M; ++j) {
             const int xr = xe - minD - (d0 + j);
-            if (R[j] != INF && xr >= 0 && xr < W) atomicMin(&rec[xr], R[j]);
+            if (R[j] != INF && xr >= 0 && xr < W) {
+                if constexpr (NB) atomicMin(&rec64[xr], ((unsigned long long)R[j] << 32) | N[j]);
+                else atomicMin(&rec[xr], R[j]);
+            }
         }
     }
     __syncthreads();
     for (int xr = threadIdx.x; xr < W; xr += blockDim.x) {
-        const uint32_t k = rec[xr];
+        const uint32_t k = NB ? (uint32_t)(rec64[xr] >> 32) : rec[xr];
         const int bestD = k == INF ? 0 : (int)(k & 0xFFFFu);
         int16_t out;
-        if (bestD > 0 && bestD < D - 1) {
+        if (NB && bestD > 0 && bestD < D - 1) {
+            const uint32_t nb = (uint32_t)rec64[xr];
+            out = subpixel_disp((float)(nb >> 16), (float)(k >> 16), (float)(nb & 0xFFFFu), bestD, D, minD);
+        } else if (bestD > 0 && bestD < D - 1) {
             const size_t i0 = rowOff + (size_t)(xr + minD + bestD) * Dp + bestD;
             out = subpixel_disp((float)vol_cost<NV>(agg, aggB, aggC, aggD, i0 - 1), (float)(k >> 16),
                                 (float)vol_cost<NV>(agg, aggB, aggC, aggD, i0 + 1), bestD, D, minD);
@@ -223,6 +276,8 @@ select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict
     }
 }
 
+constexpr size_t kSelectSmemMax = 227 * 1024;  // opt-in shared memory per block on sm_100
+
 template <int TL, int KS>
 static cudaError_t launch_select_slide(const uint16_t* agg, const uint16_t* aggB, bool wrap, int W, int H,
                                        int D, int Dp, int minD, int UR, int16_t* dispL, int16_t* dispR,
@@ -230,10 +285,13 @@ static cudaError_t launch_select_slide(const uint16_t* agg, const uint16_t* aggB
     constexpr int M = 2 * KS, kTeams = 256 / TL;
     const int seg = (W + kTeams - 1) / kTeams;
     const int S = (seg + M - 1) / M * M;
-    const size_t smem = (size_t)W * 4;
+    const bool nb = (size_t)W * 8 <= kSelectSmemMax;   // 64-bit row records fit
+    const size_t smem = (size_t)W * (nb ? 8 : 4);
     const bool four = aggB && aggC && aggD;
-    auto kern = four ? (D == Dp ? select_slide_kernel<TL, KS, true, 4> : select_slide_kernel<TL, KS, false, 4>)
-                     : (D == Dp ? select_slide_kernel<TL, KS, true, 2> : select_slide_kernel<TL, KS, false, 2>);
+    auto kern = nb ? (four ? (D == Dp ? select_slide_kernel<TL, KS, true, 4, true> : select_slide_kernel<TL, KS, false, 4, true>)
+                           : (D == Dp ? select_slide_kernel<TL, KS, true, 2, true> : select_slide_kernel<TL, KS, false, 2, true>))
+                   : (four ? (D == Dp ? select_slide_kernel<TL, KS, true, 4, false> : select_slide_kernel<TL, KS, false, 4, false>)
+                           : (D == Dp ? select_slide_kernel<TL, KS, true, 2, false> : select_slide_kernel<TL, KS, false, 2, false>));
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
@@ -242,8 +300,6 @@ static cudaError_t launch_select_slide(const uint16_t* agg, const uint16_t* aggB
                               minD, UR, S, dispL, dispR);
     return cudaGetLastError();
 }
-
-constexpr size_t kSelectSmemMax = 227 * 1024;  // opt-in shared memory per block on sm_100
 
 bool select_needs_summed_volume(int D, int Dp) {
     (void)D;
