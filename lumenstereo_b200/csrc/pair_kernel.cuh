@@ -104,9 +104,8 @@ __device__ __forceinline__ bool rows_barrier_or(int nThreads, bool v) {
 // DIAG = false: the four paths LR, RL, TB, BT alone (4-path mode).  Then no
 // row depends on another: bands have no import warp, no hand-off and no
 // per-step barrier, every row warp runs free.
-template <int KW, bool WRAP, bool FULL, int R, int T, bool DIAG = true>
-__global__ void __launch_bounds__((R / (32 / T) + (DIAG ? 1 : 0)) * 32)
-pair_kernel(PairArgs a) {
+template <int KW, bool WRAP, bool FULL, int R, int T, bool DIAG>
+__device__ __forceinline__ void pair_body(const PairArgs& a) {
     constexpr int DP = 2 * KW * T;       // padded disparities
     constexpr int SB = pair_slot_bytes(DP);
     constexpr int NL = pair_ll_words(DP);
@@ -200,6 +199,75 @@ pair_kernel(PairArgs a) {
                 exporter ? J.xbuf + pair_xbase(s, b, W, H, J.nb[0], J.nb[1]) * NL + tl * KW : nullptr;
             const unsigned long long ep = (unsigned long long)a.epoch << 32;
 
+            if constexpr (!DIAG) {
+                // one path a sweep, rows independent: costs arrive in batches of
+                // four pixels (one cp.async group a batch; batch q holds pixels
+                // 4q .. 4q+3 in ring slots p % kPPF, the ring holds two batches),
+                // and pixel u+1's cost words and P2 value are loaded during step
+                // u, before its reduction, so their latency overlaps the shuffles
+                static_assert(kPPF == 8, "two batches of four pixels");
+                ptrdiff_t qofs = pix0 * DP + off;   // bytes from J.cost of the next batch's first pixel
+                const ptrdiff_t qstep = du * DP;
+                auto prefetch_batch = [&](int q) {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const int p = 4 * q + k;
+                        if (rowOn && p < Ws) {
+                            const uint8_t* src = J.cost + (qofs + k * qstep);
+                            const uint32_t dst = w_smem_addr(costRing + (p % kPPF) * DP + off);
+                            if constexpr ((2 * KW) % 16 == 0) {
+#pragma unroll
+                                for (int c = 0; c < (2 * KW) / 16; ++c) w_cp_async16(dst + 16 * c, src + 16 * c);
+                            } else {
+#pragma unroll
+                                for (int c = 0; c < KW / 2; ++c)
+                                    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst + 4 * c),
+                                                 "l"(src + 4 * c)
+                                                 : "memory");
+                            }
+                        }
+                    }
+                    qofs += 4 * qstep;
+                    w_cp_commit();
+                };
+                uint32_t Cw[KW];
+                uint32_t p2h;
+                auto load_operands = [&](int u) {
+                    load_cost_words<KW>(costRing + (u % kPPF) * DP + off, Cw);
+                    if (WRAP || J.costScale != 1) {
+#pragma unroll
+                        for (int w = 0; w < KW; ++w) Cw[w] = scale_cost<WRAP>(Cw[w], J.costScale);
+                    }
+                    p2h = p2lut[abs(irow[u] - irow[max(u - 1, 0)])];
+                };
+                prefetch_batch(0);
+                prefetch_batch(1);
+                w_cp_wait<1>();
+                load_operands(0);
+                uint32_t LH[KW];
+#pragma unroll
+                for (int w = 0; w < KW; ++w) LH[w] = 0;
+                uint32_t minH = 0;
+                for (int u = 0; u < Ws; ++u) {
+                    uint32_t LnH[KW];
+                    wave_step<KW, T, WRAP, FULL>(LH, Cw, minH, p2h, J.p1x2, J.bsub, mk, LnH);
+                    if (u + 1 < Ws) {
+                        if ((u & 3) == 3) {
+                            prefetch_batch((u >> 2) + 2);   // into the slots of pixels u-3 .. u, all read
+                            w_cp_wait<1>();                 // batch (u >> 2) + 1, pixels u+1 .. u+4, has landed
+                        }
+                        load_operands(u + 1);
+                    }
+                    minH = wave_min_t<KW, T>(LnH);
+#pragma unroll
+                    for (int w = 0; w < KW; ++w) LH[w] = LnH[w];
+                    if (rowOn) {
+                        store_words<KW>(pout, LnH);
+                        pout += pstep;
+                    }
+                }
+                w_cp_wait<0>();
+            } else {
             // cost of pixel p = step + kPPF - 1 of this row: `cofs` (bytes from
             // J.cost) follows p, incremented instead of recomputed; the calls
             // come with step = -(kPPF - 1), -(kPPF - 2), ..., i.e. p = 0, 1, ...
@@ -252,17 +320,6 @@ pair_kernel(PairArgs a) {
                 // ---- horizontal path (its state starts at 0: L = C at u = 0) ----
                 uint32_t LnH[KW];
                 wave_step<KW, T, WRAP, FULL>(LH, Cw, minH, p2h, J.p1x2, J.bsub, mk, LnH);
-                if constexpr (!DIAG) {
-                    // one path a sweep: its vector is the sweep's partial sum
-                    minH = wave_min_t<KW, T>(LnH);
-#pragma unroll
-                    for (int w = 0; w < KW; ++w) LH[w] = LnH[w];
-                    if (rowOn) {
-                        store_words<KW>(pout, LnH);
-                        pout += pstep;
-                    }
-                    continue;
-                }
                 const uint32_t p2d = p2lut[abs(cur - iprev[um])];
                 // ---- diagonal path from the row above, pixel u-1 ----
                 const uint8_t* slot = (u == 0 || v == 0) ? zeroSlot
@@ -306,6 +363,7 @@ pair_kernel(PairArgs a) {
                 if (threadIdx.x == 0 && hasPrev) w_st_release_cta(&sctr[1], (unsigned)u);
             }
             w_cp_wait<0>();
+            }
         } else if (hasPrev) {
             // ===================== import warp: the band above's last row =====================
             const unsigned long long* xin = J.xbuf + pair_xbase(s, b - 1, W, H, J.nb[0], J.nb[1]) * NL;
@@ -401,6 +459,20 @@ pair_kernel(PairArgs a) {
     }
 }
 
+// Eight paths: R/(32/T) row warps and the import warp.
+template <int KW, bool WRAP, bool FULL, int R, int T>
+__global__ void __launch_bounds__((R / (32 / T) + 1) * 32) pair_kernel(PairArgs a) {
+    pair_body<KW, WRAP, FULL, R, T, true>(a);
+}
+
+// Four paths: row warps only.  The explicit one-CTA-an-SM register budget
+// lets the compiler keep more of the next pixel's operands in flight
+// (measured faster than the default budget).
+template <int KW, bool WRAP, bool FULL, int R, int T>
+__global__ void __launch_bounds__(R / (32 / T) * 32, 1) pair4_kernel(PairArgs a) {
+    pair_body<KW, WRAP, FULL, R, T, false>(a);
+}
+
 }  // namespace lumen
 
 namespace lumen {
@@ -411,8 +483,13 @@ template <int KW, int T, int R, bool DIAG = true>
 cudaError_t pair_launch_t(const PairArgs& a, bool wrap, bool full, int smem, int grid, cudaStream_t s,
                           int* perSM) {
     constexpr int threads = (R / (32 / T) + (DIAG ? 1 : 0)) * 32;
-    void (*k)(PairArgs) = wrap ? (full ? pair_kernel<KW, true, true, R, T, DIAG> : pair_kernel<KW, true, false, R, T, DIAG>)
-                               : (full ? pair_kernel<KW, false, true, R, T, DIAG> : pair_kernel<KW, false, false, R, T, DIAG>);
+    void (*k)(PairArgs);
+    if constexpr (DIAG)
+        k = wrap ? (full ? pair_kernel<KW, true, true, R, T> : pair_kernel<KW, true, false, R, T>)
+                 : (full ? pair_kernel<KW, false, true, R, T> : pair_kernel<KW, false, false, R, T>);
+    else
+        k = wrap ? (full ? pair4_kernel<KW, true, true, R, T> : pair4_kernel<KW, true, false, R, T>)
+                 : (full ? pair4_kernel<KW, false, true, R, T> : pair4_kernel<KW, false, false, R, T>);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(perSM, k, threads, smem);

@@ -57,8 +57,9 @@ __device__ __forceinline__ int16_t subpixel_disp(float c0, float c1, float c2, i
 // one shuffle from each neighbouring lane; a slot or a left-view minimum
 // that takes a key takes its pair, and the row array holds 64-bit
 // (key << 32 | pair) records.  Nothing is re-read, so the volumes cross
-// HBM once.  Without NB (rows too wide for 8 bytes a pixel of shared
-// memory) the neighbours are re-read from the volumes.  The 1/16-px
+// HBM once.  Without NB (lanes of more than 8 words, or rows too wide
+// for 8 bytes a pixel of shared memory) the neighbours are re-read from the
+// volumes.  The 1/16-px
 // outputs equal the reference's bit for bit either way.
 // ---------------------------------------------------------------------------
 // w = a + b (+ c + d when NV == 4) over a lane's KS words (mod 2^16 per half when wrap)
@@ -113,13 +114,12 @@ __device__ __forceinline__ uint32_t vol_cost(const uint16_t* __restrict__ a, con
     return v & 0xFFFFu;
 }
 
-// two CTAs an SM (128 registers) while the words fit; wider lanes take more registers
 template <int TL, int KS, bool FULL, int NV, bool NB>
-__global__ void __launch_bounds__(256, KS <= 8 ? 2 : 1)
-select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict__ aggB,
-                    const uint16_t* __restrict__ aggC, const uint16_t* __restrict__ aggD, int wrap,
-                    int W, int D, int Dp, int minD, int UR, int S, int16_t* __restrict__ dispL,
-                    int16_t* __restrict__ dispR) {
+__device__ __forceinline__ void
+select_slide_body(const uint16_t* __restrict__ agg, const uint16_t* __restrict__ aggB,
+                  const uint16_t* __restrict__ aggC, const uint16_t* __restrict__ aggD, int wrap,
+                  int W, int D, int Dp, int minD, int UR, int S, int16_t* __restrict__ dispL,
+                  int16_t* __restrict__ dispR) {
     constexpr int M = 2 * KS;
     constexpr uint32_t INF = 0xFFFFFFFFu;
     constexpr unsigned long long INF64 = ~0ull;
@@ -276,6 +276,27 @@ select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict
     }
 }
 
+// Neighbours re-read: the compiler's own register budget.
+template <int TL, int KS, bool FULL, int NV>
+__global__ void __launch_bounds__(256)
+select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict__ aggB,
+                    const uint16_t* __restrict__ aggC, const uint16_t* __restrict__ aggD, int wrap,
+                    int W, int D, int Dp, int minD, int UR, int S, int16_t* __restrict__ dispL,
+                    int16_t* __restrict__ dispR) {
+    select_slide_body<TL, KS, FULL, NV, false>(agg, aggB, aggC, aggD, wrap, W, D, Dp, minD, UR, S, dispL, dispR);
+}
+
+// Neighbours carried: two CTAs an SM with 128 registers for the words and their pairs
+// (measured faster than the default budget).
+template <int TL, int KS, bool FULL, int NV>
+__global__ void __launch_bounds__(256, 2)
+select_slide_nb_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict__ aggB,
+                       const uint16_t* __restrict__ aggC, const uint16_t* __restrict__ aggD, int wrap,
+                       int W, int D, int Dp, int minD, int UR, int S, int16_t* __restrict__ dispL,
+                       int16_t* __restrict__ dispR) {
+    select_slide_body<TL, KS, FULL, NV, true>(agg, aggB, aggC, aggD, wrap, W, D, Dp, minD, UR, S, dispL, dispR);
+}
+
 constexpr size_t kSelectSmemMax = 227 * 1024;  // opt-in shared memory per block on sm_100
 
 template <int TL, int KS>
@@ -285,13 +306,21 @@ static cudaError_t launch_select_slide(const uint16_t* agg, const uint16_t* aggB
     constexpr int M = 2 * KS, kTeams = 256 / TL;
     const int seg = (W + kTeams - 1) / kTeams;
     const int S = (seg + M - 1) / M * M;
-    const bool nb = (size_t)W * 8 <= kSelectSmemMax;   // 64-bit row records fit
+    // 64-bit row records fit; wider lanes keep re-reading (measured: with 10 words a
+    // lane the registers of the pairs cost more than the re-reads save)
+    const bool nb = KS <= 8 && (size_t)W * 8 <= kSelectSmemMax;
     const size_t smem = (size_t)W * (nb ? 8 : 4);
     const bool four = aggB && aggC && aggD;
-    auto kern = nb ? (four ? (D == Dp ? select_slide_kernel<TL, KS, true, 4, true> : select_slide_kernel<TL, KS, false, 4, true>)
-                           : (D == Dp ? select_slide_kernel<TL, KS, true, 2, true> : select_slide_kernel<TL, KS, false, 2, true>))
-                   : (four ? (D == Dp ? select_slide_kernel<TL, KS, true, 4, false> : select_slide_kernel<TL, KS, false, 4, false>)
-                           : (D == Dp ? select_slide_kernel<TL, KS, true, 2, false> : select_slide_kernel<TL, KS, false, 2, false>));
+    void (*kern)(const uint16_t*, const uint16_t*, const uint16_t*, const uint16_t*, int, int, int, int, int, int,
+                 int, int16_t*, int16_t*);
+    if constexpr (KS <= 8)
+        kern = nb ? (four ? (D == Dp ? select_slide_nb_kernel<TL, KS, true, 4> : select_slide_nb_kernel<TL, KS, false, 4>)
+                          : (D == Dp ? select_slide_nb_kernel<TL, KS, true, 2> : select_slide_nb_kernel<TL, KS, false, 2>))
+                  : (four ? (D == Dp ? select_slide_kernel<TL, KS, true, 4> : select_slide_kernel<TL, KS, false, 4>)
+                          : (D == Dp ? select_slide_kernel<TL, KS, true, 2> : select_slide_kernel<TL, KS, false, 2>));
+    else
+        kern = four ? (D == Dp ? select_slide_kernel<TL, KS, true, 4> : select_slide_kernel<TL, KS, false, 4>)
+                    : (D == Dp ? select_slide_kernel<TL, KS, true, 2> : select_slide_kernel<TL, KS, false, 2>);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
