@@ -481,7 +481,8 @@ def run_batch(args):
     for (p, dl, dr, w, h), o in zip(pairs, out):
         batch.add(p, dl.data_ptr(), dr.data_ptr(), w, h, o.data_ptr())
     best_rows, best_ms = batch.autotune(sptr, repeats=2)
-    tune = {"rows_per_band": best_rows, "ms": best_ms}
+    best_sched, _ = batch.config()
+    tune = {"schedule": best_sched, "rows_per_band": best_rows, "ms": best_ms}
     for _ in range(max(args.warmup, 2)):
         batch.run(sptr)
     batch.sync(sptr)
@@ -516,7 +517,8 @@ def run_batch(args):
            "config": {"workload": f"mixed_stream_{len(pairs)}_pairs", "seeds": f"100..{99 + len(pairs)}",
                       "sizes": "640x480 D64, 1280x720 D128, 1920x1080 D128, 2880x1988 D192",
                       "cost": "Census/SAD 50/50", "paths": "4/8", "pixel_disparities": pd_total,
-                      "rows_per_band": best_rows, "graph": True, "groups": info["groups"],
+                      "schedule": best_sched, "rows_per_band": best_rows, "graph": True,
+                      "groups": info["groups"],
                       "device_bytes": info["device_bytes"]},
            "plain_loop": {"value": plain_rate, "unit": "pairs/s", "ms": statistics.mean(plain_ms)},
            "speedup_vs_plain_loop": value / plain_rate,

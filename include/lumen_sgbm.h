@@ -150,12 +150,15 @@ lumen_status lumen_sgbm_tuning_load(lumen_sgbm* h, const char* path);
  * pixel.  The debug-retain flag must have been set before the compute. */
 lumen_status lumen_sgbm_debug_retain(lumen_sgbm* h, int enable);
 lumen_status lumen_sgbm_debug_copy(lumen_sgbm* h, int which, void* dst, size_t dst_bytes);
-/* Band timeline of the lockstep row-band sweeps (schedule 4) for the next
- * computes (enable = 1) or off (0).  lumen_sgbm_debug_trace_copy returns the
- * last such launch's records, 4 words per band ticket t (t = 2*band + sweep):
+/* Band timeline of the row-band sweeps for the next computes (enable = 1) or
+ * off (0).  lumen_sgbm_debug_trace_copy returns the last such launch's
+ * records, 4 words per band ticket t.  Schedule 4 (t = 2*band + sweep):
  * globaltimer ns when the band's first row and its last row finished the
  * middle pixel (u = width / 2), when the band ended, and SM id << 48 |
  * import polls << 32 | export polls << 16 | row waits on the helpers.
+ * Schedule 6 with the diagonal paths (t in the sweeps' ticket order): when
+ * the band's rows started their first pixel, finished the middle pixel and
+ * finished the row, and SM id << 32 | sweep << 16 | 1.
  * *words receives the record size; dst may be NULL to query it. */
 lumen_status lumen_sgbm_debug_trace(lumen_sgbm* h, int enable);
 lumen_status lumen_sgbm_debug_trace_copy(lumen_sgbm* h, unsigned long long* dst,
@@ -271,8 +274,10 @@ lumen_status lumen_rectify_maps_device(const double K[9], const double dist[5], 
  * of width*height bytes with row pitch width; int16 DEVICE outputs with row
  * pitch width, 1/16 px, -1 invalid).  lumen_sgbm_batch_run enqueues every pair
  * on `stream`: cost volumes per pair, one persistent aggregation launch per
- * group of pairs of one kernel class (the wavefronts of all its pairs share
- * the GPU), then selection per pair; consecutive groups overlap on the device
+ * group of pairs of one kernel class (the sweeps of all its pairs share the
+ * GPU; schedule 6, the default: the four lag-free sweeps of the plain call's
+ * 8- and 4-path default, over every pair's bands; schedule 4: the two
+ * wavefront sweeps), then selection per pair; consecutive groups overlap on the device
  * (one group's sweep beside the next one's cost volumes and the previous one's
  * selections, on internal streams joined back into `stream`).  The first run
  * after an add, a clear or an option change plans and allocates one pooled
@@ -288,15 +293,23 @@ lumen_status lumen_sgbm_batch_add(lumen_sgbm_batch* b, const lumen_stereo_params
                                   const uint8_t* d_left, const uint8_t* d_right, int width,
                                   int height, int16_t* d_out);
 lumen_status lumen_sgbm_batch_clear(lumen_sgbm_batch* b);
-/* rows_per_band: 4, 8 or 16 (0 = 8); use_graph: capture and replay; budget 0 = keep. */
+/* rows_per_band: 4, 8 or 16 with schedule 4, 16, 24 or 32 with schedule 6 (0 = the
+ * schedule's default, 8 / 16); use_graph: capture and replay; budget 0 = keep. */
 lumen_status lumen_sgbm_batch_set_options(lumen_sgbm_batch* b, int rows_per_band, int use_graph,
                                           size_t device_budget_bytes);
 lumen_status lumen_sgbm_batch_run(lumen_sgbm_batch* b, void* stream);
 /* Autotuner of the batched launch (no counterpart in the reference): runs the
- * batch with 4, 8 and 16 rows per band (`repeats` timed runs each, on
- * `stream`, writing the outputs) and keeps the fastest for later runs. */
+ * batch with schedule 6 at 16, 24 and 32 rows per band and schedule 4 at 4, 8
+ * and 16 (only the pinned schedule's, when one is set) -- `repeats` timed runs
+ * each, on `stream`, writing the outputs -- and keeps the fastest schedule and
+ * band height for later runs. */
 lumen_status lumen_sgbm_batch_autotune(lumen_sgbm_batch* b, void* stream, int repeats, int* best_rows,
                                        float* best_ms);
+/* Aggregation schedule of the batch: 0 (automatic: 6 until the autotuner
+ * picks), 4 or 6 (no counterpart in the reference). */
+lumen_status lumen_sgbm_batch_set_schedule(lumen_sgbm_batch* b, int schedule);
+/* The schedule and rows per band the next run plans with. */
+lumen_status lumen_sgbm_batch_config(const lumen_sgbm_batch* b, int* schedule, int* rows_per_band);
 lumen_status lumen_sgbm_batch_sync(lumen_sgbm_batch* b, void* stream);
 /* Pooled device bytes, number of launch groups, kernels per run. */
 lumen_status lumen_sgbm_batch_info(const lumen_sgbm_batch* b, size_t* device_bytes, int* groups,
@@ -316,7 +329,7 @@ typedef struct lumen_server lumen_server;
 typedef struct lumen_server_options {
     size_t device_budget_bytes; /* arena size; default 40 GiB */
     int max_batch_pairs;        /* default 32 */
-    int rows_per_band;          /* 4, 8 (default) or 16 */
+    int rows_per_band;          /* schedule 4: 4, 8 or 16; schedule 6: 16 (default), 24 or 32 */
     int max_inflight;           /* batch slots on the device at once, 1..8; default 2 */
     int watchdog_ms;            /* host deadline of a batch, 0 = none; default 60000 */
     long long spin_limit;       /* device-side wait limit, 0 = default (2^24) */
@@ -324,6 +337,8 @@ typedef struct lumen_server_options {
                                    whose device-side waits run out are computed again one by one
                                    through the plain call (lumen_sgbm_compute_device with the
                                    default wait limit); 0: they complete with the batch's error */
+    int schedule;               /* aggregation of the batches: 6 (default, four lag-free sweeps)
+                                   or 4 (two wavefront sweeps) */
 } lumen_server_options;
 typedef struct lumen_request_info {
     lumen_status status;

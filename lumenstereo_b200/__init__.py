@@ -277,14 +277,16 @@ class StereoSGBM:
         _check(_lib.lib().lumen_sgbm_tuning_load(self._h, path.encode()))
 
     def enable_trace(self, enable: bool = True) -> None:
-        """Record the band timeline of the lockstep row-band sweeps (schedule 4)."""
+        """Record the band timeline of the row-band sweeps (schedules 4 and 6)."""
         _check(_lib.lib().lumen_sgbm_debug_trace(self._h, int(enable)))
 
     def trace(self) -> np.ndarray:
-        """Band timeline of the last schedule-4 launch: one row per band
-        ticket (2*band + sweep): [first row at the middle pixel ns, last row at
-        the middle pixel ns, end ns, sm << 48 | import polls << 32 | export
-        polls << 16 | row waits]."""
+        """Band timeline of the last traced launch, one row per band ticket.
+        Schedule 4 (ticket 2*band + sweep): [first row at the middle pixel ns,
+        last row at the middle pixel ns, end ns, sm << 48 | import polls << 32
+        | export polls << 16 | row waits].  Schedule 6 (its ticket order):
+        [rows start the first pixel ns, rows finish the middle pixel ns, rows
+        finish the row ns, sm << 32 | sweep << 16 | 1]."""
         lib = _lib.lib()
         n = C.c_size_t(0)
         _check(lib.lumen_sgbm_debug_trace_copy(self._h, None, 0, C.byref(n)))
@@ -319,10 +321,24 @@ class StereoBatch:
     per kernel class, optionally replayed from a CUDA graph
     (lumen_sgbm_batch_* in include/lumen_sgbm.h)."""
 
-    def __init__(self, rows_per_band: int = 0, use_graph: bool = False, budget_bytes: int = 0):
+    def __init__(self, rows_per_band: int = 0, use_graph: bool = False, budget_bytes: int = 0,
+                 schedule: int = 0):
         self._h = C.c_void_p()
         _check(_lib.lib().lumen_sgbm_batch_create(C.byref(self._h)))
         self.set_options(rows_per_band, use_graph, budget_bytes)
+        if schedule:
+            self.set_schedule(schedule)
+
+    def set_schedule(self, schedule: int = 0) -> None:
+        """Aggregation of the batch: 6 (four lag-free sweeps), 4 (two wavefront
+        sweeps) or 0 (automatic: 6 until the autotuner picks)."""
+        _check(_lib.lib().lumen_sgbm_batch_set_schedule(self._h, schedule))
+
+    def config(self):
+        """(schedule, rows per band) the next run uses."""
+        sc, r = C.c_int(0), C.c_int(0)
+        _check(_lib.lib().lumen_sgbm_batch_config(self._h, C.byref(sc), C.byref(r)))
+        return sc.value, r.value
 
     def set_options(self, rows_per_band: int = 0, use_graph: bool = False, budget_bytes: int = 0) -> None:
         _check(_lib.lib().lumen_sgbm_batch_set_options(self._h, rows_per_band, int(use_graph), budget_bytes))
@@ -343,8 +359,10 @@ class StereoBatch:
         _check(_lib.lib().lumen_sgbm_batch_sync(self._h, stream))
 
     def autotune(self, stream: int = 0, repeats: int = 2):
-        """Times the batch at 4, 8 and 16 rows per band and keeps the fastest:
-        (rows, ms per run)."""
+        """Times the batch with schedule 6 at 16, 24 and 32 rows per band and
+        schedule 4 at 4, 8 and 16 (only the schedule set_schedule pinned, if
+        any) and keeps the fastest: (rows, ms per run); config() gives the
+        schedule."""
         r, ms = C.c_int(0), C.c_float(0)
         _check(_lib.lib().lumen_sgbm_batch_autotune(self._h, stream, repeats, C.byref(r), C.byref(ms)))
         return r.value, ms.value
@@ -382,9 +400,9 @@ class StereoServer:
             disparity, info = srv.wait(rid)                     # info: latency_ms, ...
     """
 
-    def __init__(self, budget_bytes: int = 40 << 30, max_batch_pairs: int = 32, rows_per_band: int = 8,
+    def __init__(self, budget_bytes: int = 40 << 30, max_batch_pairs: int = 32, rows_per_band: int = 16,
                  max_inflight: int = 2, watchdog_ms: int = 60000, spin_limit: int = 0,
-                 plain_fallback: bool = True):
+                 plain_fallback: bool = True, schedule: int = 6):
         o = _lib.CServerOptions()
         _lib.lib().lumen_server_options_default(C.byref(o))
         o.device_budget_bytes = budget_bytes
@@ -394,6 +412,7 @@ class StereoServer:
         o.watchdog_ms = watchdog_ms
         o.spin_limit = spin_limit
         o.plain_fallback = 1 if plain_fallback else 0
+        o.schedule = schedule
         self._h = C.c_void_p()
         self._outs = {}
         _check(_lib.lib().lumen_server_create(C.byref(o), C.byref(self._h)))

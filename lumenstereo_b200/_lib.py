@@ -37,7 +37,7 @@ class CParams(C.Structure):
 class CServerOptions(C.Structure):
     _fields_ = [("device_budget_bytes", C.c_size_t), ("max_batch_pairs", C.c_int),
                 ("rows_per_band", C.c_int), ("max_inflight", C.c_int), ("watchdog_ms", C.c_int),
-                ("spin_limit", C.c_longlong), ("plain_fallback", C.c_int)]
+                ("spin_limit", C.c_longlong), ("plain_fallback", C.c_int), ("schedule", C.c_int)]
 
 
 class CRequestInfo(C.Structure):
@@ -98,6 +98,8 @@ def _declare(lib):
         "lumen_sgbm_batch_sync": (i, [vp, vp]),
         "lumen_sgbm_batch_autotune": (i, [vp, vp, i, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
         "lumen_sgbm_batch_info": (i, [vp, C.POINTER(sz), C.POINTER(C.c_int), C.POINTER(C.c_ulonglong)]),
+        "lumen_sgbm_batch_set_schedule": (i, [vp, i]),
+        "lumen_sgbm_batch_config": (i, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "lumen_server_options_default": (None, [C.POINTER(CServerOptions)]),
         "lumen_server_create": (i, [C.POINTER(CServerOptions), C.POINTER(vp)]),
         "lumen_server_destroy": (i, [vp]),

@@ -535,9 +535,16 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
         }
         uint16_t* const parts[4] = {h->agg.as<uint16_t>(), h->partB.as<uint16_t>(), h->partC.as<uint16_t>(),
                                     h->partD.as<uint16_t>()};
+        unsigned long long* trace = nullptr;
+        if (h->traceOn) {
+            h->traceWords = 4 * (size_t)plan6.nTickets;
+            LCU(h->trace.ensure(h->traceWords * 8));
+            LCU(cudaMemsetAsync(h->trace.p, 0, h->traceWords * 8, s));
+            trace = h->trace.as<unsigned long long>();
+        }
         LCU(launch_aggregate_pair(pv, parts, k, wrap, plan6, h->pairBuf.as<unsigned long long>(), epoch,
                                   h->counters.as<unsigned>(), h->status.as<int>(), h->spinMax, s,
-                                  h->stallTest));
+                                  h->stallTest, trace));
         h->statusPending = true;
         nl += 1;
         cfg = SweepConfig{plan6.T, plan6.R};

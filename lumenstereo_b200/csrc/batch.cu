@@ -32,6 +32,7 @@
 #include "batch_tickets.h"
 #include "common.cuh"
 #include "kernels.cuh"
+#include "pair_kernel.cuh"
 #include "wave_kernel.cuh"
 
 namespace lumen {
@@ -104,26 +105,48 @@ lumen_status batch_pair_init(BatchPair& q, const lumen_stereo_params* p, const u
     return LUMEN_OK;
 }
 
-size_t batch_pair_layout(BatchPair& q, int R, size_t start) {
+size_t batch_pair_layout(BatchPair& q, int sched, int R, size_t start) {
     const size_t N = (size_t)q.W * q.H, ND = N * q.Dp;
+    if (sched == 6 && !q.diag) R = 16;   // the four one-path sweeps have one band height
+    q.sched = sched;
+    q.R = R;
     q.nBands = (q.H + R - 1) / R;
+    q.nb0 = (q.H + R - 1) / R;
+    q.nb1 = (q.W + R - 1) / R;
     size_t o = start;
     auto take = [&](size_t n) { const size_t r0 = o; o += align256(n); return r0; };
     q.oCost = take(ND);
     q.oAgg = take(ND * 2);
     q.oPartB = take(ND * 2);
+    q.oPartC = q.oPartD = q.oRing = q.oCtr = q.oXbuf = 0;
+    q.xbufBytes = 0;
+    if (sched == 6) {
+        q.oPartC = take(ND * 2);
+        q.oPartD = take(ND * 2);
+    }
     q.oDispL = take(N * 2);
     q.oDispR = take(N * 2);
     q.oAux0 = take(q.census ? N * 4 : N);
     q.oAux1 = take(q.census ? N * 4 : N);
-    q.oRing = take(wave_ring_bytes(q.nBands, q.Dp, q.diag));
-    q.oCtr = take(ctr_bytes(q.nBands));
+    if (sched == 6) {
+        if (q.diag) {
+            q.xbufBytes = pair_xbuf_bytes(q.W, q.H, q.Dp, R);
+            q.oXbuf = take(q.xbufBytes);
+        }
+    } else {
+        q.oRing = take(wave_ring_bytes(q.nBands, q.Dp, q.diag));
+        q.oCtr = take(ctr_bytes(q.nBands));
+    }
     return o;
 }
 
-size_t batch_pair_bytes(const BatchPair& q, int R) {
+size_t batch_pair_bytes(const BatchPair& q, int sched, int R) {
     BatchPair t = q;
-    return batch_pair_layout(t, R, 0);
+    return batch_pair_layout(t, sched, R, 0);
+}
+
+bool batch_rows_valid(int sched, int R) {
+    return sched == 4 ? (R == 4 || R == 8 || R == 16) : sched == 6 ? (R == 16 || R == 24 || R == 32) : false;
 }
 
 bool batch_same_class(const BatchPair& a, const BatchPair& b) {
@@ -149,33 +172,81 @@ void batch_group_by_class(const std::vector<BatchPair>& pairs, const std::vector
         std::stable_sort(g.pairs.begin(), g.pairs.end(), [&](int a, int b) {
             return pairs[a].W + 2 * pairs[a].H > pairs[b].W + 2 * pairs[b].H;
         });
-        for (int i : g.pairs) g.Wmax = std::max(g.Wmax, pairs[i].W);
+        for (int i : g.pairs) {
+            g.Wmax = std::max(g.Wmax, pairs[i].W);
+            g.Lmax = std::max(g.Lmax, std::max(pairs[i].W, pairs[i].H));
+        }
         groups.push_back(g);
     }
 }
 
 lumen_status batch_describe(const std::vector<BatchPair>& pairs, std::vector<BatchGroup>& groups,
-                            int R, int numSMs, std::vector<uint8_t>& host) {
+                            int sched, int R, int numSMs, std::vector<uint8_t>& host) {
     size_t dOff = 0;
     for (BatchGroup& g : groups) {
-        // a group of several pairs is throughput-bound: lane teams; a pair or
-        // two are bound by the wavefront's step latency: full-warp rows
-        const bool teams = g.pairs.size() >= 4;
-        cudaError_t e = wave_batch_plan(g.Wmax, g.Dp, R, g.wrap, g.full, g.diag, numSMs, &g.plan, teams);
-        if (e != cudaSuccess)
-            return bfail(LUMEN_ERR_INVALID_ARGUMENT,
-                         std::string("batch: no sweep configuration for a group: ") + cudaGetErrorString(e));
+        g.sched = sched;
         g.nTickets = 0;
-        for (int i : g.pairs) g.nTickets += 2 * pairs[i].nBands;
-        g.jobsOff = dOff;
-        dOff = align256(dOff + sizeof(WaveJob) * g.pairs.size());
+        if (sched == 6) {
+            // 4 paths: R is 16 (no hand-offs, the band height only groups rows)
+            const int Rg = g.diag ? R : 16;
+            cudaError_t e = pair_batch_plan(g.Lmax, g.Dp, g.wrap, g.full, g.diag, numSMs, &g.pplan, Rg);
+            if (e != cudaSuccess)
+                return bfail(LUMEN_ERR_INVALID_ARGUMENT,
+                             std::string("batch: no sweep configuration for a group: ") + cudaGetErrorString(e));
+            for (int i : g.pairs) {
+                if (pairs[i].R != Rg) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "batch: layout and plan disagree");
+                g.nTickets += 2 * pairs[i].nb0 + 2 * pairs[i].nb1;
+            }
+            g.jobsOff = dOff;
+            dOff = align256(dOff + sizeof(PairJob) * g.pairs.size());
+        } else {
+            // a group of several pairs is throughput-bound: lane teams; a pair or
+            // two are bound by the wavefront's step latency: full-warp rows
+            const bool teams = g.pairs.size() >= 4;
+            cudaError_t e = wave_batch_plan(g.Wmax, g.Dp, R, g.wrap, g.full, g.diag, numSMs, &g.plan, teams);
+            if (e != cudaSuccess)
+                return bfail(LUMEN_ERR_INVALID_ARGUMENT,
+                             std::string("batch: no sweep configuration for a group: ") + cudaGetErrorString(e));
+            for (int i : g.pairs) g.nTickets += 2 * pairs[i].nBands;
+            g.jobsOff = dOff;
+            dOff = align256(dOff + sizeof(WaveJob) * g.pairs.size());
+        }
         g.tableOff = dOff;
         dOff = align256(dOff + sizeof(uint32_t) * (size_t)g.nTickets + 4);  // + the ticket counter
     }
     host.assign(dOff, 0);
     for (BatchGroup& g : groups) {
-        WaveJob* jobs = reinterpret_cast<WaveJob*>(host.data() + g.jobsOff);
         uint32_t* table = reinterpret_cast<uint32_t*>(host.data() + g.tableOff);
+        if (sched == 6) {
+            PairJob* jobs = reinterpret_cast<PairJob*>(host.data() + g.jobsOff);
+            for (int j = 0; j < (int)g.pairs.size(); ++j) {
+                const BatchPair& q = pairs[g.pairs[j]];
+                PairView pv{reinterpret_cast<const uint8_t*>(q.base + q.oCost), q.left, nullptr};
+                uint16_t* const part[4] = {reinterpret_cast<uint16_t*>(q.base + q.oAgg),
+                                           reinterpret_cast<uint16_t*>(q.base + q.oPartB),
+                                           reinterpret_cast<uint16_t*>(q.base + q.oPartC),
+                                           reinterpret_cast<uint16_t*>(q.base + q.oPartD)};
+                jobs[j] = pair_job(pv, part, q.k, q.R,
+                                   q.diag ? reinterpret_cast<unsigned long long*>(q.base + q.oXbuf) : nullptr);
+            }
+            // band-major over the (pair, sweep) chains: every chain's band b comes
+            // one round after its band b-1, so a band waits only on an earlier
+            // ticket, and all chains start at once
+            int maxB = 0;
+            for (int i : g.pairs) maxB = std::max(maxB, std::max(pairs[i].nb0, pairs[i].nb1));
+            size_t n = 0;
+            for (int b = 0; b < maxB; ++b)
+                for (int j = 0; j < (int)g.pairs.size(); ++j) {
+                    const BatchPair& q = pairs[g.pairs[j]];
+                    for (int sw = 0; sw < 4; ++sw)
+                        if (b < (sw < 2 ? q.nb0 : q.nb1))
+                            table[n++] = (uint32_t)j << 20 | (uint32_t)sw << 18 | (uint32_t)b;
+                }
+            if ((int)n != g.nTickets) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "batch: ticket table size");
+            g.window = 0;
+            continue;
+        }
+        WaveJob* jobs = reinterpret_cast<WaveJob*>(host.data() + g.jobsOff);
         for (int j = 0; j < (int)g.pairs.size(); ++j) {
             const BatchPair& q = pairs[g.pairs[j]];
             PairView pv{reinterpret_cast<const uint8_t*>(q.base + q.oCost), q.left,
@@ -196,10 +267,15 @@ lumen_status batch_describe(const std::vector<BatchPair>& pairs, std::vector<Bat
 
 lumen_status batch_enqueue_costs(const std::vector<BatchPair>& pairs, const BatchGroup& g, const uint8_t* desc,
                                  const uint32_t* magic, cudaStream_t s, unsigned long long* launches) {
-    // counters of the group's pairs and the group's ticket
+    // schedule 4: the counters of the group's pairs; schedule 6: the row
+    // buffers (every word below the launch's epoch, 1); the group's ticket
     for (int i : g.pairs) {
         const BatchPair& q = pairs[i];
-        BCU(cudaMemsetAsync(q.base + q.oCtr, 0, ctr_bytes(q.nBands), s));
+        if (g.sched == 6) {
+            if (q.xbufBytes) BCU(cudaMemsetAsync(q.base + q.oXbuf, 0, q.xbufBytes, s));
+        } else {
+            BCU(cudaMemsetAsync(q.base + q.oCtr, 0, ctr_bytes(q.nBands), s));
+        }
     }
     unsigned* ticket = reinterpret_cast<unsigned*>(const_cast<uint8_t*>(desc) + g.tableOff +
                                                    sizeof(uint32_t) * (size_t)g.nTickets);
@@ -228,6 +304,13 @@ lumen_status batch_enqueue_wave(const BatchGroup& g, const uint8_t* desc, int* s
                                 cudaStream_t s, unsigned long long* launches) {
     unsigned* ticket = reinterpret_cast<unsigned*>(const_cast<uint8_t*>(desc) + g.tableOff +
                                                    sizeof(uint32_t) * (size_t)g.nTickets);
+    if (g.sched == 6) {
+        BCU(launch_aggregate_pair_batch(reinterpret_cast<const PairJob*>(desc + g.jobsOff),
+                                        reinterpret_cast<const uint32_t*>(desc + g.tableOff), g.nTickets, g.Lmax,
+                                        g.Dp, g.wrap, g.full, g.pplan, 1u, ticket, status, spinMax, s));
+        *launches += 1;
+        return LUMEN_OK;
+    }
     BCU(launch_aggregate_wave_batch(reinterpret_cast<const WaveJob*>(desc + g.jobsOff),
                                     reinterpret_cast<const uint32_t*>(desc + g.tableOff), g.nTickets, g.window,
                                     g.Wmax, g.Dp, g.wrap, g.full, g.diag, g.plan, ticket, status, spinMax, s));
@@ -241,8 +324,16 @@ lumen_status batch_enqueue_selects(const std::vector<BatchPair>& pairs, const Ba
         const BatchPair& q = pairs[i];
         int16_t* dl = reinterpret_cast<int16_t*>(q.base + q.oDispL);
         int16_t* dr = reinterpret_cast<int16_t*>(q.base + q.oDispR);
-        BCU(launch_select(reinterpret_cast<uint16_t*>(q.base + q.oAgg), reinterpret_cast<uint16_t*>(q.base + q.oPartB),
-                          q.wrap, q.W, q.H, q.D, q.Dp, q.p.minDisparity, q.p.uniquenessRatio, dl, dr, s));
+        uint16_t* agg = reinterpret_cast<uint16_t*>(q.base + q.oAgg);
+        uint16_t* pb = reinterpret_cast<uint16_t*>(q.base + q.oPartB);
+        uint16_t* pc = nullptr;
+        uint16_t* pd = nullptr;
+        if (g.sched == 6) {
+            pc = reinterpret_cast<uint16_t*>(q.base + q.oPartC);
+            pd = reinterpret_cast<uint16_t*>(q.base + q.oPartD);
+        }
+        BCU(launch_select(agg, pb, q.wrap, q.W, q.H, q.D, q.Dp, q.p.minDisparity, q.p.uniquenessRatio, dl, dr, s,
+                          pc, pd));
         const int lr = q.p.disp12MaxDiff >= 0 ? q.p.disp12MaxDiff * 16 : -1;
         const int spk = q.p.speckleWindowSize > 0 ? std::min(q.p.speckleWindowSize, 25) : 0;
         BCU(launch_post(dl, dr, q.W, q.H, lr, spk, q.p.speckleRange * 16, q.out, (size_t)q.W, nullptr, s));
@@ -290,7 +381,8 @@ struct lumen_sgbm_batch {
     std::vector<BatchPair> pairs;
     std::vector<BatchGroup> groups;
     bool planned = false;
-    int rows = 0;       // rows per band (0: 8)
+    int sched = 0;      // aggregation schedule: 4, 6 (0: 6)
+    int rows = 0;       // rows per band (0: the schedule's default)
     int useGraph = 0;
     size_t budget = 80ull << 30;
     int numSMs = 148;
@@ -338,7 +430,11 @@ static void batch_release(lumen_sgbm_batch* b) {
 // groups run one after the other in one region of budget bytes.
 static lumen_status batch_plan(lumen_sgbm_batch* b) {
     batch_release(b);
-    const int R = b->rows ? b->rows : 8;
+    const int sched = b->sched ? b->sched : 6;
+    const int R = b->rows ? b->rows : batch_default_rows(sched);
+    if (!batch_rows_valid(sched, R))
+        return bfail(LUMEN_ERR_INVALID_ARGUMENT, "batch: rows per band must be 4, 8 or 16 with schedule 4, "
+                                                 "16, 24 or 32 with schedule 6");
     std::vector<int> all(b->pairs.size());
     for (int i = 0; i < (int)all.size(); ++i) all[i] = i;
     std::vector<BatchGroup> classes;
@@ -364,7 +460,7 @@ static lumen_status batch_plan(lumen_sgbm_batch* b) {
                 bytes = 0;
             };
             for (int i : c.pairs) {
-                const size_t need = batch_pair_bytes(b->pairs[i], R);
+                const size_t need = batch_pair_bytes(b->pairs[i], sched, R);
                 if (need > cap) tooBig = true;
                 if (!g.pairs.empty() && bytes + need > cap) flush();
                 bytes += need;
@@ -398,7 +494,7 @@ static lumen_status batch_plan(lumen_sgbm_batch* b) {
     size_t poolNeed = 0;
     for (size_t gi = 0; gi < b->groups.size(); ++gi) {
         size_t o = b->overlap && gi % 2 ? even : 0;
-        for (int i : b->groups[gi].pairs) o = batch_pair_layout(b->pairs[i], R, o);
+        for (int i : b->groups[gi].pairs) o = batch_pair_layout(b->pairs[i], sched, R, o);
         poolNeed = std::max(poolNeed, o);
     }
     if (b->overlap) {
@@ -409,7 +505,7 @@ static lumen_status batch_plan(lumen_sgbm_batch* b) {
     b->poolBytes = poolNeed;
     for (BatchPair& q : b->pairs) q.base = static_cast<uint8_t*>(b->pool);
     std::vector<uint8_t> host;
-    lumen_status st = batch_describe(b->pairs, b->groups, R, b->numSMs, host);
+    lumen_status st = batch_describe(b->pairs, b->groups, sched, R, b->numSMs, host);
     if (st != LUMEN_OK) return st;
     BCU(cudaMalloc(&b->desc, std::max<size_t>(host.size(), 256)));
     b->descBytes = host.size();
@@ -523,8 +619,8 @@ extern "C" lumen_status lumen_sgbm_batch_clear(lumen_sgbm_batch* b) {
 extern "C" lumen_status lumen_sgbm_batch_set_options(lumen_sgbm_batch* b, int rows_per_band, int use_graph,
                                                      size_t device_budget_bytes) {
     if (!b) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "NULL batch");
-    if (rows_per_band != 0 && rows_per_band != 4 && rows_per_band != 8 && rows_per_band != 16)
-        return bfail(LUMEN_ERR_INVALID_ARGUMENT, "rows_per_band must be 0, 4, 8 or 16");
+    if (rows_per_band != 0 && !batch_rows_valid(4, rows_per_band) && !batch_rows_valid(6, rows_per_band))
+        return bfail(LUMEN_ERR_INVALID_ARGUMENT, "rows_per_band must be 0, 4, 8, 16, 24 or 32");
     cudaDeviceSynchronize();
     b->rows = rows_per_band;
     b->useGraph = use_graph ? 1 : 0;
@@ -585,12 +681,20 @@ extern "C" lumen_status lumen_sgbm_batch_autotune(lumen_sgbm_batch* b, void* str
         return bfail(LUMEN_ERR_CUDA, "batch autotune: event creation failed");
     }
     const int savedGraph = b->useGraph;
-    int bestR = 0;
+    int bestR = 0, bestS = 0;
     float bestMs = 0.f;
     lumen_status st = LUMEN_OK;
-    for (int R : {4, 8, 16}) {
+    // the schedule pinned by lumen_sgbm_batch_set_schedule, else both
+    std::vector<std::pair<int, int>> cands;
+    for (int sc : {6, 4})
+        if (!b->sched || b->sched == sc)
+            for (int R : (sc == 4 ? std::vector<int>{4, 8, 16} : std::vector<int>{16, 24, 32}))
+                cands.push_back({sc, R});
+    const int savedSched = b->sched;
+    for (auto [sc, R] : cands) {
         cudaStreamSynchronize(s);
         batch_release(b);
+        b->sched = sc;
         b->rows = R;
         b->useGraph = 0;
         st = lumen_sgbm_batch_run(b, stream);  // plans, warms up
@@ -606,6 +710,7 @@ extern "C" lumen_status lumen_sgbm_batch_autotune(lumen_sgbm_batch* b, void* str
         ms /= (float)repeats;
         if (!bestR || ms < bestMs) {
             bestR = R;
+            bestS = sc;
             bestMs = ms;
         }
     }
@@ -614,10 +719,32 @@ extern "C" lumen_status lumen_sgbm_batch_autotune(lumen_sgbm_batch* b, void* str
     cudaStreamSynchronize(s);
     batch_release(b);
     b->useGraph = savedGraph;
-    if (st != LUMEN_OK) return st;
-    b->rows = bestR;  // the next run plans (and captures) with it
+    if (st != LUMEN_OK) {
+        b->sched = savedSched;
+        return st;
+    }
+    b->sched = bestS;  // the next run plans (and captures) with them
+    b->rows = bestR;
     if (best_rows) *best_rows = bestR;
     if (best_ms) *best_ms = bestMs;
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_sgbm_batch_set_schedule(lumen_sgbm_batch* b, int schedule) {
+    if (!b) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "NULL batch");
+    if (schedule != 0 && schedule != 4 && schedule != 6)
+        return bfail(LUMEN_ERR_INVALID_ARGUMENT, "batch schedule must be 0 (automatic), 4 or 6");
+    cudaDeviceSynchronize();
+    b->sched = schedule;
+    batch_release(b);
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_sgbm_batch_config(const lumen_sgbm_batch* b, int* schedule, int* rows_per_band) {
+    if (!b) return bfail(LUMEN_ERR_INVALID_ARGUMENT, "NULL batch");
+    const int sc = b->sched ? b->sched : 6;
+    if (schedule) *schedule = sc;
+    if (rows_per_band) *rows_per_band = b->rows ? b->rows : batch_default_rows(sc);
     return LUMEN_OK;
 }
 

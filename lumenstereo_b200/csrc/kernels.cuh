@@ -102,13 +102,28 @@ int pair_lanes(int Dp);
 // cudaErrorInvalidValue: no instance for these disparities / sizes
 cudaError_t pair_plan(const SgmConsts& k, bool wrap, bool diag, int numSMs, PairPlan* plan, int R = 0,
                       int T = 0);
+// Plan of a batched launch of one kernel class: the pairs' longest sweep row
+// Lmax sizes the shared memory; nb0/nb1/nTickets/xbufBytes stay 0 (per pair);
+// grid is the resident CTA count (the launch takes at most its ticket count).
+cudaError_t pair_batch_plan(int Lmax, int Dp, bool wrap, bool full, bool diag, int numSMs, PairPlan* plan,
+                            int R = 0);
+// Row-buffer bytes of one 8-path pair (R rows per band).
+size_t pair_xbuf_bytes(int W, int H, int Dp, int R);
+struct PairJob;
+// One launch over the bands of many pairs of one class: d_jobs[pairs],
+// d_table[nTickets] (pair << 20 | sweep << 18 | band, every band after the
+// band before it in its own sweep); every row-buffer word of the pairs holds
+// an epoch below `epoch`.
+cudaError_t launch_aggregate_pair_batch(const PairJob* d_jobs, const uint32_t* d_table, int nTickets, int Lmax,
+                                        int Dp, bool wrap, bool full, const PairPlan& plan, unsigned epoch,
+                                        unsigned* ticket, int* status, long long spinMax, cudaStream_t s);
 // part[0..3]: the four sweeps' partial volumes (part[0] may be pv.agg).  xbuf:
 // the row buffers (plan.xbufBytes), every word of which holds an epoch below
 // `epoch` (zero-filled when allocated, then one epoch per launch, increasing).
 cudaError_t launch_aggregate_pair(const PairView& pv, uint16_t* const part[4], const SgmConsts& k, bool wrap,
                                   const PairPlan& plan, unsigned long long* xbuf, unsigned epoch,
                                   unsigned* counters, int* status, long long spinMax, cudaStream_t s,
-                                  int stallTest = 0);
+                                  int stallTest = 0, unsigned long long* trace = nullptr);
 
 // aggB (nullable): second partial volume summed with agg (mod 2^16 when wrap);
 // aggC, aggD (nullable, both or neither): two more (schedule 6).

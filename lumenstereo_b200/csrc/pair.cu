@@ -119,12 +119,37 @@ cudaError_t pair_plan(const SgmConsts& k, bool wrap, bool diag, int numSMs, Pair
     return cudaSuccess;
 }
 
-cudaError_t launch_aggregate_pair(const PairView& pv, uint16_t* const part[4], const SgmConsts& k, bool wrap,
-                                  const PairPlan& plan, unsigned long long* xbuf, unsigned epoch,
-                                  unsigned* counters, int* status, long long spinMax, cudaStream_t s,
-                                  int stallTest) {
-    PairArgs a{};
-    PairJob& J = a.job;
+cudaError_t pair_batch_plan(int Lmax, int Dp, bool wrap, bool full, bool diag, int numSMs, PairPlan* plan,
+                            int R) {
+    if (!pair_lanes(Dp)) return cudaErrorInvalidValue;
+    if (R == 0) R = 16;
+    const int T = pair_lanes(Dp);
+    if (!pair_instance(Dp, T, R, diag)) return cudaErrorInvalidValue;
+    PairPlan p{};
+    p.R = R;
+    p.T = T;
+    p.diag = diag;
+    p.smem = pair_smem(Lmax, Dp, R).total;
+    if (p.smem > 227 * 1024) return cudaErrorInvalidValue;
+    PairArgs dummy{};
+    int perSM = 0;
+    cudaError_t e = pair_dispatch(dummy, Dp, R, T, diag, wrap, full, p.smem, 0, nullptr, &perSM);
+    if (e != cudaSuccess) return e;
+    if (perSM < 1) return cudaErrorInvalidConfiguration;
+    p.grid = perSM * numSMs;
+    p.counterWords = 1;
+    *plan = p;
+    return cudaSuccess;
+}
+
+size_t pair_xbuf_bytes(int W, int H, int Dp, int R) {
+    const int nb0 = (H + R - 1) / R, nb1 = (W + R - 1) / R;
+    return pair_xbase(3, nb1, W, H, nb0, nb1) * (size_t)pair_ll_words(Dp) * 8;
+}
+
+PairJob pair_job(const PairView& pv, uint16_t* const part[4], const SgmConsts& k, int R,
+                 unsigned long long* xbuf) {
+    PairJob J{};
     J.cost = pv.cost;
     J.img = pv.img;
     for (int i = 0; i < 4; ++i) J.part[i] = part[i];
@@ -132,13 +157,41 @@ cudaError_t launch_aggregate_pair(const PairView& pv, uint16_t* const part[4], c
     J.W = k.W;
     J.H = k.H;
     J.D = k.D;
-    J.nb[0] = plan.nb0;
-    J.nb[1] = plan.nb1;
+    J.nb[0] = (k.H + R - 1) / R;
+    J.nb[1] = (k.W + R - 1) / R;
     J.P1 = k.P1;
     J.P2 = k.P2;
     J.costScale = k.costScale;
     J.p1x2 = k.p1x2;
     J.bsub = k.bsub;
+    return J;
+}
+
+cudaError_t launch_aggregate_pair_batch(const PairJob* d_jobs, const uint32_t* d_table, int nTickets, int Lmax,
+                                        int Dp, bool wrap, bool full, const PairPlan& plan, unsigned epoch,
+                                        unsigned* ticket, int* status, long long spinMax, cudaStream_t s) {
+    PairArgs a{};
+    a.jobs = d_jobs;
+    a.table = d_table;
+    a.nTickets = nTickets;
+    a.Lmax = Lmax;
+    a.ticket = ticket;
+    a.status = status;
+    a.spinMax = spinMax;
+    a.epoch = epoch;
+    cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    int perSM = 0;
+    return pair_dispatch(a, Dp, plan.R, plan.T, plan.diag, wrap, full, plan.smem, std::min(plan.grid, nTickets), s,
+                         &perSM);
+}
+
+cudaError_t launch_aggregate_pair(const PairView& pv, uint16_t* const part[4], const SgmConsts& k, bool wrap,
+                                  const PairPlan& plan, unsigned long long* xbuf, unsigned epoch,
+                                  unsigned* counters, int* status, long long spinMax, cudaStream_t s,
+                                  int stallTest, unsigned long long* trace) {
+    PairArgs a{};
+    a.job = pair_job(pv, part, k, plan.R, xbuf);
     a.nTickets = plan.nTickets;
     a.Lmax = std::max(k.W, k.H);
     a.ticket = counters;
@@ -146,6 +199,7 @@ cudaError_t launch_aggregate_pair(const PairView& pv, uint16_t* const part[4], c
     a.spinMax = spinMax;
     a.epoch = epoch;
     a.stallTest = stallTest;
+    a.trace = trace;
     cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned) * plan.counterWords, s);
     if (e != cudaSuccess) return e;
     int perSM = 0;

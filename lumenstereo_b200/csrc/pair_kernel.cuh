@@ -41,7 +41,10 @@
 //  * matching costs are prefetched kPPF-1 pixels ahead with cp.async;
 //    adaptive P2 is looked up from staged image rows;
 //  * bands are handed out by a ticket counter, the four sweeps interleaved,
-//    each sweep's bands in order.
+//    each sweep's bands in order.  A batched launch (PairArgs::jobs) takes
+//    its tickets from a table over the bands of many pairs of one kernel
+//    class; a CTA copies each band's pair descriptor into shared memory and
+//    rebuilds the P2 table and lane masks when the pair changes.
 // Every wait is bounded: on timeout the CTA records LUMEN_ERR_TIMEOUT in
 // *status and stops; CTAs that see a non-zero status stop taking bands.
 #pragma once
@@ -62,16 +65,39 @@ struct PairJob {
     uint32_t p1x2, bsub;
 };
 
+// Descriptor of one pair (host side, pair.cu): its volumes, row buffers
+// (8 paths), sizes, bands for R rows per band, and parameters.
+PairJob pair_job(const PairView& pv, uint16_t* const part[4], const SgmConsts& k, int R,
+                 unsigned long long* xbuf);
+
+// A launch: one pair (`job`, tickets through pair_ticket) or a batch of pairs
+// of one kernel class (`jobs`, tickets through `table`, each entry
+// pair << 20 | sweep << 18 | band, every band listed after the band before it
+// in its own sweep).
 struct PairArgs {
-    PairJob job;
-    int nTickets;                  // 2 * nb[0] + 2 * nb[1]
-    int Lmax;                      // max(W, H): staged image row length
+    PairJob job;                   // the pair when jobs == nullptr
+    const PairJob* jobs;           // batch: [pairs]
+    const uint32_t* table;         // batch: [nTickets]
+    int nTickets;                  // one pair: 2 * nb[0] + 2 * nb[1]
+    int Lmax;                      // max(W, H) over the launch's pairs: staged image row length
     unsigned* ticket;
     int* status;
     long long spinMax;
     unsigned epoch;                // high half of every row-buffer word this launch writes
     int stallTest;                 // 1: ticket 4 (band 1 of sweep 0) waits for an epoch never written
+    unsigned long long* trace;     // optional band timeline, [nTickets][4] (pair_trace_record)
 };
+
+// Band timeline record (lumen_sgbm_debug_trace) of schedule 6, per ticket:
+// [0] globaltimer ns when the band's rows start their first pixel, [1] when
+// they have finished pixel len/2, [2] when they have finished the row, [3] the
+// SM id << 32 | the sweep << 16 | 1.  Consecutive bands' [1] give the
+// hand-off lag; ([2] - [0]) / len the time of one step.
+__device__ __forceinline__ unsigned long long pair_now() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    return t;
+}
 
 // 64-bit (payload, epoch) words of the row buffers: volatile accesses reach
 // the GPU-wide L2 and each 64-bit element is single-copy atomic, so a reader
@@ -129,17 +155,13 @@ __device__ __forceinline__ void pair_body(const PairArgs& a) {
     const int tl = lane & (T - 1);      // lane within the row's team
     const int off = tl * 2 * KW;        // first disparity of this lane
     const int r = warp * RPW + lane / T;
-    const PairJob& J = a.job;
-    const int W = J.W, H = J.H;
 
     for (int i = threadIdx.x; i < SB / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(sm + L.zero)[i] = 0u;
-    // adaptive P2 (src/sgbm_kernels.cu:301-310) as a table of |dI|, replicated in both halves
-    for (int g = threadIdx.x; g < 256; g += blockDim.x)
-        reinterpret_cast<uint32_t*>(sm + L.lut)[g] =
-            ((uint32_t)max(J.P1 + 1, J.P2 * 8 / max(8, g)) & 0xFFFFu) * 0x10001u;
     LaneMasks<KW> mk;
-    make_lane_masks<KW>(tl, J.D, mk);
-    __syncthreads();
+    int curJob = -1;   // the pair whose P2 table and lane masks are set up
+    // the band's pair, copied from the launch's parameters or job table
+    PairJob* const sJob = reinterpret_cast<PairJob*>(sm + L.job);
+    static_assert(sizeof(PairJob) <= kPairJobBytes, "pair descriptor slot");
 
     for (;;) {
         if (threadIdx.x == 0) {
@@ -147,13 +169,39 @@ __device__ __forceinline__ void pair_body(const PairArgs& a) {
             if (*(volatile int*)a.status != 0) t = a.nTickets;
             sflag[0] = t;
             sflag[1] = 0;
+            if (t < a.nTickets) {
+                int s, b, jb = 0;
+                if (a.jobs) {
+                    const uint32_t e = a.table[t];
+                    jb = (int)(e >> 20);
+                    s = (int)(e >> 18) & 3;
+                    b = (int)(e & 0x3FFFFu);
+                    *sJob = a.jobs[jb];
+                } else {
+                    pair_ticket(t, a.job.nb[0], a.job.nb[1], s, b);
+                    if (curJob < 0) *sJob = a.job;
+                }
+                sflag[2] = s;
+                sflag[3] = b;
+                sflag[4] = jb;
+            }
         }
         if (threadIdx.x < 2) sctr[threadIdx.x] = 0u;
         __syncthreads();
         const int t = sflag[0];
         if (t >= a.nTickets) break;
-        int s, b;
-        pair_ticket(t, J.nb[0], J.nb[1], s, b);
+        const int s = sflag[2], b = sflag[3], jb = sflag[4];
+        const PairJob& J = *sJob;
+        const int W = J.W, H = J.H;
+        if (jb != curJob) {
+            // adaptive P2 (src/sgbm_kernels.cu:301-310) as a table of |dI|, replicated
+            // in both halves (read after the staging barrier below)
+            for (int g = threadIdx.x; g < 256; g += blockDim.x)
+                reinterpret_cast<uint32_t*>(sm + L.lut)[g] =
+                    ((uint32_t)max(J.P1 + 1, J.P2 * 8 / max(8, g)) & 0xFFFFu) * 0x10001u;
+            make_lane_masks<KW>(tl, J.D, mk);
+            curJob = jb;
+        }
         const bool tr = s >= 2;
         const int Ws = tr ? H : W, Hs = tr ? W : H;
         const int nbS = tr ? J.nb[1] : J.nb[0];
@@ -198,6 +246,10 @@ __device__ __forceinline__ void pair_body(const PairArgs& a) {
             unsigned long long* xo =
                 exporter ? J.xbuf + pair_xbase(s, b, W, H, J.nb[0], J.nb[1]) * NL + tl * KW : nullptr;
             const unsigned long long ep = (unsigned long long)a.epoch << 32;
+            // the pair's fields the steps use, in registers
+            const uint8_t* const costBase = J.cost;
+            const int costScale = J.costScale;
+            const uint32_t p1x2 = J.p1x2, bsub = J.bsub;
 
             if constexpr (!DIAG) {
                 // one path a sweep, rows independent: costs arrive in batches of
@@ -213,7 +265,7 @@ __device__ __forceinline__ void pair_body(const PairArgs& a) {
                     for (int k = 0; k < 4; ++k) {
                         const int p = 4 * q + k;
                         if (rowOn && p < Ws) {
-                            const uint8_t* src = J.cost + (qofs + k * qstep);
+                            const uint8_t* src = costBase + (qofs + k * qstep);
                             const uint32_t dst = w_smem_addr(costRing + (p % kPPF) * DP + off);
                             if constexpr ((2 * KW) % 16 == 0) {
 #pragma unroll
@@ -234,9 +286,9 @@ __device__ __forceinline__ void pair_body(const PairArgs& a) {
                 uint32_t p2h;
                 auto load_operands = [&](int u) {
                     load_cost_words<KW>(costRing + (u % kPPF) * DP + off, Cw);
-                    if (WRAP || J.costScale != 1) {
+                    if (WRAP || costScale != 1) {
 #pragma unroll
-                        for (int w = 0; w < KW; ++w) Cw[w] = scale_cost<WRAP>(Cw[w], J.costScale);
+                        for (int w = 0; w < KW; ++w) Cw[w] = scale_cost<WRAP>(Cw[w], costScale);
                     }
                     p2h = p2lut[abs(irow[u] - irow[max(u - 1, 0)])];
                 };
@@ -250,7 +302,7 @@ __device__ __forceinline__ void pair_body(const PairArgs& a) {
                 uint32_t minH = 0;
                 for (int u = 0; u < Ws; ++u) {
                     uint32_t LnH[KW];
-                    wave_step<KW, T, WRAP, FULL>(LH, Cw, minH, p2h, J.p1x2, J.bsub, mk, LnH);
+                    wave_step<KW, T, WRAP, FULL>(LH, Cw, minH, p2h, p1x2, bsub, mk, LnH);
                     if (u + 1 < Ws) {
                         if ((u & 3) == 3) {
                             prefetch_batch((u >> 2) + 2);   // into the slots of pixels u-3 .. u, all read
@@ -278,7 +330,7 @@ __device__ __forceinline__ void pair_body(const PairArgs& a) {
                 const ptrdiff_t o = cofs;
                 cofs += cstep;
                 if (rowOn && p >= 0 && p < Ws) {
-                    const uint8_t* src = J.cost + o;
+                    const uint8_t* src = costBase + o;
                     const uint32_t dst = w_smem_addr(costRing + (p % kPPF) * DP + off);
                     if constexpr ((2 * KW) % 16 == 0) {
 #pragma unroll
@@ -300,6 +352,8 @@ __device__ __forceinline__ void pair_body(const PairArgs& a) {
             for (int w = 0; w < KW; ++w) LH[w] = 0;
             uint32_t minH = 0;
             unsigned impSeen = 0;
+            unsigned long long* const trec = (a.trace && threadIdx.x == 0) ? a.trace + 4 * (size_t)t : nullptr;
+            if (trec) trec[0] = pair_now();
             for (int u = 0; u < Ws; ++u) {
                 // ---- the band above's pixel u-1 must be in the import ring (warp 0 holds row 0) ----
                 if (warp == 0 && hasPrev && u >= 1 && ok)
@@ -309,9 +363,9 @@ __device__ __forceinline__ void pair_body(const PairArgs& a) {
                 w_cp_wait<kPPF - 1>();
                 uint32_t Cw[KW];
                 load_cost_words<KW>(costRing + (u % kPPF) * DP + off, Cw);
-                if (WRAP || J.costScale != 1) {
+                if (WRAP || costScale != 1) {
 #pragma unroll
-                    for (int w = 0; w < KW; ++w) Cw[w] = scale_cost<WRAP>(Cw[w], J.costScale);
+                    for (int w = 0; w < KW; ++w) Cw[w] = scale_cost<WRAP>(Cw[w], costScale);
                 }
                 // ---- adaptive P2: horizontal predecessor (u-1, v), diagonal (u-1, v-1) ----
                 const int um = max(u - 1, 0);
@@ -319,7 +373,7 @@ __device__ __forceinline__ void pair_body(const PairArgs& a) {
                 const uint32_t p2h = p2lut[abs(cur - irow[um])];
                 // ---- horizontal path (its state starts at 0: L = C at u = 0) ----
                 uint32_t LnH[KW];
-                wave_step<KW, T, WRAP, FULL>(LH, Cw, minH, p2h, J.p1x2, J.bsub, mk, LnH);
+                wave_step<KW, T, WRAP, FULL>(LH, Cw, minH, p2h, p1x2, bsub, mk, LnH);
                 const uint32_t p2d = p2lut[abs(cur - iprev[um])];
                 // ---- diagonal path from the row above, pixel u-1 ----
                 const uint8_t* slot = (u == 0 || v == 0) ? zeroSlot
@@ -329,7 +383,7 @@ __device__ __forceinline__ void pair_body(const PairArgs& a) {
                 load_words<KW>(reinterpret_cast<const uint16_t*>(slot) + off, Lp);
                 const uint32_t mp = *reinterpret_cast<const uint32_t*>(slot + 2 * DP);
                 uint32_t LnD[KW];
-                wave_step<KW, T, WRAP, FULL>(Lp, Cw, mp, p2d, J.p1x2, J.bsub, mk, LnD);
+                wave_step<KW, T, WRAP, FULL>(Lp, Cw, mp, p2d, p1x2, bsub, mk, LnD);
                 minH = wave_min_t<KW, T>(LnH);
                 const uint32_t minD = wave_min_t<KW, T>(LnD);
                 uint32_t S[KW];
@@ -361,6 +415,13 @@ __device__ __forceinline__ void pair_body(const PairArgs& a) {
                     break;
                 }
                 if (threadIdx.x == 0 && hasPrev) w_st_release_cta(&sctr[1], (unsigned)u);
+                if (trec && u == Ws / 2) trec[1] = pair_now();
+            }
+            if (trec) {
+                unsigned smid;
+                asm volatile("mov.u32 %0, %%smid;\n" : "=r"(smid));
+                trec[2] = pair_now();
+                trec[3] = (unsigned long long)smid << 32 | (unsigned)s << 16 | 1u;
             }
             w_cp_wait<0>();
             }
@@ -460,8 +521,16 @@ __device__ __forceinline__ void pair_body(const PairArgs& a) {
 }
 
 // Eight paths: R/(32/T) row warps and the import warp.
+// Register budget: 16-row bands of 8-lane rows are held to three CTAs an SM
+// (their shared memory at 1080p allows three) and 24-row bands to two; the
+// 16-lane instances keep the compiler's own choice (0), except the widest
+// (320 disparities), which is held to one CTA an SM.
+template <int KW, int R, int T>
+constexpr int pair_min_blocks() {
+    return T == 8 ? (R == 16 ? 3 : R == 24 ? 2 : 0) : (KW == 10 ? 1 : 0);
+}
 template <int KW, bool WRAP, bool FULL, int R, int T>
-__global__ void __launch_bounds__((R / (32 / T) + 1) * 32) pair_kernel(PairArgs a) {
+__global__ void __launch_bounds__((R / (32 / T) + 1) * 32, pair_min_blocks<KW, R, T>()) pair_kernel(PairArgs a) {
     pair_body<KW, WRAP, FULL, R, T, true>(a);
 }
 

@@ -29,8 +29,9 @@ LUMEN_PAIR_HD constexpr int pair_slot_bytes(int Dp) { return 2 * Dp + 16; }
 LUMEN_PAIR_HD constexpr int pair_ll_words(int Dp) { return Dp / 2 + 2; }
 
 struct PairSmem {
-    int img, cost, slots, imp, zero, lut, misc, total, Lp;
+    int img, cost, slots, imp, zero, lut, job, misc, total, Lp;
 };
+constexpr int kPairJobBytes = 128;   // the band's pair descriptor (PairJob) in shared memory
 LUMEN_PAIR_HD PairSmem pair_smem(int Lmax, int Dp, int R) {
     PairSmem s;
     s.Lp = (Lmax + 15) & ~15;
@@ -49,6 +50,8 @@ LUMEN_PAIR_HD PairSmem pair_smem(int Lmax, int Dp, int R) {
     o += SB;
     s.lut = o;
     o += 256 * 4;
+    s.job = o;
+    o += kPairJobBytes;
     s.misc = o;
     o += 32 * 4;
     s.total = o;

@@ -168,9 +168,9 @@ lumen_status sfail(lumen_status s, const std::string& m) { return set_error(s, m
 
 // Bytes of a request's slice: images (raw copies too when rectified), the
 // output map, then the working buffers of the batched launch core.
-size_t request_bytes(const BatchPair& q, int calib, int R) {
+size_t request_bytes(const BatchPair& q, int calib, int sched, int R) {
     const size_t img = image_bytes(q.W, q.H);
-    return 2 * img + (calib >= 0 ? 2 * img : 0) + align256((size_t)q.W * q.H * 2) + batch_pair_bytes(q, R);
+    return 2 * img + (calib >= 0 ? 2 * img : 0) + align256((size_t)q.W * q.H * 2) + batch_pair_bytes(q, sched, R);
 }
 
 void complete(lumen_server* S, Request* r, lumen_status st, const std::string& err) {
@@ -276,14 +276,14 @@ lumen_status slot_launch(lumen_server* S, Slot& sl, std::vector<Request*>& adm) 
         if (ps != LUMEN_OK) return ps;
         q.base = S->arenaBase + r->off;
         size_t o = b.used;
-        batch_pair_layout(q, R, o);
+        batch_pair_layout(q, S->opt.schedule, R, o);
         sl.pairs.push_back(q);
     }
     std::vector<int> idx(sl.pairs.size());
     for (int i = 0; i < (int)idx.size(); ++i) idx[i] = i;
     batch_group_by_class(sl.pairs, idx, sl.groups);
     std::vector<uint8_t> host;
-    lumen_status ds = batch_describe(sl.pairs, sl.groups, R, S->numSMs, host);
+    lumen_status ds = batch_describe(sl.pairs, sl.groups, S->opt.schedule, R, S->numSMs, host);
     if (ds != LUMEN_OK) return ds;
     if (host.size() > sl.descCap) {
         if (sl.dDesc) cudaFree(sl.dDesc);
@@ -509,11 +509,12 @@ extern "C" void lumen_server_options_default(lumen_server_options* o) {
     *o = lumen_server_options{};
     o->device_budget_bytes = 40ull << 30;
     o->max_batch_pairs = 32;
-    o->rows_per_band = 8;
+    o->rows_per_band = 16;
     o->max_inflight = 2;
     o->watchdog_ms = 60000;
     o->spin_limit = 0;
     o->plain_fallback = 1;
+    o->schedule = 6;
 }
 
 extern "C" lumen_status lumen_server_create(const lumen_server_options* opt, lumen_server** out) {
@@ -525,8 +526,10 @@ extern "C" lumen_status lumen_server_create(const lumen_server_options* opt, lum
     if (o.device_budget_bytes < (1u << 20)) return sfail(LUMEN_ERR_INVALID_ARGUMENT, "budget below 1 MiB");
     if (o.max_batch_pairs < 1 || o.max_batch_pairs > 4095)
         return sfail(LUMEN_ERR_INVALID_ARGUMENT, "max_batch_pairs must be in [1, 4095]");
-    if (o.rows_per_band != 4 && o.rows_per_band != 8 && o.rows_per_band != 16)
-        return sfail(LUMEN_ERR_INVALID_ARGUMENT, "rows_per_band must be 4, 8 or 16");
+    if (o.schedule != 4 && o.schedule != 6) return sfail(LUMEN_ERR_INVALID_ARGUMENT, "schedule must be 4 or 6");
+    if (!batch_rows_valid(o.schedule, o.rows_per_band))
+        return sfail(LUMEN_ERR_INVALID_ARGUMENT,
+                     "rows_per_band must be 4, 8 or 16 with schedule 4, 16, 24 or 32 with schedule 6");
     if (o.max_inflight < 1 || o.max_inflight > 8) return sfail(LUMEN_ERR_INVALID_ARGUMENT, "max_inflight must be in [1, 8]");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -698,7 +701,7 @@ extern "C" lumen_status lumen_server_submit(lumen_server* S, const lumen_stereo_
     r->calib = calib_id;
     r->W = width;
     r->H = height;
-    r->need = request_bytes(q, calib_id, S->opt.rows_per_band);
+    r->need = request_bytes(q, calib_id, S->opt.schedule, S->opt.rows_per_band);
     if (r->need > S->opt.device_budget_bytes) {
         delete r;
         std::lock_guard<std::mutex> g(S->mu);

@@ -40,10 +40,13 @@
 // Every wait is bounded: on timeout the CTA records LUMEN_ERR_TIMEOUT in
 // *status and stops; CTAs that see a non-zero status stop taking bands.
 //
-// Recurrence (src/sgbm_kernels.cu:338-360): packed uint16x2 minima
-// (__vminu2, full rate on sm_100; the three-input DPX forms issue at a
-// quarter of it), L = m + C - minL' as one IADD3 in the no-wrap mode; the warp
-// minimum comes back from redux.sync already replicated in both halves.
+// Recurrence (src/sgbm_kernels.cu:338-360): packed uint16x2 words.  The
+// no-wrap mode takes one three-input minimum and one add-minimum (the DPX
+// forms __vimin3_u16x2, __viaddmin_u16x2; measured at half the issue rate of
+// __vminu2 on B200, lumen_debug_op_rates) and L = m + C - minL' as one IADD3;
+// the wrap mode keeps per-halfword modular adds and two-input minima.  A
+// lane's words are reduced with three-input minima; the warp minimum comes
+// back from redux.sync (full-warp rows) or an xor butterfly (lane teams).
 #pragma once
 #include <algorithm>
 
@@ -259,15 +262,19 @@ __device__ __forceinline__ void wave_step(const uint32_t (&Lp)[KW], const uint32
         for (int j = 0; j <= KW; ++j) nb[j] = (nb[j] & ~mk.nbMask[j]) | (bsub & mk.nbMask[j]);
     }
     if (!WRAP) {
-        // every valid halfword stays in [0, 65535] (host-proved), so plain 32-bit
-        // adds never carry across halves there; padded halves (d >= D) are
-        // overwritten with 0xFFFF below and carries only move into other padded
-        // halves.
-        const uint32_t mp2 = mpx2 + p2x2;
+        // every valid halfword stays in [0, 65535] (host-proved), so no sum
+        // below wraps there.  With P2adj > P1 (the P2 table's floor is P1+1),
+        //   min(L', L'[d-1]+P1, L'[d+1]+P1, minL'+P2adj)
+        //     = min(min(L'[d-1], L'[d+1], minL'+P2adj-P1) + P1, L')
+        // i.e. one three-input minimum and one add-minimum (DPX), then
+        // L = m + C - minL' as one IADD3 (m >= minL', no borrow).  Padded halves
+        // (d >= D) are overwritten with 0xFFFF below; their garbage borrows only
+        // into other padded halves.
+        const uint32_t mpp = mpx2 + p2x2 - p1x2;
 #pragma unroll
         for (int i = 0; i < KW; ++i) {
-            const uint32_t t = __vminu2(nb[i], nb[i + 1]) + p1x2;
-            const uint32_t m = __vminu2(__vminu2(t, Lp[i]), mp2);
+            const uint32_t t = __vimin3_u16x2(nb[i], nb[i + 1], mpp);
+            const uint32_t m = __viaddmin_u16x2(t, p1x2, Lp[i]);
             uint32_t l = m + Cw[i] - mpx2;
             if (!FULL) l |= mk.padMask[i];
             Ln[i] = l;
@@ -300,20 +307,41 @@ __device__ __forceinline__ uint32_t wave_min(const uint32_t (&L)[KW], unsigned g
     return __reduce_min_sync(gmask, m);
 }
 
+// min over a lane's KW words (per half): three-input minima (DPX) in a
+// ternary tree
+template <int KW>
+__device__ __forceinline__ uint32_t wave_lane_min(const uint32_t (&L)[KW]) {
+    uint32_t a[KW];
+#pragma unroll
+    for (int i = 0; i < KW; ++i) a[i] = L[i];
+    int n = KW;
+#pragma unroll
+    for (int it = 0; it < 4; ++it) {
+        if (n > 1) {
+            int k = 0;
+#pragma unroll
+            for (int i = 0; i < KW; i += 3) {
+                if (i < n) {
+                    if (i + 2 < n) a[k] = __vimin3_u16x2(a[i], a[i + 1], a[i + 2]);
+                    else if (i + 1 < n) a[k] = __vminu2(a[i], a[i + 1]);
+                    else a[k] = a[i];
+                    ++k;
+                }
+            }
+            n = k;
+        }
+    }
+    return a[0];
+}
+
 // min over a team of T lanes' disparities, replicated in both halves
 template <int KW, int T>
 __device__ __forceinline__ uint32_t wave_min_t(const uint32_t (&L)[KW]) {
     if constexpr (T == 32) {
         return wave_min<KW>(L, kFullMask);
     } else {
-        uint32_t a[KW];
-#pragma unroll
-        for (int i = 0; i < KW; ++i) a[i] = L[i];
-#pragma unroll
-        for (int s = 1; s < KW; s *= 2)
-#pragma unroll
-            for (int i = 0; i + s < KW; i += 2 * s) a[i] = __vminu2(a[i], a[i + s]);
-        uint32_t m = __vminu2(a[0], __byte_perm(a[0], a[0], 0x1032));
+        uint32_t m = wave_lane_min<KW>(L);
+        m = __vminu2(m, __byte_perm(m, m, 0x1032));
 #pragma unroll
         for (int o = T / 2; o > 0; o >>= 1) m = __vminu2(m, __shfl_xor_sync(kFullMask, m, o));
         return m;

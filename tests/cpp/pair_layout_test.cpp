@@ -104,7 +104,8 @@ int main() {
                 CHECK(m.Lp >= L && m.Lp % 16 == 0);
                 CHECK(m.cost % 128 == 0 && m.cost >= (RR + 1) * L);
                 CHECK(m.slots % 16 == 0 && m.imp % 16 == 0 && m.zero % 16 == 0 && m.lut % 4 == 0 &&
-                      m.misc % 4 == 0);
+                      m.job % 16 == 0 && m.misc % 4 == 0);
+                CHECK(m.misc - m.job == kPairJobBytes);
                 CHECK(m.imp - m.slots == RR * 2 * pair_slot_bytes(Dp));
                 CHECK(m.zero - m.imp == kPQ * pair_slot_bytes(Dp));
                 CHECK(pair_slot_bytes(Dp) % 16 == 0);

@@ -43,13 +43,15 @@ def _plain(torch, pairs):
     return refs
 
 
-@pytest.mark.parametrize("rows,graph,budget", [(0, False, 0), (4, False, 0), (16, True, 0), (8, True, 24 << 20)])
-def test_batch_matches_plain_calls(rows, graph, budget):
+@pytest.mark.parametrize("schedule,rows,graph,budget", [
+    (0, 0, False, 0), (6, 24, True, 0), (6, 32, False, 0), (6, 16, True, 48 << 20),
+    (4, 4, False, 0), (4, 16, True, 0), (4, 8, True, 24 << 20)])
+def test_batch_matches_plain_calls(schedule, rows, graph, budget):
     torch = pytest.importorskip("torch")
     pairs = _pairs(torch)
     refs = _plain(torch, pairs)
     outs = [torch.full((h, w), 0x7ABC, dtype=torch.int16, device="cuda") for _, _, _, w, h in pairs]
-    with StereoBatch(rows_per_band=rows, use_graph=graph, budget_bytes=budget) as b:
+    with StereoBatch(rows_per_band=rows, use_graph=graph, budget_bytes=budget, schedule=schedule) as b:
         for (p, dl, dr, w, h), o in zip(pairs, outs):
             b.add(p, dl.data_ptr(), dr.data_ptr(), w, h, o.data_ptr())
         for rep in range(2):  # the second run replays (graph) or reuses the plan
@@ -61,25 +63,28 @@ def test_batch_matches_plain_calls(rows, graph, budget):
                 assert np.array_equal(o.cpu().numpy(), ref), (i, rep)
         info = b.info()
         if budget:
-            assert info["groups"] > 4, info  # the 24 MiB budget splits the larger classes
+            assert info["groups"] > 4, info  # the small budget splits the larger classes
+        assert b.config() == (schedule or 6, rows or (8 if schedule == 4 else 16))
         assert info["launches"] > 0
 
 
-@pytest.mark.parametrize("rows", [4, 8])
-def test_batch_many_wide_pairs(rows):
-    """24 pairs of one class, 2048 px wide and tall enough (160 rows) that a
-    band can only finish while the bands several ring lengths below it run:
-    the tickets exceed the resident CTAs, so the batch is cut into chunks
-    whose hand-off window fits them.  Exact against the plain call."""
+@pytest.mark.parametrize("schedule,rows,paths", [(4, 4, 4), (4, 8, 4), (6, 16, 8), (6, 24, 8), (6, 16, 4)])
+def test_batch_many_wide_pairs(schedule, rows, paths):
+    """24 pairs of one class, 2048 px wide and 160 rows tall: the tickets
+    exceed the resident CTAs many times over.  Schedule 4: a band can only
+    finish while the bands several ring lengths below it run, so the batch is
+    cut into chunks whose hand-off window fits them.  Schedule 6: CTAs take
+    band after band, of different pairs and sweeps, each waiting only on the
+    band above it in its own sweep.  Exact against the plain call."""
     torch = pytest.importorskip("torch")
     pairs = []
     for i in range(24):
         left, right, _ = synth.make_pair(synth.PairSpec(2048, 160, 4, 1, 40, 2.0, 500 + i))
-        p = StereoParams(maxDisparity=64, numDirections=4, speckleWindowSize=0, P2=400 + 100 * (i % 5))
+        p = StereoParams(maxDisparity=64, numDirections=paths, speckleWindowSize=0, P2=400 + 100 * (i % 5))
         pairs.append((p, torch.from_numpy(left).cuda(), torch.from_numpy(right).cuda(), 2048, 160))
     refs = _plain(torch, pairs)
     outs = [torch.full((h, w), 0x7ABC, dtype=torch.int16, device="cuda") for _, _, _, w, h in pairs]
-    with StereoBatch(rows_per_band=rows, use_graph=True) as b:
+    with StereoBatch(rows_per_band=rows, use_graph=True, schedule=schedule) as b:
         for (p, dl, dr, w, h), o in zip(pairs, outs):
             b.add(p, dl.data_ptr(), dr.data_ptr(), w, h, o.data_ptr())
         b.run()
@@ -100,7 +105,9 @@ def test_batch_autotune_keeps_outputs():
         for (p, dl, dr, w, h), o in zip(pairs, outs):
             b.add(p, dl.data_ptr(), dr.data_ptr(), w, h, o.data_ptr())
         rows, ms = b.autotune()
-        assert rows in (4, 8, 16) and ms > 0
+        sched, r2 = b.config()
+        assert r2 == rows and ms > 0
+        assert (sched, rows) in [(4, 4), (4, 8), (4, 16), (6, 16), (6, 24), (6, 32)]
         for o in outs:
             o.fill_(0)
         b.run()
@@ -109,8 +116,8 @@ def test_batch_autotune_keeps_outputs():
         assert np.array_equal(o.cpu().numpy(), ref)
 
 
-@pytest.mark.parametrize("rows", [8, 16])
-def test_batch_lane_team_classes(rows):
+@pytest.mark.parametrize("schedule,rows", [(4, 8), (4, 16), (6, 16), (6, 24)])
+def test_batch_lane_team_classes(schedule, rows):
     """Groups of four or more pairs run with narrow lane teams per row (8
     lanes for 64/128 padded disparities, 16 for 192-320): every class of them
     (both path sets, uint16 wrap, partial padding, odd sizes) against the
@@ -132,7 +139,7 @@ def test_batch_lane_team_classes(rows):
             pairs.append((p, torch.from_numpy(left).cuda(), torch.from_numpy(right).cuda(), w, h))
     refs = _plain(torch, pairs)
     outs = [torch.full((h, w), 0x7ABC, dtype=torch.int16, device="cuda") for _, _, _, w, h in pairs]
-    with StereoBatch(rows_per_band=rows, use_graph=True) as b:
+    with StereoBatch(rows_per_band=rows, use_graph=True, schedule=schedule) as b:
         for (p, dl, dr, w, h), o in zip(pairs, outs):
             b.add(p, dl.data_ptr(), dr.data_ptr(), w, h, o.data_ptr())
         b.run()

@@ -80,9 +80,9 @@ def test_budget_admission_and_rejections_keep_serving():
     reqs = _requests()[:4]
     refs = _plain(reqs)
     # a budget that holds about one 200x120 D128 request at a time
-    with StereoServer(budget_bytes=24 << 20, max_batch_pairs=8, max_inflight=3) as srv:
+    with StereoServer(budget_bytes=48 << 20, max_batch_pairs=8, max_inflight=3) as srv:
         _register(srv)
-        with pytest.raises(OutOfBudgetException):  # 640x480 D256 cannot fit 24 MiB
+        with pytest.raises(OutOfBudgetException):  # 640x480 D256 cannot fit 48 MiB
             srv.submit(StereoParams(maxDisparity=256), np.zeros((480, 640), np.uint8), np.zeros((480, 640), np.uint8))
         with pytest.raises(StereoException):  # invalid disparity range
             srv.submit(StereoParams(minDisparity=10, maxDisparity=5), reqs[0][1], reqs[0][2])
@@ -94,7 +94,7 @@ def test_budget_admission_and_rejections_keep_serving():
     for k, out in enumerate(outs):
         assert np.array_equal(out, refs[k % len(refs)]), k
     assert st["rejected"] == 3 and st["completed"] == len(ids)
-    assert st["peak_admitted_bytes"] <= 24 << 20
+    assert st["peak_admitted_bytes"] <= 48 << 20
     assert st["batches"] >= 2
 
 

@@ -39,5 +39,5 @@ def test_server_options_defaults():
     o = _lib.CServerOptions()
     lib.lumen_server_options_default(o)
     assert o.device_budget_bytes == 40 << 30
-    assert (o.max_batch_pairs, o.rows_per_band, o.max_inflight, o.watchdog_ms) == (32, 8, 2, 60000)
-    assert o.plain_fallback == 1
+    assert (o.max_batch_pairs, o.rows_per_band, o.max_inflight, o.watchdog_ms) == (32, 16, 2, 60000)
+    assert o.plain_fallback == 1 and o.schedule == 6
