@@ -346,7 +346,8 @@ def run_ours(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
         "config": workload_config(args.workload, world),
         "schedule": {"requested": args.schedule or "auto", "used": tuning[0],
-                     "lanes_per_pixel": tuning[1], "warps_per_block": tuning[2]},
+                     "lanes_per_pixel": tuning[1], "warps_per_block": tuning[2],
+                     "column_rows": sgbm.get_tuning_columns()},
         "roofline": {"bound": "hbm", "kernel": "sgm aggregation stage",
                      "achieved": achieved, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
                      "frac": achieved / hbm,

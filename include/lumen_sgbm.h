@@ -129,8 +129,16 @@ lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule);
  * without an instance falls back to the default.  0, 0 restores the automatic choice.
  * Values are identical for every setting. */
 lumen_status lumen_sgbm_set_tuning(lumen_sgbm* h, int lanes_per_pixel, int warps_per_block);
+/* Schedule 6 with 8 paths: rows per band of the column sweeps when they run as
+ * a launch of their own beside the row sweeps' (16, 24 or 32), 0 for one
+ * launch of all four sweeps, -1 for the automatic choice (the tuned value,
+ * else 24; a configuration pinned by lumen_sgbm_set_tuning alone keeps one
+ * launch).  No counterpart in the reference. */
+lumen_status lumen_sgbm_set_tuning_columns(lumen_sgbm* h, int rows_per_band);
 /* The schedule and configuration the last compute used: {schedule, lanes, warps}. */
 lumen_status lumen_sgbm_get_tuning(const lumen_sgbm* h, int out[3]);
+/* Rows per band of the column sweeps' own launch in the last compute (0: none). */
+lumen_status lumen_sgbm_get_tuning_columns(const lumen_sgbm* h, int* rows_per_band);
 /* Autotuner (no counterpart in the reference): runs every aggregation schedule
  * and sweep configuration `repeats` times on the given DEVICE pair, keeps the
  * fastest for this (size, disparity range, cost mode, path set) key, and

@@ -255,6 +255,18 @@ class StereoSGBM:
         """Pin the fused-sweep configuration (0, 0 = automatic)."""
         _check(_lib.lib().lumen_sgbm_set_tuning(self._h, lanes_per_pixel, warps_per_block))
 
+    def set_tuning_columns(self, rows_per_band: int = -1) -> None:
+        """Schedule 6 with 8 paths: the column sweeps in a launch of their own
+        with this many rows per band (16, 24, 32), 0 for one launch of all four
+        sweeps, -1 automatic."""
+        _check(_lib.lib().lumen_sgbm_set_tuning_columns(self._h, rows_per_band))
+
+    def get_tuning_columns(self) -> int:
+        """Rows per band of the column sweeps' own launch in the last compute (0: none)."""
+        r = C.c_int(0)
+        _check(_lib.lib().lumen_sgbm_get_tuning_columns(self._h, C.byref(r)))
+        return r.value
+
     def get_tuning(self):
         """(schedule, lanes per pixel, warps per block) the last compute used."""
         out = (C.c_int * 3)()

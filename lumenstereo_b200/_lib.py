@@ -71,6 +71,8 @@ def _declare(lib):
         "lumen_sgbm_debug_set_paths": (i, [vp, C.c_uint32]),
         "lumen_sgbm_set_schedule": (i, [vp, i]),
         "lumen_sgbm_set_tuning": (i, [vp, i, i]),
+        "lumen_sgbm_set_tuning_columns": (i, [vp, i]),
+        "lumen_sgbm_get_tuning_columns": (i, [vp, C.POINTER(C.c_int)]),
         "lumen_sgbm_debug_set_wait_limit": (i, [vp, C.c_longlong]),
         "lumen_sgbm_debug_stall_test": (i, [vp, i]),
         "lumen_sgbm_get_tuning": (i, [vp, C.POINTER(C.c_int)]),

@@ -69,6 +69,8 @@ struct lumen_sgbm {
     lumen_stereo_params params{};
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;         // schedule 6: the column sweeps' own launch
+    cudaEvent_t evFork = nullptr, evJoin = nullptr;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     DevBuf inL, inR, gray[2], pref[2], census[2], cost, agg, dispL, dispR, out, dbgLR, magic;
     DevBuf partB, xring, counters, status;  // sweep schedule: backward partial, exchange rings
@@ -83,6 +85,7 @@ struct lumen_sgbm {
     int stallTest = 0;                      // lumen_sgbm_debug_stall_test
     bool statusPending = false;
     SweepConfig forced{0, 0};               // lumen_sgbm_set_tuning (0 = automatic)
+    int forcedNC = -1;                      // lumen_sgbm_set_tuning_columns (-1 = automatic)
     std::map<std::string, std::pair<int, SweepConfig>> tuned;  // key -> (schedule, config)
     int lastSchedule = 0;
     SweepConfig lastConfig{0, 0};
@@ -163,6 +166,9 @@ extern "C" lumen_status lumen_sgbm_create(const lumen_stereo_params* params, lum
     if (e == cudaSuccess) e = h->status.ensure(sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(h->status.p, 0, sizeof(int));
     for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaEventCreate(&h->ev[i]);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->evJoin, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         lumen_sgbm_destroy(h);
         return fail(LUMEN_ERR_CUDA, std::string("lumen_sgbm_create: ") + cudaGetErrorString(e));
@@ -181,6 +187,9 @@ extern "C" lumen_status lumen_sgbm_destroy(lumen_sgbm* h) {
         b->release();
     for (auto& e : h->ev)
         if (e) cudaEventDestroy(e);
+    if (h->evFork) cudaEventDestroy(h->evFork);
+    if (h->evJoin) cudaEventDestroy(h->evJoin);
+    if (h->stream2) cudaStreamDestroy(h->stream2);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return LUMEN_OK;
@@ -303,11 +312,25 @@ extern "C" lumen_status lumen_sgbm_set_tuning(lumen_sgbm* h, int lanes, int warp
     return LUMEN_OK;
 }
 
+extern "C" lumen_status lumen_sgbm_set_tuning_columns(lumen_sgbm* h, int rows) {
+    if (!h) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL handle");
+    if (!(rows == -1 || rows == 0 || rows == 16 || rows == 24 || rows == 32))
+        return fail(LUMEN_ERR_INVALID_ARGUMENT, "column rows must be -1 (automatic), 0, 16, 24 or 32");
+    h->forcedNC = rows;
+    return LUMEN_OK;
+}
+
 extern "C" lumen_status lumen_sgbm_get_tuning(const lumen_sgbm* h, int out[3]) {
     if (!h || !out) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL argument");
     out[0] = h->lastSchedule;
     out[1] = h->lastConfig.T;
     out[2] = h->lastConfig.NW;
+    return LUMEN_OK;
+}
+
+extern "C" lumen_status lumen_sgbm_get_tuning_columns(const lumen_sgbm* h, int* rows) {
+    if (!h || !rows) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL argument");
+    *rows = h->lastConfig.NC;
     return LUMEN_OK;
 }
 
@@ -474,7 +497,15 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
         const bool diag = mask == 0xFFu;
         const int R6 = (cfgChosen && (cfg.NW == 16 || cfg.NW == 24 || cfg.NW == 32)) ? cfg.NW : 0;
         const int T6 = cfgChosen ? cfg.T : 0;
-        bool ok6 = pair_plan(k, wrap, diag, h->numSMs, &plan6, R6, T6) == cudaSuccess ||
+        // the column sweeps' own launch: pinned, tuned, or the default (a
+        // configuration pinned by lumen_sgbm_set_tuning alone keeps one launch)
+        const int Rc6 = !diag                ? 0
+                        : h->forcedNC >= 0   ? h->forcedNC
+                        : h->forced.T        ? 0
+                        : cfgChosen          ? cfg.NC
+                                             : kPairDefaultColumnRows;
+        bool ok6 = pair_plan(k, wrap, diag, h->numSMs, &plan6, R6, T6, Rc6) == cudaSuccess ||
+                   pair_plan(k, wrap, diag, h->numSMs, &plan6, 0, 0, Rc6) == cudaSuccess ||
                    pair_plan(k, wrap, diag, h->numSMs, &plan6) == cudaSuccess;
         if (ok6)
             ok6 = h->partB.ensure(ND * 2) == cudaSuccess && h->partC.ensure(ND * 2) == cudaSuccess &&
@@ -537,17 +568,17 @@ static lumen_status run_pipeline(lumen_sgbm* h, const uint8_t* dl, const uint8_t
                                     h->partD.as<uint16_t>()};
         unsigned long long* trace = nullptr;
         if (h->traceOn) {
-            h->traceWords = 4 * (size_t)plan6.nTickets;
+            h->traceWords = 4 * ((size_t)plan6.nTickets + plan6.nTicketsC);
             LCU(h->trace.ensure(h->traceWords * 8));
             LCU(cudaMemsetAsync(h->trace.p, 0, h->traceWords * 8, s));
             trace = h->trace.as<unsigned long long>();
         }
         LCU(launch_aggregate_pair(pv, parts, k, wrap, plan6, h->pairBuf.as<unsigned long long>(), epoch,
                                   h->counters.as<unsigned>(), h->status.as<int>(), h->spinMax, s,
-                                  h->stallTest, trace));
+                                  h->stallTest, trace, h->stream2, h->evFork, h->evJoin));
         h->statusPending = true;
         nl += 1;
-        cfg = SweepConfig{plan6.T, plan6.R};
+        cfg = SweepConfig{plan6.T, plan6.R, plan6.Rc};
         aggB = parts[1];
         aggC = parts[2];
         aggD = parts[3];
@@ -686,16 +717,22 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
             cands.push_back({4, SweepConfig{tl, 32}});
         }
         // schedule 6 takes `warps` as its rows per band (4 paths: 16 only)
+        // (8 paths: all four sweeps in one launch, or the column sweeps in a
+        // launch of their own with `NC` rows per band)
         const int t6 = pair_lanes(Dp);
         if (t6) {
             cands.push_back({6, SweepConfig{t6, 16}});
             if (mask == 0xFFu) {
                 cands.push_back({6, SweepConfig{t6, 24}});
                 cands.push_back({6, SweepConfig{t6, 32}});
+                for (int nw : {16, 24})
+                    for (int nc : {16, 24, 32})
+                        if (nc >= nw) cands.push_back({6, SweepConfig{t6, nw, nc}});
             }
         }
     }
     const SweepConfig savedForced = h->forced;
+    const int savedNC = h->forcedNC;
     const int savedSched = h->schedule;
     std::ostringstream rep;
     float bestMs = 1e30f;
@@ -703,6 +740,7 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
     for (auto& c : cands) {
         h->schedule = c.first;
         h->forced = c.second;
+        h->forcedNC = c.second.NC;
         float acc = 0.f;
         bool ok = true;
         for (int r = 0; r <= repeats; ++r) {  // first run warms up
@@ -715,17 +753,20 @@ extern "C" lumen_status lumen_sgbm_autotune(lumen_sgbm* h, const uint8_t* d_left
             if (st != LUMEN_OK) { ok = false; break; }
             if (r > 0) acc += h->timings[0];
         }
-        if (!ok || h->lastSchedule != c.first) continue;
+        if (!ok || h->lastSchedule != c.first || h->lastConfig.NC != c.second.NC) continue;
         const float ms = acc / repeats;
-        rep << "schedule=" << c.first << " lanes=" << c.second.T << " warps=" << c.second.NW
-            << " ms=" << ms << "\n";
+        rep << "schedule=" << c.first << " lanes=" << c.second.T << " warps=" << c.second.NW;
+        if (c.second.NC) rep << " cols=" << c.second.NC;
+        rep << " ms=" << ms << "\n";
         if (ms < bestMs) { bestMs = ms; best = c; }
     }
     h->schedule = savedSched;
     h->forced = savedForced;
+    h->forcedNC = savedNC;
     h->tuned[key] = best;
-    rep << "best schedule=" << best.first << " lanes=" << best.second.T << " warps="
-        << best.second.NW << " key=" << key << "\n";
+    rep << "best schedule=" << best.first << " lanes=" << best.second.T << " warps=" << best.second.NW;
+    if (best.second.NC) rep << " cols=" << best.second.NC;
+    rep << " key=" << key << "\n";
     if (report && report_bytes) {
         const std::string r = rep.str();
         std::snprintf(report, report_bytes, "%s", r.c_str());
@@ -739,7 +780,7 @@ extern "C" lumen_status lumen_sgbm_tuning_save(const lumen_sgbm* h, const char* 
     if (!f) return fail(LUMEN_ERR_INVALID_ARGUMENT, std::string("cannot write ") + path);
     for (auto& kv : h->tuned)
         f << kv.first << " " << kv.second.first << " " << kv.second.second.T << " "
-          << kv.second.second.NW << "\n";
+          << kv.second.second.NW << " " << kv.second.second.NC << "\n";
     return LUMEN_OK;
 }
 
@@ -747,11 +788,16 @@ extern "C" lumen_status lumen_sgbm_tuning_load(lumen_sgbm* h, const char* path) 
     if (!h || !path) return fail(LUMEN_ERR_INVALID_ARGUMENT, "NULL argument");
     std::ifstream f(path);
     if (!f) return fail(LUMEN_ERR_INVALID_ARGUMENT, std::string("cannot read ") + path);
-    std::string key;
-    int sched, T, NW;
-    while (f >> key >> sched >> T >> NW)
-        if (sched == 1 || sched == 4 || sched == 6)  // entries of retired schedules are skipped
-            h->tuned[key] = {sched, SweepConfig{T, NW}};
+    // key schedule lanes rows [column rows]; entries of retired schedules are skipped
+    std::string line;
+    while (std::getline(f, line)) {
+        std::istringstream in(line);
+        std::string key;
+        int sched = 0, T = 0, NW = 0, NC = 0;
+        if (!(in >> key >> sched >> T >> NW)) continue;
+        if (!(in >> NC)) NC = 0;
+        if (sched == 1 || sched == 4 || sched == 6) h->tuned[key] = {sched, SweepConfig{T, NW, NC}};
+    }
     return LUMEN_OK;
 }
 

@@ -38,7 +38,11 @@ cudaError_t launch_aggregate_per_direction(const PairView& pv, const SgmConsts& 
 struct SweepConfig {
     int T;
     int NW;
+    int NC = 0;   // schedule 6: rows per band of the column sweeps' own launch (0: one launch)
 };
+// Untuned schedule 6 with 8 paths: the column sweeps in a launch of their own
+// with 24-row bands (1920x1080 D128: aggregation 1.90 -> 1.66 ms).
+constexpr int kPairDefaultColumnRows = 24;
 
 // ---- schedule 4: lockstep row-band fused sweeps (wave.cu, wave_kernel.cuh) ----
 struct WavePlan {
@@ -88,20 +92,25 @@ struct PairPlan {
     int R, T;              // rows per band, lanes per row
     bool diag;             // 8 paths (the diagonals ride along); false: LR, RL, TB, BT alone
     int nb0, nb1;          // bands of the row sweeps, of the column sweeps
-    int nTickets;          // 2 * nb0 + 2 * nb1
+    int nTickets;          // 2 * nb0 + 2 * nb1 (split: 2 * nb0, the row sweeps' launch)
     int grid;              // CTAs launched (persistent, ticket-scheduled)
     int smem;              // dynamic shared memory per CTA
     size_t xbufBytes;      // band-boundary row buffers, all sweeps
-    size_t counterWords;   // the ticket counter
+    size_t counterWords;   // ticket counters (one a launch)
+    // Rc > 0 (8 paths): the column sweeps run as a second, concurrent launch
+    // with Rc rows per band; its tickets, CTAs and shared memory
+    int Rc, nTicketsC, gridC, smemC;
 };
 // lanes per row of schedule 6 for a padded disparity count (0: no instance)
 int pair_lanes(int Dp);
 // diag: 8 paths; false: the 4 paths LR, RL, TB, BT (one per sweep, no band
 // hand-offs).  R: rows per band, 16, 24 or 32 with diag, 16 without (0: the
-// default, 16); T: lanes per row (0 or pair_lanes(Dp)).
+// default, 16); T: lanes per row (0 or pair_lanes(Dp)); Rc (diag only): 0
+// runs all four sweeps in one launch, 16, 24 or 32 runs the column sweeps as
+// a launch of their own with Rc rows per band (the row sweeps keep R).
 // cudaErrorInvalidValue: no instance for these disparities / sizes
 cudaError_t pair_plan(const SgmConsts& k, bool wrap, bool diag, int numSMs, PairPlan* plan, int R = 0,
-                      int T = 0);
+                      int T = 0, int Rc = 0);
 // Plan of a batched launch of one kernel class: the pairs' longest sweep row
 // Lmax sizes the shared memory; nb0/nb1/nTickets/xbufBytes stay 0 (per pair);
 // grid is the resident CTA count (the launch takes at most its ticket count).
@@ -120,10 +129,14 @@ cudaError_t launch_aggregate_pair_batch(const PairJob* d_jobs, const uint32_t* d
 // part[0..3]: the four sweeps' partial volumes (part[0] may be pv.agg).  xbuf:
 // the row buffers (plan.xbufBytes), every word of which holds an epoch below
 // `epoch` (zero-filled when allocated, then one epoch per launch, increasing).
+// With plan.Rc the column sweeps' launch goes to s2, forked from s by evFork
+// and joined back by evJoin.
 cudaError_t launch_aggregate_pair(const PairView& pv, uint16_t* const part[4], const SgmConsts& k, bool wrap,
                                   const PairPlan& plan, unsigned long long* xbuf, unsigned epoch,
                                   unsigned* counters, int* status, long long spinMax, cudaStream_t s,
-                                  int stallTest = 0, unsigned long long* trace = nullptr);
+                                  int stallTest = 0, unsigned long long* trace = nullptr,
+                                  cudaStream_t s2 = nullptr, cudaEvent_t evFork = nullptr,
+                                  cudaEvent_t evJoin = nullptr);
 
 // aggB (nullable): second partial volume summed with agg (mod 2^16 when wrap);
 // aggC, aggD (nullable, both or neither): two more (schedule 6).

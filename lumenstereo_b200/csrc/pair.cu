@@ -92,29 +92,45 @@ static cudaError_t pair_dispatch(const PairArgs& a, int Dp, int R, int T, bool d
     return cudaErrorInvalidValue;
 }
 
-cudaError_t pair_plan(const SgmConsts& k, bool wrap, bool diag, int numSMs, PairPlan* plan, int R, int T) {
+cudaError_t pair_plan(const SgmConsts& k, bool wrap, bool diag, int numSMs, PairPlan* plan, int R, int T, int Rc) {
     if (!pair_lanes(k.Dp)) return cudaErrorInvalidValue;
     if (R == 0) R = 16;
     if (T == 0) T = pair_lanes(k.Dp);
     if (!pair_instance(k.Dp, T, R, diag)) return cudaErrorInvalidValue;
+    if (Rc && (!diag || !pair_instance(k.Dp, T, Rc, true))) return cudaErrorInvalidValue;
     PairPlan p{};
     p.R = R;
     p.T = T;
     p.diag = diag;
+    p.Rc = Rc;
     p.nb0 = (k.H + R - 1) / R;
-    p.nb1 = (k.W + R - 1) / R;
-    p.nTickets = 2 * p.nb0 + 2 * p.nb1;
-    p.smem = pair_smem(std::max(k.W, k.H), k.Dp, R).total;
-    if (p.smem > 227 * 1024) return cudaErrorInvalidValue;
+    p.nb1 = (k.W + (Rc ? Rc : R) - 1) / (Rc ? Rc : R);
+    const bool full = k.D == k.Dp;
     PairArgs dummy{};
     int perSM = 0;
-    cudaError_t e = pair_dispatch(dummy, k.Dp, R, T, diag, wrap, k.D == k.Dp, p.smem, 0, nullptr, &perSM);
+    if (!Rc) {
+        p.nTickets = 2 * p.nb0 + 2 * p.nb1;
+        p.smem = pair_smem(std::max(k.W, k.H), k.Dp, R).total;
+    } else {
+        // row sweeps stage rows of W pixels, column sweeps columns of H
+        p.nTickets = 2 * p.nb0;
+        p.smem = pair_smem(k.W, k.Dp, R).total;
+        p.nTicketsC = 2 * p.nb1;
+        p.smemC = pair_smem(k.H, k.Dp, Rc).total;
+        if (p.smemC > 227 * 1024) return cudaErrorInvalidValue;
+        cudaError_t e = pair_dispatch(dummy, k.Dp, Rc, T, true, wrap, full, p.smemC, 0, nullptr, &perSM);
+        if (e != cudaSuccess) return e;
+        if (perSM < 1) return cudaErrorInvalidConfiguration;
+        p.gridC = std::min(p.nTicketsC, perSM * numSMs);
+    }
+    if (p.smem > 227 * 1024) return cudaErrorInvalidValue;
+    cudaError_t e = pair_dispatch(dummy, k.Dp, R, T, diag, wrap, full, p.smem, 0, nullptr, &perSM);
     if (e != cudaSuccess) return e;
     if (perSM < 1) return cudaErrorInvalidConfiguration;
     p.grid = std::min(p.nTickets, perSM * numSMs);
     // band-boundary rows only when the diagonals cross the bands
     p.xbufBytes = diag ? pair_xbase(3, p.nb1, k.W, k.H, p.nb0, p.nb1) * (size_t)pair_ll_words(k.Dp) * 8 : 0;
-    p.counterWords = 1;   // the ticket counter
+    p.counterWords = Rc ? 2 : 1;   // the ticket counter of each launch
     *plan = p;
     return cudaSuccess;
 }
@@ -189,9 +205,11 @@ cudaError_t launch_aggregate_pair_batch(const PairJob* d_jobs, const uint32_t* d
 cudaError_t launch_aggregate_pair(const PairView& pv, uint16_t* const part[4], const SgmConsts& k, bool wrap,
                                   const PairPlan& plan, unsigned long long* xbuf, unsigned epoch,
                                   unsigned* counters, int* status, long long spinMax, cudaStream_t s,
-                                  int stallTest, unsigned long long* trace) {
+                                  int stallTest, unsigned long long* trace, cudaStream_t s2,
+                                  cudaEvent_t evFork, cudaEvent_t evJoin) {
     PairArgs a{};
     a.job = pair_job(pv, part, k, plan.R, xbuf);
+    a.job.nb[1] = plan.nb1;   // the column sweeps' bands (their own height when split)
     a.nTickets = plan.nTickets;
     a.Lmax = std::max(k.W, k.H);
     a.ticket = counters;
@@ -200,10 +218,29 @@ cudaError_t launch_aggregate_pair(const PairView& pv, uint16_t* const part[4], c
     a.epoch = epoch;
     a.stallTest = stallTest;
     a.trace = trace;
+    const bool full = k.D == k.Dp;
     cudaError_t e = cudaMemsetAsync(counters, 0, sizeof(unsigned) * plan.counterWords, s);
     if (e != cudaSuccess) return e;
     int perSM = 0;
-    return pair_dispatch(a, k.Dp, plan.R, plan.T, plan.diag, wrap, k.D == k.Dp, plan.smem, plan.grid, s, &perSM);
+    if (!plan.Rc) return pair_dispatch(a, k.Dp, plan.R, plan.T, plan.diag, wrap, full, plan.smem, plan.grid, s, &perSM);
+    if (!s2 || !evFork || !evJoin) return cudaErrorInvalidValue;
+    // the row sweeps on s, the column sweeps on s2: the two share only the
+    // (disjoint) row buffers and partial volumes, and wait on nothing of each other
+    PairArgs ac = a;
+    a.sweeps = 1;
+    a.Lmax = k.W;
+    ac.sweeps = 2;
+    ac.nTickets = plan.nTicketsC;
+    ac.Lmax = k.H;
+    ac.ticket = counters + 1;
+    if (trace) ac.trace = trace + 4 * (size_t)plan.nTickets;
+    e = cudaEventRecord(evFork, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, evFork, 0);
+    if (e == cudaSuccess) e = pair_dispatch(a, k.Dp, plan.R, plan.T, true, wrap, full, plan.smem, plan.grid, s, &perSM);
+    if (e == cudaSuccess) e = pair_dispatch(ac, k.Dp, plan.Rc, plan.T, true, wrap, full, plan.smemC, plan.gridC, s2, &perSM);
+    if (e == cudaSuccess) e = cudaEventRecord(evJoin, s2);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, evJoin, 0);
+    return e;
 }
 
 }  // namespace lumen

@@ -84,7 +84,8 @@ struct PairArgs {
     int* status;
     long long spinMax;
     unsigned epoch;                // high half of every row-buffer word this launch writes
-    int stallTest;                 // 1: ticket 4 (band 1 of sweep 0) waits for an epoch never written
+    int sweeps;                    // one pair: 0 all four sweeps, 1 the row sweeps (0, 1), 2 the column sweeps (2, 3)
+    int stallTest;                 // 1: band 1 of sweep 0 waits for an epoch never written
     unsigned long long* trace;     // optional band timeline, [nTickets][4] (pair_trace_record)
 };
 
@@ -178,7 +179,12 @@ __device__ __forceinline__ void pair_body(const PairArgs& a) {
                     b = (int)(e & 0x3FFFFu);
                     *sJob = a.jobs[jb];
                 } else {
-                    pair_ticket(t, a.job.nb[0], a.job.nb[1], s, b);
+                    if (a.sweeps == 0) {
+                        pair_ticket(t, a.job.nb[0], a.job.nb[1], s, b);
+                    } else {   // two sweeps of one kind, bands in order
+                        s = (a.sweeps == 1 ? 0 : 2) + (t & 1);
+                        b = t >> 1;
+                    }
                     if (curJob < 0) *sJob = a.job;
                 }
                 sflag[2] = s;
@@ -428,7 +434,7 @@ __device__ __forceinline__ void pair_body(const PairArgs& a) {
         } else if (hasPrev) {
             // ===================== import warp: the band above's last row =====================
             const unsigned long long* xin = J.xbuf + pair_xbase(s, b - 1, W, H, J.nb[0], J.nb[1]) * NL;
-            const unsigned want = (a.stallTest && t == 4) ? a.epoch + 1u : a.epoch;
+            const unsigned want = (a.stallTest && s == 0 && b == 1) ? a.epoch + 1u : a.epoch;
             const int nImp = Ws - 1;     // row 0 uses pixels 0 .. Ws-2
             constexpr int PER = (kPG * PAIRS + 31) / 32;
             unsigned freeSeen = 0;

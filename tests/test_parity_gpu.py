@@ -200,6 +200,7 @@ def test_parity_schedule6_pair_sweeps(D, size, census, oracle_mod):
         disp = s.compute(left, right)
         agg = s.intermediate("agg", (h, w, D), np.uint16)
         assert s.get_tuning()[0] == 6
+        assert s.get_tuning_columns() == 24   # untuned: the column sweeps in their own launch
     assert np.array_equal(agg, ref["agg"])
     assert_subpix_close(disp, ref_disp)
     with StereoSGBM(to_params(pd)) as s:
@@ -230,6 +231,38 @@ def test_parity_schedule6_configurations(D, size, lanes, rows, oracle_mod):
             agg = s.intermediate("agg", (h, w, D), np.uint16)
             assert s.get_tuning() == (6, lanes, rows), s.get_tuning()
         assert np.array_equal(agg, ref["agg"]), (census, lanes, rows)
+        assert_subpix_close(disp, ref_disp)
+
+
+@pytest.mark.parametrize("D,size,lanes,rows,cols",
+                         [(D, size, 8, rows, cols)
+                          for D, size in [(40, (131, 53)), (128, (97, 150)), (100, (700, 90)), (64, (40, 200))]
+                          for rows, cols in [(16, 16), (16, 24), (16, 32), (24, 24), (24, 32)]] +
+                         [(D, size, 16, 16, cols) for D, size in [(150, (160, 70)), (290, (330, 61))]
+                          for cols in (16, 24, 32)])
+def test_parity_schedule6_column_launch(D, size, lanes, rows, cols, oracle_mod):
+    """The column sweeps as a launch of their own beside the row sweeps' (with
+    their own band height, on a second stream): the summed volume equals the
+    oracle's bit for bit, both cost modes, partial last bands included."""
+    w, h = size
+    left, right, _ = synth.make_pair(synth.PairSpec(w, h, 4, 1, min(D - 1, 40), 2.0, 400 + D + w))
+    for census in (0, 1):
+        pd = params_dict(maxDisparity=D, numDirections=8, speckleWindowSize=0, matchingCostMode=census)
+        ref_disp, ref = oracle_mod.sgbm(pd, left, right, intermediates=True)
+        with StereoSGBM(to_params(pd)) as s:
+            s.set_schedule(6)
+            s.set_tuning(lanes, rows)
+            s.set_tuning_columns(cols)
+            s.retain_intermediates(True)
+            disp = s.compute(left, right)
+            agg = s.intermediate("agg", (h, w, D), np.uint16)
+            assert s.get_tuning() == (6, lanes, rows), s.get_tuning()
+            assert s.get_tuning_columns() == cols
+            # and one launch of all four sweeps gives the same maps
+            s.set_tuning_columns(0)
+            assert np.array_equal(s.compute(left, right), disp)
+            assert s.get_tuning_columns() == 0
+        assert np.array_equal(agg, ref["agg"]), (census, lanes, rows, cols)
         assert_subpix_close(disp, ref_disp)
 
 
