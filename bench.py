@@ -60,7 +60,8 @@ def parse():
                          "serve: Poisson request stream through the served form")
     ap.add_argument("--pairs", type=int, default=0,
                     help="distinct pairs of the mixed stream (batch: 64, serve: 32)")
-    ap.add_argument("--requests", type=int, default=200, help="requests per offered rate (--mode serve)")
+    ap.add_argument("--requests", type=int, default=200,
+                    help="requests per offered rate (--mode serve; 0: 25 s of arrivals, at most 10000)")
     ap.add_argument("--rates", default="20,50,100,200,300,400", help="offered rates, requests/s (--mode serve)")
     return ap.parse_args()
 
@@ -580,7 +581,9 @@ def run_serve(args):
     for item in pool:
         plain_one(item)
     plain_rate = len(pool) / (time.perf_counter() - t0)
-    srv = StereoServer(budget_bytes=40 << 30, max_batch_pairs=32, rows_per_band=16, max_inflight=2)
+    srv_sched = args.schedule if args.schedule in (4, 6) else 6
+    srv = StereoServer(budget_bytes=40 << 30, max_batch_pairs=32, rows_per_band=16, max_inflight=2,
+                       schedule=srv_sched)
     for key, (w, h, m) in maps.items():
         srv.set_calibration(key, w, h, *m)
     # warm-up pass, and the bit-exact check of every pool pair
@@ -591,7 +594,8 @@ def run_serve(args):
     sweep = []
     with ClockSampler(local) as clocks:
         for rate in rates:
-            n = args.requests
+            # --requests 0: 25 s of arrivals at this rate, at most 10,000 requests
+            n = args.requests or int(min(10000, max(200, 25 * rate)))
             gaps = rng.exponential(1.0 / rate, n)
             picks = rng.integers(0, len(pool), n)
             sub = [None] * n
@@ -629,14 +633,15 @@ def run_serve(args):
     st = srv.stats()
     best = max(sweep, key=lambda r: r["achieved_pairs_per_s"])
     res = {"metric": "served pairs/s with p50/p99 latency", "value": best["achieved_pairs_per_s"],
-           "unit": "pairs/s", "n_gpus": world, "steps": len(rates) * args.requests, "warmup": len(pool),
+           "unit": "pairs/s", "n_gpus": world, "steps": sum(r["requests"] for r in sweep), "warmup": len(pool),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16",
            "data": "synthetic",
            "config": {"workload": f"served_stream_pool_{len(pool)}_pairs", "seeds": f"10000..{9999 + len(pool)}",
                       "calibrations": "16 ids (seed % 16), rectified on the device from resident maps",
-                      "arrivals": "Poisson", "requests_per_rate": args.requests,
+                      "arrivals": "Poisson",
+                      "requests_per_rate": args.requests or "25 s of arrivals, at most 10000",
                       "budget_bytes": 40 << 30, "max_batch_pairs": 32, "max_inflight": 2,
-                      "rows_per_band": 16},
+                      "schedule": srv_sched, "rows_per_band": 16},
            "p50_ms": best["p50_ms"], "p99_ms": best["p99_ms"], "p999_ms": best["p999_ms"],
            "rates": sweep,
            "plain_serial": {"value": plain_rate, "unit": "pairs/s",
