@@ -56,6 +56,7 @@ def test_profiled_traffic_belongs_to_the_captured_schedule():
     without a capture reports none."""
     import bench
     assert bench.profiled_traffic("1920x1080_d128_sad_8path", 4) == 6.42
-    assert bench.profiled_traffic("1920x1080_d128_sad_8path", 6) == 13.59
+    assert bench.profiled_traffic("1920x1080_d128_sad_8path", 6) == 13.16
+    assert bench.profiled_traffic("1920x1080_d128_census_8path", 6) == 13.15
     assert bench.profiled_traffic("1920x1080_d128_sad_8path", 1) is None
     assert bench.profiled_traffic("640x480_d64_census_4path", 4) is None
