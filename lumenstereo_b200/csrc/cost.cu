@@ -5,6 +5,8 @@
 //   SAD    src/sgbm_kernels.cu:70-212   integer mean of |Lf-Rf| over the valid
 //                                       part of the window, 255 if none valid
 //   Census src/sgbm_kernels.cu:250-286  (h*255+12)/24, 255 in the 2-px border
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -88,73 +90,126 @@ __global__ void census_kernel(const uint8_t* __restrict__ gl, const uint8_t* __r
 __device__ __forceinline__ uint32_t census_cost_of(int h) { return (uint32_t)((85 * h + 4) >> 3); }
 
 // src/sgbm_kernels.cu:250-286 (computeCostCensus_naive).  One CTA per (row,
-// 64-pixel tile); the right descriptors the tile can reach are staged in
-// shared memory; each thread writes 16 consecutive disparities of one pixel
-// as one 16-byte store (a warp's stores are contiguous).  Interior pixels
-// (every reachable right pixel inside the 2-px border) skip the per-disparity
-// border tests and convert two Hamming distances per instruction:
-// ((85*(h0 | h1<<16) + 0x40004) >> 3) & 0x00FF00FF.
-constexpr int kCensusTile = 64;
+// 128-pixel tile).  The tile's left descriptors and every right descriptor it
+// can reach are staged in shared memory; a thread takes 4 consecutive pixels
+// x 16 consecutive disparities and reads the 19 right descriptors that block
+// reaches as five aligned 16-byte loads (right column x - d for pixel i,
+// disparity dlo + k is window word 15 + i - k).  Blocks whose pixels and
+// right columns all lie inside the 2-px border convert two Hamming distances
+// per instruction, ((85*(h0 | h1<<16) + 0x40004) >> 3) & 0x00FF00FF; the
+// others take the per-disparity border rules.  The tile's costs go through
+// shared memory (rows padded so the 16-byte writes of a quarter-warp hit
+// distinct banks) and leave as contiguous 16-byte stores.
+constexpr int kCensusTile = 128;
+constexpr int kCensusPx = 4;   // consecutive pixels a thread
+
+// shared-memory words: left descriptors, right descriptors, cost tile
+__host__ __device__ inline int census_tile_pitch_words(int Dp) {
+    const int w = Dp / 4;
+    return w % 8 == 0 ? w + 4 : w;   // an odd multiple of 4 words between rows
+}
+__host__ __device__ inline int census_right_words(int Dp) { return kCensusTile + Dp + 4; }
+__host__ __device__ inline size_t census_smem_bytes(int Dp) {
+    return 4 * ((size_t)kCensusTile + census_right_words(Dp) + (size_t)kCensusTile * census_tile_pitch_words(Dp));
+}
+
 __global__ void __launch_bounds__(256)
 census_cost_kernel(const uint32_t* __restrict__ cl, const uint32_t* __restrict__ cr, int W,
                    int H, int D, int Dp, int minD, uint8_t* __restrict__ cost) {
-    extern __shared__ uint32_t sm_cr[];  // kCensusTile + Dp - 1 entries
+    extern __shared__ __align__(16) uint32_t sm_c[];
+    uint32_t* const sl = sm_c;                       // kCensusTile left descriptors
+    uint32_t* const sr = sm_c + kCensusTile;         // right descriptors of columns lo, lo+1, ...
+    const int RW = census_right_words(Dp);
+    const int P = census_tile_pitch_words(Dp);
+    uint32_t* const tile = sr + RW;                  // costs, pixel p at word p * P
     const int y = blockIdx.y;
     const int x0 = blockIdx.x * kCensusTile;
-    const int lo = x0 - minD - (Dp - 1);  // leftmost right-image column reached
-    const int n = kCensusTile + Dp - 1;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int lo = x0 - minD - (Dp - 1);             // right column of sr[0]
+    for (int i = threadIdx.x; i < RW; i += blockDim.x) {
         const int rx = lo + i;
-        sm_cr[i] = (rx >= 0 && rx < W) ? cr[(size_t)y * W + rx] : 0u;
+        sr[i] = (rx >= 0 && rx < W) ? cr[(size_t)y * W + rx] : 0u;
+    }
+    for (int i = threadIdx.x; i < kCensusTile; i += blockDim.x) {
+        const int x = x0 + i;
+        sl[i] = x < W ? cl[(size_t)y * W + x] : 0u;
     }
     __syncthreads();
     const int chunks = Dp / 16;
-    const bool rowOk = (y >= 2 && y < H - 2);
-    // thread -> one 16-disparity chunk, striding over the tile's pixels
-    const int ch = threadIdx.x % chunks;
-    const int pxStep = blockDim.x / chunks;
-    const int px0 = threadIdx.x / chunks;
-    if (px0 >= pxStep) return;  // no barrier below
-    for (int px = px0; px < kCensusTile; px += pxStep) {
-        const int x = x0 + px;
-        if (x >= W) break;
-        const bool leftOk = rowOk && x >= 2 && x < W - 2;
+    const bool rowOk = y >= 2 && y < H - 2;
+    constexpr int groups = kCensusTile / kCensusPx;
+    // item -> (pixel group pg, chunk ch), pg fastest: a quarter-warp's window
+    // loads cover 128 contiguous bytes
+    for (int it = threadIdx.x; it < groups * chunks; it += blockDim.x) {
+        const int pg = it % groups, ch = it / groups;
+        const int xb = x0 + pg * kCensusPx;
+        if (xb >= W) continue;
         const int dlo = ch * 16;
-        const int rxHi = x - minD - dlo, rxLo = rxHi - 15;  // right columns of this chunk
-        uint32_t wv[4];
-        if (leftOk && rxLo >= 2 && rxHi < W - 2 && dlo + 16 <= D) {
-            const uint32_t a = cl[(size_t)y * W + x];
-            const uint32_t* rp = sm_cr + (rxHi - lo);
+        const int rxTop = xb + kCensusPx - 1 - minD - dlo;   // right column of (pixel 3, dlo)
+        uint8_t* const out = reinterpret_cast<uint8_t*>(tile) + (size_t)pg * kCensusPx * P * 4 + dlo;
+        const bool fast = rowOk && xb >= 2 && xb + kCensusPx - 1 < W - 2 && rxTop - 18 >= 2 &&
+                          rxTop < W - 2 && dlo + 16 <= D;
+        if (fast) {
+            // window word m holds right column rxTop - 18 + m; its index in sr is a
+            // multiple of 4 (pg*4 - dlo + Dp - 16)
+            uint32_t w[20];
+            const uint4* wp = reinterpret_cast<const uint4*>(sr + (rxTop - 18 - lo));
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const uint32_t h0 = __popc(a ^ rp[-(4 * q + 0)]);
-                const uint32_t h1 = __popc(a ^ rp[-(4 * q + 1)]);
-                const uint32_t h2 = __popc(a ^ rp[-(4 * q + 2)]);
-                const uint32_t h3 = __popc(a ^ rp[-(4 * q + 3)]);
-                const uint32_t c02 = ((85u * (h0 | (h2 << 16)) + 0x40004u) >> 3) & 0x00FF00FFu;
-                const uint32_t c13 = ((85u * (h1 | (h3 << 16)) + 0x40004u) >> 3) & 0x00FF00FFu;
-                wv[q] = c02 | (c13 << 8);
+            for (int q = 0; q < 5; ++q) {
+                const uint4 v = wp[q];
+                w[4 * q] = v.x; w[4 * q + 1] = v.y; w[4 * q + 2] = v.z; w[4 * q + 3] = v.w;
+            }
+#pragma unroll
+            for (int i = 0; i < kCensusPx; ++i) {
+                const uint32_t a = sl[pg * kCensusPx + i];
+                uint32_t wv[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const uint32_t h0 = __popc(a ^ w[15 + i - (4 * q + 0)]);
+                    const uint32_t h1 = __popc(a ^ w[15 + i - (4 * q + 1)]);
+                    const uint32_t h2 = __popc(a ^ w[15 + i - (4 * q + 2)]);
+                    const uint32_t h3 = __popc(a ^ w[15 + i - (4 * q + 3)]);
+                    const uint32_t c02 = ((85u * (h0 | (h2 << 16)) + 0x40004u) >> 3) & 0x00FF00FFu;
+                    const uint32_t c13 = ((85u * (h1 | (h3 << 16)) + 0x40004u) >> 3) & 0x00FF00FFu;
+                    wv[q] = c02 | (c13 << 8);
+                }
+                *reinterpret_cast<uint4*>(out + (size_t)i * P * 4) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
             }
         } else {
-            const uint32_t a = leftOk ? cl[(size_t)y * W + x] : 0u;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                uint32_t packed = 0;
+            for (int i = 0; i < kCensusPx; ++i) {
+                const int x = xb + i;
+                const bool leftOk = rowOk && x >= 2 && x < W - 2;
+                const uint32_t a = leftOk ? sl[pg * kCensusPx + i] : 0u;
+                uint32_t wv[4];
 #pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    const int d = dlo + q * 4 + b;
-                    const int rx = x - minD - d;
-                    uint32_t c;
-                    if (d >= D) c = 0u;
-                    else if (!leftOk || rx < 2 || rx >= W - 2) c = 255u;
-                    else c = census_cost_of(__popc(a ^ sm_cr[rx - lo]));
-                    packed |= c << (8 * b);
+                for (int q = 0; q < 4; ++q) {
+                    uint32_t packed = 0;
+#pragma unroll
+                    for (int bb = 0; bb < 4; ++bb) {
+                        const int d = dlo + q * 4 + bb;
+                        const int rx = x - minD - d;
+                        uint32_t c;
+                        if (d >= D) c = 0u;
+                        else if (!leftOk || rx < 2 || rx >= W - 2) c = 255u;
+                        else c = census_cost_of(__popc(a ^ sr[rx - lo]));
+                        packed |= c << (8 * bb);
+                    }
+                    wv[q] = packed;
                 }
-                wv[q] = packed;
+                *reinterpret_cast<uint4*>(out + (size_t)i * P * 4) = make_uint4(wv[0], wv[1], wv[2], wv[3]);
             }
         }
-        *reinterpret_cast<uint4*>(cost + ((size_t)y * W + x) * Dp + dlo) =
-            make_uint4(wv[0], wv[1], wv[2], wv[3]);
+    }
+    __syncthreads();
+    // the tile's rows, contiguous in the volume, as 16-byte stores
+    const int npx = min(kCensusTile, W - x0);
+    const int cpr = Dp / 16;                         // 16-byte chunks a pixel
+    uint8_t* const dst = cost + ((size_t)y * W + x0) * Dp;
+    for (int c = threadIdx.x; c < npx * cpr; c += blockDim.x) {
+        const int px = c / cpr, k = c - px * cpr;
+        const uint4 v = *reinterpret_cast<const uint4*>(reinterpret_cast<const uint8_t*>(tile) +
+                                                        (size_t)px * P * 4 + 16 * k);
+        *reinterpret_cast<uint4*>(dst + (size_t)c * 16) = v;
     }
 }
 
@@ -617,14 +672,16 @@ void launch_census(const uint8_t* gl, const uint8_t* gr, int W, int H, uint32_t*
 
 cudaError_t launch_census_cost(const uint32_t* cl, const uint32_t* cr, int W, int H, int D,
                                int Dp, int minD, uint8_t* cost, cudaStream_t s) {
-    const size_t smem = (size_t)(kCensusTile + Dp - 1) * 4;
+    const size_t smem = census_smem_bytes(Dp);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(census_cost_kernel,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
     dim3 g((W + kCensusTile - 1) / kCensusTile, H);
-    census_cost_kernel<<<g, 256, smem, s>>>(cl, cr, W, H, D, Dp, minD, cost);
+    // one thread a (4-pixel group, 16-disparity chunk) item, up to 256
+    const int threads = std::min(256, (kCensusTile / kCensusPx) * (Dp / 16));
+    census_cost_kernel<<<g, threads, smem, s>>>(cl, cr, W, H, D, Dp, minD, cost);
     return cudaGetLastError();
 }
 

@@ -339,12 +339,23 @@ def test_autotune_and_cache(tmp_path):
         rep = s.autotune(dl.data_ptr(), dr.data_ptr(), 320, 180)
         assert "best schedule=" in rep
         assert np.array_equal(s.compute(left, right), ref)  # uses the tuned choice
+        tuned = (s.get_tuning(), s.get_tuning_columns())
         path = str(tmp_path / "tune.txt")
         s.save_tuning(path)
     with StereoSGBM(p) as s2:
         s2.load_tuning(path)
         assert np.array_equal(s2.compute(left, right), ref)
-    assert open(path).read().strip()
+        assert (s2.get_tuning(), s2.get_tuning_columns()) == tuned   # the column launch included
+    lines = open(path).read().split()
+    assert len(lines) == 5   # key schedule lanes rows column-rows
+    # a cache written before the column launch existed (four fields) still loads: one launch
+    old = tmp_path / "old.txt"
+    old.write_text(" ".join(lines[:3] + ["16"]) + "\n")
+    with StereoSGBM(p) as s3:
+        s3.load_tuning(str(old))
+        assert np.array_equal(s3.compute(left, right), ref)
+        if int(lines[1]) == 6:
+            assert s3.get_tuning_columns() == 0
 
 
 @pytest.mark.parametrize("k", range(8))
