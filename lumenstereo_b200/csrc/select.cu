@@ -114,7 +114,26 @@ __device__ __forceinline__ uint32_t vol_cost(const uint16_t* __restrict__ a, con
     return v & 0xFFFFu;
 }
 
-template <int TL, int KS, bool FULL, int NV, bool NB>
+// Shared-memory ring of the staged pixels (PF > 0): per slot, volume and
+// 16-byte quarter of a lane's words, one uint4 a thread (consecutive threads
+// consecutive uint4, so a warp's loads hit distinct banks).
+__host__ __device__ inline size_t select_ring_bytes(int PF, int NV, int KS) {
+    return (size_t)PF * NV * (KS / 4) * 256 * 16;
+}
+__device__ __forceinline__ void sel_cp16(void* smem, const void* gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
+                 "l"(gmem)
+                 : "memory");
+}
+
+// PF = 0: the next pixel's words are loaded into registers one pixel ahead.
+// PF = 2 or 3 (needs KS % 4 == 0): each thread copies its words of pixel
+// x + PF - 1 into a PF-slot shared ring with cp.async while it works on pixel
+// x, so PF - 1 pixels of every team are in flight and the registers hold only
+// summed words.  The launcher takes it where it measured faster (4-word
+// lanes); with 8-word lanes the register form's loads stall the warps (4
+// cycles per issued instruction) but the staged form was slower still.
+template <int TL, int KS, bool FULL, int NV, bool NB, int PF = 0>
 __device__ __forceinline__ void
 select_slide_body(const uint16_t* __restrict__ agg, const uint16_t* __restrict__ aggB,
                   const uint16_t* __restrict__ aggC, const uint16_t* __restrict__ aggD, int wrap,
@@ -123,7 +142,8 @@ select_slide_body(const uint16_t* __restrict__ agg, const uint16_t* __restrict__
     constexpr int M = 2 * KS;
     constexpr uint32_t INF = 0xFFFFFFFFu;
     constexpr unsigned long long INF64 = ~0ull;
-    extern __shared__ uint32_t rec[];  // [W] right-view keys of the row
+    static_assert(PF == 0 || (KS % 4 == 0 && (PF == 2 || PF == 3)), "staged ring");
+    extern __shared__ __align__(16) uint32_t rec[];  // [W] right-view keys of the row (then the ring)
     unsigned long long* const rec64 = reinterpret_cast<unsigned long long*>(rec);  // [W] (key << 32 | pair), NB
     const int y = blockIdx.x;
     for (int i = threadIdx.x; i < W; i += blockDim.x) {
@@ -145,22 +165,72 @@ select_slide_body(const uint16_t* __restrict__ agg, const uint16_t* __restrict__
 #pragma unroll
     for (int j = 0; j < M; ++j) R[j] = INF, N[j] = 0;
     uint32_t wn[KS];
-    if (xs < W)
+    // the staged ring (PF > 0), after the row records
+    constexpr int KQ = KS / 4 > 0 ? KS / 4 : 1;
+    uint4* const ring = reinterpret_cast<uint4*>(reinterpret_cast<uint8_t*>(rec) +
+                                                 (((size_t)W * (NB ? 8 : 4) + 15) & ~(size_t)15));
+    const int nvol = NV == 4 ? 4 : (rowB ? 2 : 1);
+    auto stage = [&](int j, int slot) {   // pixel xs + j of the segment into ring slot `slot`
+        if constexpr (PF > 0) {
+            const int x = xs + j;
+            if (j < S && x < W) {
+                const uint16_t* const src[4] = {rowA, rowB, rowC, rowD};
+#pragma unroll
+                for (int v = 0; v < (NV == 4 ? 4 : 2); ++v)
+                    if (v < nvol)
+#pragma unroll
+                        for (int q = 0; q < KQ; ++q)
+                            sel_cp16(&ring[((slot * NV + v) * KQ + q) * 256 + threadIdx.x],
+                                     src[v] + (size_t)x * Dp + 8 * q);
+            }
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+        }
+    };
+    if constexpr (PF > 0) {
+#pragma unroll
+        for (int k = 0; k < PF - 1; ++k) stage(k, k);
+    } else if (xs < W) {
         slide_load<KS, NV>(rowA + (size_t)xs * Dp, rowB ? rowB + (size_t)xs * Dp : nullptr,
                            NV == 4 ? rowC + (size_t)xs * Dp : nullptr, NV == 4 ? rowD + (size_t)xs * Dp : nullptr,
                            wrap, wn);
+    }
+    int slotNow = 0;   // ring slot of the current pixel (PF > 0)
     for (int s = 0; s < S; s += M) {
 #pragma unroll
         for (int u = 0; u < M; ++u) {
             const int x = xs + s + u;
             const bool px = x < W;
             uint32_t w[KS];
+            if constexpr (PF > 0) {
+                // pixel x + PF - 1 into the slot pixel x - 1 left; then pixel x has landed
+                const int slotNext = slotNow == 0 ? PF - 1 : slotNow - 1;
+                stage(s + u + PF - 1, slotNext);
+                asm volatile("cp.async.wait_group %0;\n" ::"n"(PF - 1) : "memory");
 #pragma unroll
-            for (int k = 0; k < KS; ++k) w[k] = wn[k];
-            if (x + 1 < W && (s + u + 1) < S)
-                slide_load<KS, NV>(rowA + (size_t)(x + 1) * Dp, rowB ? rowB + (size_t)(x + 1) * Dp : nullptr,
-                                   NV == 4 ? rowC + (size_t)(x + 1) * Dp : nullptr,
-                                   NV == 4 ? rowD + (size_t)(x + 1) * Dp : nullptr, wrap, wn);
+                for (int q = 0; q < KQ; ++q) {
+                    uint4 v = ring[((slotNow * NV + 0) * KQ + q) * 256 + threadIdx.x];
+                    if (nvol > 1) {
+                        const uint4 b = ring[((slotNow * NV + 1) * KQ + q) * 256 + threadIdx.x];
+                        v = make_uint4(vsum(v.x, b.x, wrap), vsum(v.y, b.y, wrap), vsum(v.z, b.z, wrap),
+                                       vsum(v.w, b.w, wrap));
+                    }
+                    if (NV == 4) {
+                        const uint4 c = ring[((slotNow * NV + 2) * KQ + q) * 256 + threadIdx.x];
+                        const uint4 d = ring[((slotNow * NV + 3) * KQ + q) * 256 + threadIdx.x];
+                        v = make_uint4(vsum(v.x, vsum(c.x, d.x, wrap), wrap), vsum(v.y, vsum(c.y, d.y, wrap), wrap),
+                                       vsum(v.z, vsum(c.z, d.z, wrap), wrap), vsum(v.w, vsum(c.w, d.w, wrap), wrap));
+                    }
+                    w[4 * q] = v.x; w[4 * q + 1] = v.y; w[4 * q + 2] = v.z; w[4 * q + 3] = v.w;
+                }
+                slotNow = slotNow + 1 == PF ? 0 : slotNow + 1;
+            } else {
+#pragma unroll
+                for (int k = 0; k < KS; ++k) w[k] = wn[k];
+                if (x + 1 < W && (s + u + 1) < S)
+                    slide_load<KS, NV>(rowA + (size_t)(x + 1) * Dp, rowB ? rowB + (size_t)(x + 1) * Dp : nullptr,
+                                       NV == 4 ? rowC + (size_t)(x + 1) * Dp : nullptr,
+                                       NV == 4 ? rowD + (size_t)(x + 1) * Dp : nullptr, wrap, wn);
+            }
             // slide by one: the slot leaving this lane (logical M-1, physical
             // (M-1-u) mod M) enters the next lane as its logical slot 0 and
             // this lane's logical 0 takes the previous lane's
@@ -288,13 +358,13 @@ select_slide_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict
 
 // Neighbours carried: two CTAs an SM with 128 registers for the words and their pairs
 // (measured faster than the default budget).
-template <int TL, int KS, bool FULL, int NV>
+template <int TL, int KS, bool FULL, int NV, int PF>
 __global__ void __launch_bounds__(256, 2)
 select_slide_nb_kernel(const uint16_t* __restrict__ agg, const uint16_t* __restrict__ aggB,
                        const uint16_t* __restrict__ aggC, const uint16_t* __restrict__ aggD, int wrap,
                        int W, int D, int Dp, int minD, int UR, int S, int16_t* __restrict__ dispL,
                        int16_t* __restrict__ dispR) {
-    select_slide_body<TL, KS, FULL, NV, true>(agg, aggB, aggC, aggD, wrap, W, D, Dp, minD, UR, S, dispL, dispR);
+    select_slide_body<TL, KS, FULL, NV, true, PF>(agg, aggB, aggC, aggD, wrap, W, D, Dp, minD, UR, S, dispL, dispR);
 }
 
 constexpr size_t kSelectSmemMax = 227 * 1024;  // opt-in shared memory per block on sm_100
@@ -309,16 +379,39 @@ static cudaError_t launch_select_slide(const uint16_t* agg, const uint16_t* aggB
     // 64-bit row records fit; wider lanes keep re-reading (measured: with 10 words a
     // lane the registers of the pairs cost more than the re-reads save)
     const bool nb = KS <= 8 && (size_t)W * 8 <= kSelectSmemMax;
-    const size_t smem = (size_t)W * (nb ? 8 : 4);
     const bool four = aggB && aggC && aggD;
+    size_t smem = (size_t)W * (nb ? 8 : 4);
+    // the staged ring for lanes of 4 words (640x480 D64: selection + post 0.088 ->
+    // 0.057 ms): three slots (two pixels in flight) when two CTAs an SM still fit,
+    // else two; lanes of 8 words keep the register form (1080p D128: 0.525 ms
+    // against 0.695 staged)
+    int pf = 0;
+    if (nb && KS == 4) {
+        const size_t base = (smem + 15) & ~(size_t)15;
+        for (int cand : {3, 2})
+            if (!pf && 2 * (base + select_ring_bytes(cand, four ? 4 : 2, KS) + 1024) <= 228 * 1024) pf = cand;
+        if (pf) smem = base + select_ring_bytes(pf, four ? 4 : 2, KS);
+    }
     void (*kern)(const uint16_t*, const uint16_t*, const uint16_t*, const uint16_t*, int, int, int, int, int, int,
                  int, int16_t*, int16_t*);
-    if constexpr (KS <= 8)
-        kern = nb ? (four ? (D == Dp ? select_slide_nb_kernel<TL, KS, true, 4> : select_slide_nb_kernel<TL, KS, false, 4>)
-                          : (D == Dp ? select_slide_nb_kernel<TL, KS, true, 2> : select_slide_nb_kernel<TL, KS, false, 2>))
-                  : (four ? (D == Dp ? select_slide_kernel<TL, KS, true, 4> : select_slide_kernel<TL, KS, false, 4>)
-                          : (D == Dp ? select_slide_kernel<TL, KS, true, 2> : select_slide_kernel<TL, KS, false, 2>));
-    else
+    if constexpr (KS <= 8) {
+        constexpr int P3 = KS == 4 ? 3 : 0, P2 = KS == 4 ? 2 : 0;
+        auto pick = [&](auto full3_4, auto part3_4, auto full3_2, auto part3_2) {
+            return four ? (D == Dp ? full3_4 : part3_4) : (D == Dp ? full3_2 : part3_2);
+        };
+        if (!nb)
+            kern = pick(select_slide_kernel<TL, KS, true, 4>, select_slide_kernel<TL, KS, false, 4>,
+                        select_slide_kernel<TL, KS, true, 2>, select_slide_kernel<TL, KS, false, 2>);
+        else if (pf == 3)
+            kern = pick(select_slide_nb_kernel<TL, KS, true, 4, P3>, select_slide_nb_kernel<TL, KS, false, 4, P3>,
+                        select_slide_nb_kernel<TL, KS, true, 2, P3>, select_slide_nb_kernel<TL, KS, false, 2, P3>);
+        else if (pf == 2)
+            kern = pick(select_slide_nb_kernel<TL, KS, true, 4, P2>, select_slide_nb_kernel<TL, KS, false, 4, P2>,
+                        select_slide_nb_kernel<TL, KS, true, 2, P2>, select_slide_nb_kernel<TL, KS, false, 2, P2>);
+        else
+            kern = pick(select_slide_nb_kernel<TL, KS, true, 4, 0>, select_slide_nb_kernel<TL, KS, false, 4, 0>,
+                        select_slide_nb_kernel<TL, KS, true, 2, 0>, select_slide_nb_kernel<TL, KS, false, 2, 0>);
+    } else
         kern = four ? (D == Dp ? select_slide_kernel<TL, KS, true, 4> : select_slide_kernel<TL, KS, false, 4>)
                     : (D == Dp ? select_slide_kernel<TL, KS, true, 2> : select_slide_kernel<TL, KS, false, 2>);
     if (smem > 48 * 1024) {
