@@ -120,6 +120,10 @@ __device__ __forceinline__ uint32_t vol_cost(const uint16_t* __restrict__ a, con
 __host__ __device__ inline size_t select_ring_bytes(int PF, int NV, int KS) {
     return (size_t)PF * NV * (KS / 4) * 256 * 16;
 }
+constexpr int kSelL2Ahead = 3;   // pixels of L2 prefetch ahead (register form)
+__device__ __forceinline__ void sel_prefetch_l2(const void* gmem) {
+    asm volatile("prefetch.global.L2 [%0];\n" ::"l"(gmem));
+}
 __device__ __forceinline__ void sel_cp16(void* smem, const void* gmem) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((uint32_t)__cvta_generic_to_shared(smem)),
                  "l"(gmem)
@@ -226,6 +230,18 @@ select_slide_body(const uint16_t* __restrict__ agg, const uint16_t* __restrict__
             } else {
 #pragma unroll
                 for (int k = 0; k < KS; ++k) w[k] = wn[k];
+                // the team's pixel three ahead into L2 (one 128-byte line a request,
+                // every fourth lane of a team for lanes of 8 words): the register
+                // load-ahead of the next pixel then comes from L2
+                if (x + kSelL2Ahead < W && (s + u + kSelL2Ahead) < S && (tl * M * 2) % 128 == 0) {
+                    const size_t o = (size_t)(x + kSelL2Ahead) * Dp;
+                    sel_prefetch_l2(rowA + o);
+                    if (rowB) sel_prefetch_l2(rowB + o);
+                    if (NV == 4) {
+                        sel_prefetch_l2(rowC + o);
+                        sel_prefetch_l2(rowD + o);
+                    }
+                }
                 if (x + 1 < W && (s + u + 1) < S)
                     slide_load<KS, NV>(rowA + (size_t)(x + 1) * Dp, rowB ? rowB + (size_t)(x + 1) * Dp : nullptr,
                                        NV == 4 ? rowC + (size_t)(x + 1) * Dp : nullptr,
