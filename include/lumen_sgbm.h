@@ -114,10 +114,12 @@ const char* lumen_last_error_string(void);
 lumen_status lumen_sgbm_debug_set_paths(lumen_sgbm* h, uint32_t path_mask);
 /* Aggregation schedule: 0 = automatic (autotuner / heuristic), 1 = one kernel
  * per direction, 4 = two fused wavefront sweeps with lockstep row bands and
- * helper warps for the band hand-offs (the batched form's kernel), 6 = four
+ * helper warps for the band hand-offs (the batched form's usual pick), 6 = four
  * lag-free sweeps, two over rows and two over columns: two paths each with 8
- * paths, one path each with 4 (then no band waits on another) -- the default
- * for padded disparities up to 320; wider ranges fall back to schedule 4.
+ * paths (the row and the column sweeps as two concurrent launches unless
+ * tuned otherwise), one path each with 4 (then no band waits on another) --
+ * the default for padded disparities up to 320; wider ranges fall back to
+ * schedule 4.
  * Other values are refused (LUMEN_ERR_INVALID_ARGUMENT).  Outputs are
  * identical for every schedule. */
 lumen_status lumen_sgbm_set_schedule(lumen_sgbm* h, int schedule);
