@@ -14,12 +14,14 @@
 //    slots is free.  A batch is uploaded, rectified through the resident maps
 //    of its calibration id (lumen_rectifier), and computed by the batched
 //    launch core (batch_core.cuh): per pair cost volumes on the slot's
-//    stream, one persistent sweep launch per kernel class on the server's
-//    aggregation stream (sweep launches of different batches never overlap,
-//    so each one's resident CTAs cover its hand-off window), per pair
-//    selection, and the copy back.  A batch admitted while another is on the
-//    GPU overlaps with it: its uploads and cost volumes run beside the other's
-//    sweep, its sweep follows the other's directly.
+//    stream, one persistent sweep launch per kernel class, per pair
+//    selection, and the copy back.  Schedule 4's sweep launches go to the
+//    server's aggregation stream (sweep launches of different batches never
+//    overlap, so each one's resident CTAs cover its hand-off window);
+//    schedule 6's bands wait only on earlier bands of their own launch, so
+//    its sweeps stay on the slot's stream and batches overlap entirely.  A
+//    batch admitted while another is on the GPU overlaps with it: its
+//    uploads and cost volumes run beside the other's sweep.
 //  * The thread retires batches whose completion event has fired: results go
 //    to the callers' buffers, arena slices are freed, waiters are woken.  A
 //    batch still running after `watchdog_ms` has its requests completed with
@@ -316,7 +318,7 @@ lumen_status slot_launch(lumen_server* S, Slot& sl, std::vector<Request*>& adm) 
     unsigned long long nl = 0;
     lumen_status es = batch_enqueue_groups(sl.pairs, sl.groups, sl.dDesc, S->magic, sl.dStatus,
                                            S->opt.spin_limit ? S->opt.spin_limit : (1ll << 24), sl.s,
-                                           S->agg, sl.evs.data(), &nl);
+                                           S->opt.schedule == 6 ? nullptr : S->agg, sl.evs.data(), &nl);
     if (es != LUMEN_OK) return es;
     for (size_t i = 0; i < adm.size(); ++i) {
         const size_t n = (size_t)adm[i]->W * adm[i]->H;
