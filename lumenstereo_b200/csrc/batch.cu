@@ -398,9 +398,6 @@ struct lumen_sgbm_batch {
     // selS, cost volumes on the caller's stream
     bool overlap = false;
     cudaStream_t aggS = nullptr, selS = nullptr;
-    // schedule 6: odd groups' sweeps on a second stream, so that consecutive
-    // groups' sweeps overlap (its bands wait only on their own launch's)
-    cudaStream_t aggS2 = nullptr;
     std::vector<cudaEvent_t> evs;  // fork, 2 joins, then 3 per group
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -501,7 +498,7 @@ static lumen_status batch_plan(lumen_sgbm_batch* b) {
         poolNeed = std::max(poolNeed, o);
     }
     if (b->overlap) {
-        b->evs.resize(4 + 3 * b->groups.size(), nullptr);   // + the second sweep stream's join
+        b->evs.resize(3 + 3 * b->groups.size(), nullptr);
         for (cudaEvent_t& e : b->evs) BCU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
     BCU(cudaMalloc(&b->pool, std::max<size_t>(poolNeed, 256)));
@@ -530,7 +527,6 @@ static lumen_status batch_enqueue(lumen_sgbm_batch* b, cudaStream_t s) {
     cudaEvent_t* ev = b->evs.data();
     BCU(cudaEventRecord(ev[0], s));
     BCU(cudaStreamWaitEvent(b->aggS, ev[0], 0));
-    BCU(cudaStreamWaitEvent(b->aggS2, ev[0], 0));
     BCU(cudaStreamWaitEvent(b->selS, ev[0], 0));
     for (size_t gi = 0; gi < b->groups.size(); ++gi) {
         const BatchGroup& g = b->groups[gi];
@@ -539,23 +535,19 @@ static lumen_status batch_enqueue(lumen_sgbm_batch* b, cudaStream_t s) {
         lumen_status st = batch_enqueue_costs(b->pairs, g, desc, b->magic, s, &nl);
         if (st != LUMEN_OK) return st;
         BCU(cudaEventRecord(costsDone, s));
-        cudaStream_t sw = (g.sched == 6 && gi % 2) ? b->aggS2 : b->aggS;
-        BCU(cudaStreamWaitEvent(sw, costsDone, 0));
-        st = batch_enqueue_wave(g, desc, b->status, b->spinMax, sw, &nl);
+        BCU(cudaStreamWaitEvent(b->aggS, costsDone, 0));
+        st = batch_enqueue_wave(g, desc, b->status, b->spinMax, b->aggS, &nl);
         if (st != LUMEN_OK) return st;
-        BCU(cudaEventRecord(sweepDone, sw));
+        BCU(cudaEventRecord(sweepDone, b->aggS));
         BCU(cudaStreamWaitEvent(b->selS, sweepDone, 0));
         st = batch_enqueue_selects(b->pairs, g, b->selS, &nl);
         if (st != LUMEN_OK) return st;
         BCU(cudaEventRecord(selDone, b->selS));
     }
-    cudaEvent_t join2 = ev[3 + 3 * b->groups.size()];
     BCU(cudaEventRecord(ev[1], b->aggS));
     BCU(cudaEventRecord(ev[2], b->selS));
-    BCU(cudaEventRecord(join2, b->aggS2));
     BCU(cudaStreamWaitEvent(s, ev[1], 0));
     BCU(cudaStreamWaitEvent(s, ev[2], 0));
-    BCU(cudaStreamWaitEvent(s, join2, 0));
     b->launches = nl;
     return LUMEN_OK;
 }
@@ -580,7 +572,6 @@ extern "C" lumen_status lumen_sgbm_batch_create(lumen_sgbm_batch** out) {
     if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prLeast, &prGreatest);
     // sweeps first: their CTAs wait on one another, the other kernels do not
     if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&b->aggS, cudaStreamNonBlocking, prGreatest);
-    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&b->aggS2, cudaStreamNonBlocking, prGreatest);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->selS, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
@@ -599,7 +590,6 @@ extern "C" lumen_status lumen_sgbm_batch_destroy(lumen_sgbm_batch* b) {
     if (b->magic) cudaFree(b->magic);
     if (b->capStream) cudaStreamDestroy(b->capStream);
     if (b->aggS) cudaStreamDestroy(b->aggS);
-    if (b->aggS2) cudaStreamDestroy(b->aggS2);
     if (b->selS) cudaStreamDestroy(b->selS);
     delete b;
     return LUMEN_OK;
