@@ -63,6 +63,10 @@ def parse():
     ap.add_argument("--requests", type=int, default=200,
                     help="requests per offered rate (--mode serve; 0: 25 s of arrivals, at most 10000)")
     ap.add_argument("--inflight", type=int, default=2, help="batches on the device at once (--mode serve)")
+    # the server counts every working byte of a request against its arena (about 10 bytes a
+    # pixel-disparity with schedule 6); 120 GiB keeps the cost volumes in flight near 12 GB,
+    # inside a 40 GB cost-volume budget
+    ap.add_argument("--budget-gib", type=int, default=120, help="device arena of the server, GiB (--mode serve)")
     ap.add_argument("--rates", default="20,50,100,200,300,400", help="offered rates, requests/s (--mode serve)")
     return ap.parse_args()
 
@@ -583,7 +587,8 @@ def run_serve(args):
         plain_one(item)
     plain_rate = len(pool) / (time.perf_counter() - t0)
     srv_sched = args.schedule if args.schedule in (4, 6) else 6
-    srv = StereoServer(budget_bytes=40 << 30, max_batch_pairs=32, rows_per_band=16, max_inflight=args.inflight,
+    srv = StereoServer(budget_bytes=args.budget_gib << 30, max_batch_pairs=32, rows_per_band=16,
+                       max_inflight=args.inflight,
                        schedule=srv_sched)
     for key, (w, h, m) in maps.items():
         srv.set_calibration(key, w, h, *m)
@@ -641,7 +646,7 @@ def run_serve(args):
                       "calibrations": "16 ids (seed % 16), rectified on the device from resident maps",
                       "arrivals": "Poisson",
                       "requests_per_rate": args.requests or "25 s of arrivals, at most 10000",
-                      "budget_bytes": 40 << 30, "max_batch_pairs": 32, "max_inflight": args.inflight,
+                      "budget_bytes": args.budget_gib << 30, "max_batch_pairs": 32, "max_inflight": args.inflight,
                       "schedule": srv_sched, "rows_per_band": 16},
            "p50_ms": best["p50_ms"], "p99_ms": best["p99_ms"], "p999_ms": best["p999_ms"],
            "rates": sweep,
