@@ -101,6 +101,13 @@ CASES = {
                                      numDirections=8)),
     "census_minD100_wide": (120, 16, dict(minDisparity=100, maxDisparity=164,
                                           matchingCostMode=1)),
+    # widths divisible by 4: the 5x5 SAD kernel stages right rows a word at a time
+    # (Dp 128 with minDisparity, 192, 256 with a partial last quad, 320 with one
+    # column-sum buffer), tiles running past both image edges and 70 rows (3 row tiles)
+    "sad_minD5_d128_w4": (136, 70, dict(minDisparity=5, maxDisparity=133, numDirections=8)),
+    "sad_d192_w4": (200, 40, dict(maxDisparity=192, numDirections=8)),
+    "sad_minD7_d250_w4": (264, 36, dict(minDisparity=7, maxDisparity=257)),
+    "sad_d300_w4": (324, 24, dict(maxDisparity=300, numDirections=8)),
 }
 
 
